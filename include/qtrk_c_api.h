@@ -1,0 +1,233 @@
+/*
+ * qtrk_c_api.h — C ABI of libqtrk_b200.so, a drop-in for QTrk's tracker DLL.
+ *
+ * Every entry point below has the name, argument list, argument meaning and packed
+ * struct layout of the reference declaration it replaces (cputrack/qtrk_c_api.h and
+ * cputrack/utils.h of jcnossen/qtrk), so the .NET P/Invoke mirror
+ * (QTrkDotNet/QTrkDLL.cs:244-405) and ctypes/cgo-style callers bind unchanged.
+ * The localization work behind them runs on one NVIDIA B200 (sm_100a) in hand-written
+ * CUDA kernels; the library has no CPU fallback: when no usable GPU is present
+ * QTrkCreateInstance returns NULL and QTrkGetLastError() says why.
+ *
+ * Differences in behaviour from the reference, all additive:
+ *  - no C++ exception crosses this ABI (the reference lets them escape,
+ *    cputrack/qtrk_c_api.cpp:62-175); errors are logged per instance and returned by
+ *    QTrkGetWarnings, or by QTrkGetLastError for calls without an instance;
+ *  - results come back in FIFO order, like the reference CUDA tracker
+ *    (cudatrack/QueuedCUDATracker.cu:726-737);
+ *  - the declared-but-never-defined reference entry points
+ *    (QTrkSetPixelCalibrationImages, QTrkSetPixelCalibrationFactors,
+ *    QTrkEnableRadialZLUTCompareProfile, QTrkGetRadialZLUTCompareProfile,
+ *    QTrkBuildLUTFromFrame) are implemented;
+ *  - QTrkB200* entry points at the end extend the ABI (device-resident batches,
+ *    tensor-core Z match, adjoint gradients, serving statistics).
+ */
+#ifndef QTRK_B200_C_API_H
+#define QTRK_B200_C_API_H
+
+#include <stdint.h>
+#include <stddef.h>
+#ifndef __cplusplus
+#include <stdbool.h>
+#endif
+
+#if defined(_WIN32)
+#define QTRK_CALLCONV __cdecl
+#define QTRK_EXPORT __declspec(dllexport)
+#else
+#define QTRK_CALLCONV
+#define QTRK_EXPORT __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+#define QTRK_API extern "C" QTRK_EXPORT
+#else
+#define QTRK_API QTRK_EXPORT
+#endif
+
+/* Localization mode bit flags; values of cputrack/qtrk_c_api.h:5-20. */
+enum LocalizeModeEnum {
+    LT_OnlyCOM = 0,
+    LT_XCor1D = 1,
+    LT_QI = 2,
+    LT_Gaussian2D = 4,
+    LT_ZLUTAlign = 8,
+    LT_LocalizeZ = 16,
+    LT_NormalizeProfile = 64,
+    LT_ClearFirstFourPixels = 128,
+    LT_FourierLUT = 256,
+    LT_LocalizeZWeighted = 512,
+    /* Extension bits (no reference counterpart). */
+    LT_B200_ZMatchBF16 = 1 << 20,    /* Z cross term on the tensor cores (BF16, FP32 accumulate) */
+    LT_B200_JointRefine = 1 << 21,   /* joint Gauss-Newton (x,y,z) refinement after the Z fit */
+    LT_B200_Gaussian5P = 1 << 22,    /* 5-parameter (x,y,I0,bg,sigma) full-Newton Gaussian MLE */
+    LT_Force32Bit = (int)0xffffffff
+};
+typedef int LocMode_t;
+
+/* cputrack/qtrk_c_api.h:24-29 */
+enum QTRK_PixelDataType { QTrkU8 = 0, QTrkU16 = 1, QTrkFloat = 2 };
+typedef int QTRK_PixelDataType_t;
+
+#pragma pack(push, 4)
+/* cputrack/std_incl.h:20-116 (pack(4)) */
+typedef struct vector2f { float x, y; } vector2f;
+typedef struct vector3f { float x, y, z; } vector3f;
+/* TImageData<float>, cputrack/utils.h:77-138 (pack(4)): data, w, h */
+typedef struct ImageData { float *data; int w, h; } ImageData;
+#pragma pack(pop)
+
+#pragma pack(push, 1)
+/* 24 bytes; cputrack/qtrk_c_api.h:34-45 */
+typedef struct LocalizationJob {
+    uint32_t frame, timestamp;
+    int32_t zlutIndex;
+    vector3f initialPos;
+} LocalizationJob;
+
+/* 52 bytes; cputrack/qtrk_c_api.h:49-57 */
+typedef struct LocalizationResult {
+    LocalizationJob job;
+    vector3f pos;
+    vector2f firstGuess;
+    uint32_t error;
+    float imageMean;
+} LocalizationResult;
+
+/* 84 bytes; cputrack/qtrk_c_api.h:59-114 (field order is the ABI) */
+typedef struct QTrkSettings {
+    int width, height;
+    int numThreads;
+    int cuda_device;
+    float com_bgcorrection;
+    float zlut_minradius;
+    float zlut_radial_coverage;
+    float zlut_angular_coverage;
+    float zlut_roi_coverage;
+    int qi_iterations;
+    float qi_minradius;
+    float qi_radial_coverage;
+    float qi_angular_coverage;
+    float qi_roi_coverage;
+    float qi_angstep_factor;
+    int xc1_profileLength;
+    int xc1_profileWidth;
+    int xc1_iterations;
+    int gauss2D_iterations;
+    float gauss2D_sigma;
+    int downsample;
+} QTrkSettings;
+
+/* 108 bytes; cputrack/qtrk_c_api.h:123-138 */
+typedef struct QTrkComputedConfig {
+    QTrkSettings base;
+    int zlut_radialsteps;
+    int zlut_angularsteps;
+    float zlut_maxradius;
+    int qi_radialsteps;
+    int qi_angstepspq;
+    float qi_maxradius;
+} QTrkComputedConfig;
+
+/* 8 bytes; cputrack/qtrk_c_api.h:116-119 */
+typedef struct ROIPosition { int x, y; } ROIPosition;
+#pragma pack(pop)
+
+#define QTrkCUDA_UseList -3
+#define QTrkCUDA_UseAll -2
+#define QTrkCUDA_UseBest -1
+
+/* cputrack/QueuedTracker.h:305-308 */
+#define BUILDLUT_IMAGELUT 1
+#define BUILDLUT_FOURIER 2
+#define BUILDLUT_NORMALIZE 4
+#define BUILDLUT_BIASCORRECT 8
+
+#ifdef __cplusplus
+struct QueuedTracker;
+#else
+typedef struct QueuedTracker QueuedTracker;
+#endif
+
+/* ---- configuration (cputrack/qtrk_c_api.cpp:12-25) ---- */
+QTRK_API void QTRK_CALLCONV TestDLLCallConv(int a);                                   /* qtrk_c_api.cpp:12 */
+QTRK_API void QTRK_CALLCONV QTrkGetDefaultConfig(QTrkSettings *cfg);                  /* qtrk_c_api.cpp:17 */
+QTRK_API void QTRK_CALLCONV QTrkGetComputedConfig(QTrkSettings *base, QTrkComputedConfig *cfg); /* qtrk_c_api.cpp:22 */
+
+/* ---- instance lifecycle (cputrack/qtrk_c_api.h:144-148) ---- */
+QTRK_API struct QueuedTracker *QTRK_CALLCONV QTrkCreateInstance(QTrkSettings *cfg);   /* qtrk_c_api.h:144 */
+QTRK_API void QTRK_CALLCONV QTrkFreeInstance(struct QueuedTracker *qtrk);             /* qtrk_c_api.h:145 */
+QTRK_API void QTRK_CALLCONV QTrkSetLocalizationMode(struct QueuedTracker *qtrk, LocMode_t locType); /* qtrk_c_api.h:148 */
+
+/* ---- pixel calibration (declared, never defined, in cputrack/qtrk_c_api.h:152-153) ---- */
+QTRK_API void QTRK_CALLCONV QTrkSetPixelCalibrationImages(struct QueuedTracker *qtrk, float *offset, float *gain);
+/* No instance argument in the reference declaration: sets the factors of every live instance
+ * and the default of instances created later. */
+QTRK_API void QTRK_CALLCONV QTrkSetPixelCalibrationFactors(float offsetFactor, float gainFactor);
+
+/* ---- scheduling (cputrack/qtrk_c_api.h:158-163) ---- */
+QTRK_API void QTRK_CALLCONV QTrkScheduleLocalization(struct QueuedTracker *qtrk, void *data, int pitch,
+                                                     QTRK_PixelDataType_t pdt, const LocalizationJob *jobInfo);
+QTRK_API void QTRK_CALLCONV QTrkClearResults(struct QueuedTracker *qtrk);             /* qtrk_c_api.h:159 */
+QTRK_API void QTRK_CALLCONV QTrkFlush(struct QueuedTracker *qtrk);                    /* qtrk_c_api.h:160 */
+QTRK_API int QTRK_CALLCONV QTrkScheduleFrame(struct QueuedTracker *qtrk, void *imgptr, int pitch, int width,
+                                             int height, ROIPosition *positions, int numROI,
+                                             QTRK_PixelDataType_t pdt, const LocalizationJob *jobInfo); /* qtrk_c_api.h:163 */
+
+/* ---- Z-LUT (cputrack/qtrk_c_api.h:165-185) ---- */
+/* No instance argument in the reference declarations (qtrk_c_api.h:165-166): they act on the
+ * most recently created live instance. */
+QTRK_API void QTRK_CALLCONV QTrkEnableRadialZLUTCompareProfile(bool enabled);
+QTRK_API void QTRK_CALLCONV QTrkGetRadialZLUTCompareProfile(float *dst); /* dst = [count * planes] */
+QTRK_API void QTRK_CALLCONV QTrkSetRadialZLUT(struct QueuedTracker *qtrk, float *data, int count, int planes); /* qtrk_c_api.h:169 */
+QTRK_API void QTRK_CALLCONV QTrkGetRadialZLUT(struct QueuedTracker *qtrk, float *dst);                        /* qtrk_c_api.h:170 */
+QTRK_API void QTRK_CALLCONV QTrkGetRadialZLUTSize(struct QueuedTracker *qtrk, int *count, int *planes, int *radialsteps); /* qtrk_c_api.h:171 */
+QTRK_API void QTRK_CALLCONV QTrkSetRadialWeights(struct QueuedTracker *qtrk, float *zcmp);                    /* qtrk_c_api.h:174 */
+QTRK_API void QTRK_CALLCONV QTrkBeginLUT(struct QueuedTracker *qtrk, unsigned int flags);                     /* qtrk_c_api.h:178 */
+QTRK_API void QTRK_CALLCONV QTrkBuildLUT(struct QueuedTracker *qtrk, void *data, int pitch, QTRK_PixelDataType_t pdt,
+                                         int plane, vector2f *known_pos);                                     /* qtrk_c_api.h:179 */
+QTRK_API void QTRK_CALLCONV QTrkBuildLUTFromFrame(struct QueuedTracker *qtrk, ImageData *frame, int plane,
+                                                  ROIPosition *roipos, int numroi);                           /* qtrk_c_api.h:184 */
+QTRK_API void QTRK_CALLCONV QTrkFinalizeLUT(struct QueuedTracker *qtrk);                                      /* qtrk_c_api.h:185 */
+
+/* ---- results and state (cputrack/qtrk_c_api.h:187-199) ---- */
+QTRK_API int QTRK_CALLCONV QTrkGetResultCount(struct QueuedTracker *qtrk);                                    /* qtrk_c_api.h:187 */
+QTRK_API int QTRK_CALLCONV QTrkFetchResults(struct QueuedTracker *qtrk, LocalizationResult *results, int maxResults); /* qtrk_c_api.h:188 */
+QTRK_API int QTRK_CALLCONV QTrkGetQueueLength(struct QueuedTracker *qtrk, int *maxQueueLen);                  /* qtrk_c_api.h:190 */
+QTRK_API bool QTRK_CALLCONV QTrkIsIdle(struct QueuedTracker *qtrk);                                           /* qtrk_c_api.h:191 */
+QTRK_API void QTRK_CALLCONV QTrkGetProfileReport(struct QueuedTracker *qtrk, char *dst, int maxStrLen);       /* qtrk_c_api.h:198 */
+QTRK_API void QTRK_CALLCONV QTrkGetWarnings(struct QueuedTracker *qtrk, char *dst, int maxStrLen);            /* qtrk_c_api.h:199 */
+
+/* ---- profile utilities exported by the reference (cputrack/utils.h:182-188,216) ---- */
+QTRK_API void QTRK_CALLCONV ComputeRadialProfile(float *dst, int radialSteps, int angularSteps, float minradius,
+                                                 float maxradius, vector2f center, ImageData *src, float mean,
+                                                 bool normalize);                                            /* utils.h:182 */
+QTRK_API void QTRK_CALLCONV NormalizeRadialProfile(float *prof, int rsteps);                                  /* utils.h:183 */
+QTRK_API void QTRK_CALLCONV NormalizeImage(ImageData *image);                                                 /* utils.h:185 */
+QTRK_API void QTRK_CALLCONV GenerateImageFromLUT(ImageData *image, ImageData *zlut, float minradius, float maxradius,
+                                                 vector3f pos, bool useSplineInterp, int ovs);                /* utils.h:186 */
+QTRK_API void QTRK_CALLCONV GenerateGaussianSpotImage(ImageData *img, vector2f pos, float sigma, float I0, float Ibg); /* utils.h:216 */
+
+/* ================= Extensions (no reference counterpart) ================= */
+
+/* Text of the last error raised by a call that has no instance to report to (e.g. a failed
+ * QTrkCreateInstance). Returns the number of characters written. */
+QTRK_API int QTRK_CALLCONV QTrkB200GetLastError(char *dst, int maxStrLen);
+
+/* Number of CUDA kernels this instance launched since creation (all streams). */
+QTRK_API int64_t QTRK_CALLCONV QTrkB200GetKernelLaunchCount(struct QueuedTracker *qtrk);
+
+/*
+ * Localize `count` ROIs that are already resident in device memory, on the caller's CUDA
+ * stream (cudaStream_t passed as void*; NULL = legacy default stream). ROI i starts at
+ * d_pixels + i * roi_stride_bytes; rows are `pitch` bytes apart. d_jobs (device,
+ * LocalizationJob[count]) may be NULL (job = {frame=i, zlutIndex=0}). d_results receives
+ * LocalizationResult[count] (device). Uses the instance's mode, LUT and settings. Returns 0
+ * on success, a negative code on a bad argument (see QTrkGetWarnings). Asynchronous.
+ */
+QTRK_API int QTRK_CALLCONV QTrkB200LocalizeDevice(struct QueuedTracker *qtrk, const void *d_pixels, int pitch,
+                                                  int64_t roi_stride_bytes, QTRK_PixelDataType_t pdt, int count,
+                                                  const LocalizationJob *d_jobs, LocalizationResult *d_results,
+                                                  void *stream);
+
+#endif /* QTRK_B200_C_API_H */

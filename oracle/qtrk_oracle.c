@@ -1,0 +1,696 @@
+/*
+ * qtrk_oracle.c — FP64 CPU restatement of QTrk's bead-localization path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This file is the checker for the GPU library: tests/,
+ * __graft_entry__.smoke() and bench.py's cpu_baseline leg may load it; the product
+ * library never does. It restates, in double precision and in my own code, the
+ * algorithms of the reference CPU tracker (jcnossen/qtrk cputrack/), keeping every
+ * discrete decision of the reference identical (int truncations, the bilinear
+ * "outside" rule, sample-count thresholds, the argmax window of the quadratic fit).
+ * It is pinned against the reference itself, compiled from its own sources into
+ * oracle/_ref/libqtrk_ref.so (tests/test_oracle_pin.py) and through the committed
+ * fixtures in tests/golden/.
+ *
+ * The QI cross-correlation is evaluated as a direct O(L^2) circular correlation in
+ * double instead of KISS FFT: the result of the reference's FFT path
+ * (cpu_tracker.cpp:375-406) is the same mathematical quantity, so only rounding differs.
+ *
+ * Beyond the reference it also holds FP64 versions of the extensions of the GPU library:
+ * the 5-parameter Gaussian MLE, the radial-profile/LUT cost with its analytic gradient
+ * (x, y, z and LUT entries), and the joint Gauss-Newton (x,y,z) refinement.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORACLE_API __attribute__((visibility("default")))
+
+/* Reference constants: QueuedTracker.h:349,359 (fit weights), QueuedTracker.h:261 (min samples). */
+static const double QI_WEIGHTS[7] = {0.14, 0.5, 0.85, 1.0, 0.85, 0.5, 0.14};
+static const double ZLUT_WEIGHTS[7] = {0.15, 0.5, 0.85, 1.0, 0.85, 0.5, 0.15};
+#define MIN_RADPROFILE_SMP_COUNT 4
+#define REF_PI_F 3.141593 /* the reference writes pi as 3.141593f in its angle tables */
+
+/* Localization mode flags, cputrack/qtrk_c_api.h:5-20. */
+#define LT_QI 2
+#define LT_Gaussian2D 4
+#define LT_LocalizeZ 16
+#define LT_NormalizeProfile 64
+#define LT_ClearFirstFourPixels 128
+
+#pragma pack(push, 1)
+typedef struct {
+    int width, height, numThreads, cuda_device;
+    float com_bgcorrection, zlut_minradius, zlut_radial_coverage, zlut_angular_coverage, zlut_roi_coverage;
+    int qi_iterations;
+    float qi_minradius, qi_radial_coverage, qi_angular_coverage, qi_roi_coverage, qi_angstep_factor;
+    int xc1_profileLength, xc1_profileWidth, xc1_iterations, gauss2D_iterations;
+    float gauss2D_sigma;
+    int downsample;
+    int zlut_radialsteps, zlut_angularsteps;
+    float zlut_maxradius;
+    int qi_radialsteps, qi_angstepspq;
+    float qi_maxradius;
+} oracle_config; /* layout of QTrkComputedConfig, cputrack/qtrk_c_api.h:59-138 */
+#pragma pack(pop)
+
+/* NearestPowerOf2, utils.cpp:644-652 (int/float arithmetic kept as in the reference). */
+ORACLE_API int oracle_nearest_pow2(int v)
+{
+    int r = 1;
+    while (r < v) r *= 2;
+    if (fabsf((float)(r - v)) < fabsf((float)(r / 2 - v))) return r;
+    return r / 2;
+}
+
+/* QTrkComputedConfig::Update, QueuedTracker.cpp:6-21. Float arithmetic and int truncation as
+ * in the reference, because the step counts it produces are discrete. */
+ORACLE_API void oracle_update_config(oracle_config *c)
+{
+    int roi = c->width / 2;
+    c->zlut_maxradius = roi * c->zlut_roi_coverage;
+    float zlut_perimeter = 2 * 3.141593f * c->zlut_maxradius;
+    c->zlut_angularsteps = (int)(zlut_perimeter * c->zlut_angular_coverage);
+    c->zlut_radialsteps = (int)((c->zlut_maxradius - c->zlut_minradius) * c->zlut_radial_coverage);
+    c->qi_maxradius = roi * c->qi_roi_coverage;
+    float qi_perimeter = 2 * 3.141593f * c->qi_maxradius;
+    c->qi_angstepspq = (int)(qi_perimeter * c->qi_angular_coverage / 4);
+    c->qi_radialsteps = (int)((c->qi_maxradius - c->qi_minradius) * c->qi_radial_coverage);
+    c->qi_radialsteps = oracle_nearest_pow2(c->qi_radialsteps);
+}
+
+/* ComputeRadialBinWindow, utils.cpp:665-677. */
+ORACLE_API void oracle_radial_bin_window(int rsteps, double *dst)
+{
+    for (int i = 0; i < rsteps; i++) {
+        double x = i / (double)rsteps;
+        double fall = 1.0 - exp(-(1 - x) * (1 - x) / 0.05);
+        double rise = 1.0 - exp(-(x * x) / 0.01);
+        dst[i] = sqrt(fall * rise * x * 2);
+    }
+}
+
+/* Interpolate, utils.h:40-58: truncating conversion, outside when rx<0, ry<0, rx+1>=w, ry+1>=h. */
+static double bilinear(const double *img, int w, int h, double x, double y, int *outside)
+{
+    int rx = (int)x, ry = (int)y;
+    if (rx < 0 || ry < 0 || rx + 1 >= w || ry + 1 >= h) {
+        *outside = 1;
+        return 0.0;
+    }
+    *outside = 0;
+    double v00 = img[w * ry + rx], v10 = img[w * ry + rx + 1];
+    double v01 = img[w * (ry + 1) + rx], v11 = img[w * (ry + 1) + rx + 1];
+    double fx = x - rx, fy = y - ry;
+    double v0 = v00 + (v10 - v00) * fx;
+    double v1 = v01 + (v11 - v01) * fx;
+    return v0 + (v1 - v0) * fy;
+}
+
+/* CPUTracker::CheckBoundaries, cpu_tracker.cpp:182-188. */
+static int check_boundaries(double cx, double cy, double radius, int w, int h)
+{
+    return cx + radius >= w || cx - radius < 0 || cy + radius >= h || cy - radius < 0;
+}
+
+/* CPUTracker::ComputeMeanAndCOM, cpu_tracker.cpp:681-729. out = {x, y, mean, stdev}. */
+ORACLE_API void oracle_com(const double *img, int w, int h, double bgcorrection, double *out)
+{
+    double sum = 0, sum2 = 0;
+    int n = w * h;
+    for (int i = 0; i < n; i++) {
+        sum += img[i];
+        sum2 += img[i] * img[i];
+    }
+    double mean = sum / n;
+    double stdev = sqrt(sum2 / n - mean * mean);
+    double s = 0, mx = 0, my = 0;
+    for (int x = 0; x < w; x++)
+        for (int y = 0; y < h; y++) {
+            double v = fabs(img[y * w + x] - mean) - bgcorrection * stdev;
+            if (v < 0) v = 0;
+            s += v;
+            mx += x * v;
+            my += y * v;
+        }
+    out[0] = mx / s;
+    out[1] = my / s;
+    out[2] = mean;
+    out[3] = stdev;
+}
+
+/* LsqSqQuadFit + ComputeMaxInterp<T,7>::Compute, LsqQuadraticFit.h:8-129,132-176.
+ * Note the reference's weight indexing: weights[0..numpoints) even when the window is
+ * clipped at the start of the array. */
+ORACLE_API double oracle_max_interp7(const double *data, int len, const double *weights)
+{
+    int iMax = 0;
+    double vMax = data[0];
+    for (int k = 1; k < len; k++)
+        if (data[k] > vMax) {
+            vMax = data[k];
+            iMax = k;
+        }
+    int startPos = iMax - 3 > 0 ? iMax - 3 : 0;
+    int endPos = iMax + 4 < len ? iMax + 4 : len;
+    int np = endPos - startPos;
+    if (np < 3) return iMax;
+    double Sx = 0, Sy = 0, Sx2 = 0, Sx3 = 0, Sx4 = 0, Sxy = 0, Sx2y = 0, Sw = 0;
+    for (int i = 0; i < np; i++) {
+        double x = (startPos + i) - iMax, y = data[startPos + i], wt = weights[i];
+        double sq = x * x;
+        Sx += x * wt;
+        Sy += y * wt;
+        Sx2 += sq * wt;
+        Sx3 += sq * x * wt;
+        Sx4 += sq * sq * wt;
+        Sxy += x * y * wt;
+        Sx2y += sq * y * wt;
+        Sw += wt;
+    }
+    double s40 = Sx4, s30 = Sx3, s20 = Sx2, s10 = Sx, s21 = Sx2y, s11 = Sxy, s01 = Sy, s00 = Sw;
+    double d = s40 * (s20 * s00 - s10 * s10) - s30 * (s30 * s00 - s10 * s20) + s20 * (s30 * s10 - s20 * s20);
+    double a = (s21 * (s20 * s00 - s10 * s10) - s11 * (s30 * s00 - s10 * s20) + s01 * (s30 * s10 - s20 * s20)) / d;
+    double b = (s40 * (s11 * s00 - s01 * s10) - s30 * (s21 * s00 - s01 * s20) + s20 * (s21 * s10 - s11 * s20)) / d;
+    if (fabs(a) < 1e-9) return iMax;
+    return iMax + (-b / (2 * a));
+}
+
+/* CPUTracker::ComputeQuadrantProfile, cpu_tracker.cpp:631-677, with the quadrant
+ * direction table of cpu_tracker.cpp:294-300 (angular_pq entries). */
+static void quadrant_profile(const double *img, int w, int h, double mean, double *dst, int nr, int angular_pq,
+                             int angsteps, int q, double minR, double maxR, double cx, double cy,
+                             const double *rweights)
+{
+    static const int qmat[8] = {1, 1, -1, 1, -1, -1, 1, -1};
+    int mx = qmat[2 * q], my = qmat[2 * q + 1];
+    if (angsteps < MIN_RADPROFILE_SMP_COUNT) angsteps = MIN_RADPROFILE_SMP_COUNT;
+    double rstep = (maxR - minR) / nr;
+    /* (int)angstepf * a: the reference truncates the stride before multiplying (cpu_tracker.cpp:655-657). */
+    int stride = (int)((double)angular_pq / angsteps);
+    for (int i = 0; i < nr; i++) {
+        double sum = 0, r = minR + rstep * i;
+        int n = 0;
+        for (int a = 0; a < angsteps; a++) {
+            int j = stride * a;
+            double ang = 0.5 * REF_PI_F * (j + 0.5) / angular_pq;
+            double x = cx + mx * cos(ang) * r, y = cy + my * sin(ang) * r;
+            int out;
+            double v = bilinear(img, w, h, x, y, &out);
+            if (!out) {
+                sum += v;
+                n++;
+            }
+        }
+        dst[i] = n >= MIN_RADPROFILE_SMP_COUNT ? sum / n : mean;
+        if (rweights) dst[i] *= rweights[i];
+    }
+}
+
+/* CPUTracker::QI_ComputeOffset, cpu_tracker.cpp:375-406: autoconvolution of the profile with
+ * its reverse (unnormalised inverse FFT, so values carry the factor L), fftshift by nr,
+ * 7-point weighted quadratic fit, (max - nr) * pi/4. */
+static double qi_offset(const double *prof, int nr)
+{
+    int L = 2 * nr;
+    double *ac = (double *)malloc(sizeof(double) * L);
+    for (int x = 0; x < L; x++) {
+        int n = (x + nr) % L;
+        double s = 0;
+        for (int m = 0; m < L; m++) s += prof[(n + m) % L] * prof[L - 1 - m];
+        ac[x] = L * s;
+    }
+    double maxPos = oracle_max_interp7(ac, L, QI_WEIGHTS);
+    free(ac);
+    return (maxPos - nr) * (3.14159265359 / 4);
+}
+
+/* CPUTracker::ComputeQI, cpu_tracker.cpp:285-360. out = {x, y, boundaryHit}. */
+ORACLE_API void oracle_qi(const double *img, int w, int h, double mean, double init_x, double init_y, int iterations,
+                          int nr, int angular_pq, double angstep_factor, double minR, double maxR,
+                          const double *rweights, double *out)
+{
+    double *q = (double *)malloc(sizeof(double) * nr * 4);
+    double *prof = (double *)malloc(sizeof(double) * nr * 2);
+    double cx = init_x, cy = init_y;
+    double pixelsPerProfLen = (maxR - minR) / nr;
+    int bhit = 0;
+    /* the reference keeps angsteps as a float (cpu_tracker.cpp:314) and truncates it per call */
+    float angsteps = angular_pq / powf((float)angstep_factor, (float)iterations);
+    for (int k = 0; k < iterations; k++) {
+        bhit = check_boundaries(cx, cy, maxR, w, h);
+        for (int qu = 0; qu < 4; qu++)
+            quadrant_profile(img, w, h, mean, q + qu * nr, nr, angular_pq, (int)angsteps, qu, minR, maxR, cx, cy,
+                             rweights);
+        double *q0 = q, *q1 = q + nr, *q2 = q + 2 * nr, *q3 = q + 3 * nr;
+        for (int r = 0; r < nr; r++) {
+            prof[nr - r - 1] = q1[r] + q2[r];
+            prof[nr + r] = q0[r] + q3[r];
+        }
+        double offX = qi_offset(prof, nr);
+        for (int r = 0; r < nr; r++) {
+            prof[nr + r] = q0[r] + q1[r];
+            prof[nr - r - 1] = q2[r] + q3[r];
+        }
+        double offY = qi_offset(prof, nr);
+        cx += offX * pixelsPerProfLen;
+        cy += offY * pixelsPerProfLen;
+        angsteps *= (float)angstep_factor;
+    }
+    out[0] = cx;
+    out[1] = cy;
+    out[2] = bhit;
+    free(q);
+    free(prof);
+}
+
+/* NormalizeRadialProfile, utils.cpp:230-261. */
+ORACLE_API void oracle_normalize_profile(double *prof, int n)
+{
+    double sum = 0;
+    for (int i = 0; i < n; i++) sum += prof[i];
+    double mean = sum / n, rms2 = 0;
+    for (int i = 0; i < n; i++) {
+        prof[i] -= mean;
+        rms2 += prof[i] * prof[i];
+    }
+    double inv = 1.0 / sqrt(rms2 / n);
+    for (int i = 0; i < n; i++) prof[i] *= inv;
+}
+
+/* ComputeRadialProfile, utils.cpp:275-320: full-circle directions 2*pi*j/angsteps, more than
+ * MIN_RADPROFILE_SMP_COUNT in-bounds samples or the fallback value `mean`. */
+ORACLE_API void oracle_radial_profile(const double *img, int w, int h, double mean, double cx, double cy, int nbins,
+                                      int angsteps, double minR, double maxR, int normalize, double *dst)
+{
+    double rstep = (maxR - minR) / nbins;
+    for (int i = 0; i < nbins; i++) {
+        double sum = 0, r = minR + rstep * i;
+        int n = 0;
+        for (int a = 0; a < angsteps; a++) {
+            double ang = 2 * REF_PI_F * a / angsteps;
+            int out;
+            double v = bilinear(img, w, h, cx + cos(ang) * r, cy + sin(ang) * r, &out);
+            if (!out) {
+                sum += v;
+                n++;
+            }
+        }
+        dst[i] = n > MIN_RADPROFILE_SMP_COUNT ? sum / n : mean;
+    }
+    if (normalize) oracle_normalize_profile(dst, nbins);
+}
+
+/* CPUTracker::LUTProfileCompare, cpu_tracker.cpp:791-868 (LUTProfMaxQuadraticFit):
+ * score_k = -sum_r (w_r (p_r - L_kr))^2, then the 7-point fit over planes. */
+ORACLE_API double oracle_lut_compare(const double *prof, const float *lut, int planes, int nbins,
+                                     const double *weights, double *scores)
+{
+    double *s = scores ? scores : (double *)malloc(sizeof(double) * planes);
+    for (int k = 0; k < planes; k++) {
+        double acc = 0;
+        for (int r = 0; r < nbins; r++) {
+            double d = prof[r] - (double)lut[k * nbins + r];
+            if (weights) d *= weights[r];
+            acc -= d * d;
+        }
+        s[k] = acc;
+    }
+    double z = oracle_max_interp7(s, planes, ZLUT_WEIGHTS);
+    if (!scores) free(s);
+    return z;
+}
+
+/* erf<T>, utils.h:395-417: Abramowitz & Stegun 7.1.26, evaluated in double. */
+ORACLE_API double oracle_erf_as(double x)
+{
+    const double a1 = 0.254829592, a2 = -0.284496736, a3 = 1.421413741, a4 = -1.453152027, a5 = 1.061405429,
+                 p = 0.3275911;
+    int sign = x < 0 ? -1 : 1;
+    x = fabs(x);
+    double t = 1.0 / (1.0 + p * x);
+    double y = 1.0 - (((((a5 * t + a4) * t) + a3) * t + a2) * t + a1) * t * exp(-x * x);
+    return sign * y;
+}
+
+/* CPUTracker::Compute2DGaussianMLE, cpu_tracker.cpp:514-589: 4 parameters (x, y, I0, bg),
+ * fixed sigma, per-parameter (diagonal) Newton steps. out = {x, y, I0, bg}. */
+ORACLE_API void oracle_gauss2d(const double *img, int w, int h, double mean, double init_x, double init_y,
+                               int iterations, double sigma, double *out)
+{
+    double px = init_x, py = init_y, I0 = mean * 0.5 * w * h, bg = mean * 0.5;
+    const double k1 = 1.0 / (sqrt(2.0) * sigma);
+    const double k2 = 1.0 / (sqrt(2 * 3.14159265359) * sigma);
+    const double k3 = 1.0 / (sqrt(2 * 3.14159265359) * sigma * sigma * sigma);
+    for (int it = 0; it < iterations; it++) {
+        double dx = 0, dy = 0, dI = 0, dB = 0, ddx = 0, ddy = 0, ddI = 0, ddB = 0;
+        for (int y = 0; y < h; y++)
+            for (int x = 0; x < w; x++) {
+                double X0 = (x - px + .5) * k1, Y0 = (y - py + .5) * k1;
+                double X1 = (x - px - .5) * k1, Y1 = (y - py - .5) * k1;
+                double DX = 0.5 * oracle_erf_as(X0) - 0.5 * oracle_erf_as(X1);
+                double DY = 0.5 * oracle_erf_as(Y0) - 0.5 * oracle_erf_as(Y1);
+                double mu = bg + I0 * DX * DY;
+                double dmx = I0 * k2 * (exp(-X1 * X1) - exp(-X0 * X0)) * DY;
+                double dmy = I0 * k2 * (exp(-Y1 * Y1) - exp(-Y0 * Y0)) * DX;
+                double dmI = DX * DY;
+                double smp = img[y * w + x];
+                double f = smp / mu - 1;
+                dx += dmx * f;
+                dy += dmy * f;
+                dI += dmI * f;
+                dB += f;
+                double d2x = I0 * k3 * ((x - px - .5) * exp(-X1 * X1) - (x - px + .5) * exp(-X0 * X0)) * DY;
+                double d2y = I0 * k3 * ((y - py - .5) * exp(-Y1 * Y1) - (y - py + .5) * exp(-Y0 * Y0)) * DX;
+                ddx += d2x * f - dmx * dmx * smp / (mu * mu);
+                ddy += d2y * f - dmy * dmy * smp / (mu * mu);
+                ddI += -dmI * dmI * smp / (mu * mu);
+                ddB += -smp / (mu * mu);
+            }
+        px -= dx / ddx;
+        py -= dy / ddy;
+        I0 -= dI / ddI;
+        bg -= dB / ddB;
+    }
+    out[0] = px;
+    out[1] = py;
+    out[2] = I0;
+    out[3] = bg;
+}
+
+/*
+ * One ROI through QueuedCPUTracker::ProcessJob, QueuedCPUTracker.cpp:273-361, for the modes in
+ * scope (COM, QI, Gaussian2D, LocalizeZ, NormalizeProfile, ClearFirstFourPixels).
+ * img: W*H pixels already converted to double (SetImage, cpu_tracker.h:123-134), after the
+ * per-bead offset/gain step. lut: this ROI's bead LUT [planes][zlut_radialsteps] or NULL.
+ * out = {x, y, z, com_x, com_y, error, imageMean}.
+ */
+ORACLE_API void oracle_localize(const oracle_config *c, int mode, double *img, const float *lut, int planes,
+                                const double *zweights, double *out)
+{
+    int w = c->width, h = c->height;
+    if (mode & LT_ClearFirstFourPixels) img[0] = img[1] = img[2] = img[3] = 0;
+    double com[4];
+    oracle_com(img, w, h, c->com_bgcorrection, com);
+    double mean = com[2];
+    if (isnan(com[0]) || isnan(com[1])) {
+        com[0] = w / 2;
+        com[1] = h / 2;
+    }
+    double x = com[0], y = com[1], z = 0;
+    int bhit = 0;
+    if (mode & LT_QI) {
+        double *rw = (double *)malloc(sizeof(double) * c->qi_radialsteps);
+        oracle_radial_bin_window(c->qi_radialsteps, rw);
+        double q[3];
+        oracle_qi(img, w, h, mean, com[0], com[1], c->qi_iterations, c->qi_radialsteps, c->qi_angstepspq,
+                  c->qi_angstep_factor, c->qi_minradius, c->qi_maxradius, rw, q);
+        x = q[0];
+        y = q[1];
+        bhit = (int)q[2];
+        free(rw);
+    } else if (mode & LT_Gaussian2D) {
+        double g[4];
+        oracle_gauss2d(img, w, h, mean, com[0], com[1], c->gauss2D_iterations, c->gauss2D_sigma, g);
+        x = g[0];
+        y = g[1];
+    }
+    if (mode & LT_LocalizeZ) {
+        int nb = c->zlut_radialsteps;
+        double *prof = (double *)malloc(sizeof(double) * nb);
+        bhit = check_boundaries(x, y, c->zlut_maxradius, w, h);
+        oracle_radial_profile(img, w, h, mean, x, y, nb, c->zlut_angularsteps, c->zlut_minradius, c->zlut_maxradius,
+                              (mode & LT_NormalizeProfile) != 0, prof);
+        z = lut ? oracle_lut_compare(prof, lut, planes, nb, zweights, 0) : 0.0;
+        free(prof);
+    }
+    out[0] = x;
+    out[1] = y;
+    out[2] = z;
+    out[3] = com[0];
+    out[4] = com[1];
+    out[5] = bhit;
+    out[6] = mean;
+}
+
+/*
+ * One bead of QueuedCPUTracker::BuildLUT, QueuedCPUTracker.cpp:580-646: position from
+ * known_pos, or COM (no background correction) + QI without radial weights (line 603);
+ * the radial profile (normalised iff BUILDLUT_NORMALIZE) uses the tracker's mean as the
+ * fallback, which is 0 when known_pos skips ComputeMeanAndCOM (SetImage resets it,
+ * cpu_tracker.h:135). The profile is added to lut_row.
+ */
+ORACLE_API void oracle_build_lut_bead(const oracle_config *c, const double *img, int has_known, double kx, double ky,
+                                      int normalize, double *lut_row)
+{
+    int w = c->width, h = c->height;
+    double x = kx, y = ky, mean = 0;
+    if (!has_known) {
+        double com[4], q[3];
+        oracle_com(img, w, h, 0.0, com);
+        mean = com[2];
+        oracle_qi(img, w, h, mean, com[0], com[1], c->qi_iterations, c->qi_radialsteps, c->qi_angstepspq,
+                  c->qi_angstep_factor, c->qi_minradius, c->qi_maxradius, 0, q);
+        x = q[0];
+        y = q[1];
+    }
+    int nb = c->zlut_radialsteps;
+    double *prof = (double *)malloc(sizeof(double) * nb);
+    oracle_radial_profile(img, w, h, mean, x, y, nb, c->zlut_angularsteps, c->zlut_minradius, c->zlut_maxradius,
+                          normalize, prof);
+    for (int i = 0; i < nb; i++) lut_row[i] += prof[i];
+    free(prof);
+}
+
+/* ======================= extensions (no reference counterpart) ======================= */
+
+/* Integrated-Gaussian pixel model of utils.cpp:393-402 with exact erf; used by the
+ * 5-parameter MLE below. */
+static void gauss_pixel(double x, double y, double px, double py, double s, double *D, double *dDx, double *dDs,
+                        int axis_is_y)
+{
+    (void)axis_is_y;
+    (void)y;
+    double a0 = (x - px + 0.5) / (sqrt(2.0) * s), a1 = (x - px - 0.5) / (sqrt(2.0) * s);
+    *D = 0.5 * (erf(a0) - erf(a1));
+    double g0 = exp(-a0 * a0), g1 = exp(-a1 * a1);
+    /* d/dpx of D */
+    *dDx = (g1 - g0) / (sqrt(2 * M_PI) * s);
+    /* d/ds of D */
+    *dDs = -((x - px + 0.5) * g0 - (x - px - 0.5) * g1) / (sqrt(2 * M_PI) * s * s);
+}
+
+/* Solve the 5x5 system A d = b by Gaussian elimination with partial pivoting; returns 0 if singular. */
+static int solve5(double A[5][5], double b[5], double d[5])
+{
+    double M[5][6];
+    for (int i = 0; i < 5; i++) {
+        for (int j = 0; j < 5; j++) M[i][j] = A[i][j];
+        M[i][5] = b[i];
+    }
+    for (int c = 0; c < 5; c++) {
+        int p = c;
+        for (int r = c + 1; r < 5; r++)
+            if (fabs(M[r][c]) > fabs(M[p][c])) p = r;
+        if (fabs(M[p][c]) < 1e-300) return 0;
+        if (p != c)
+            for (int j = 0; j < 6; j++) {
+                double t = M[c][j];
+                M[c][j] = M[p][j];
+                M[p][j] = t;
+            }
+        for (int r = c + 1; r < 5; r++) {
+            double f = M[r][c] / M[c][c];
+            for (int j = c; j < 6; j++) M[r][j] -= f * M[c][j];
+        }
+    }
+    for (int i = 4; i >= 0; i--) {
+        double s = M[i][5];
+        for (int j = i + 1; j < 5; j++) s -= M[i][j] * d[j];
+        d[i] = s / M[i][i];
+    }
+    return 1;
+}
+
+/*
+ * 5-parameter Poisson MLE of an integrated Gaussian spot (x, y, I0, bg, sigma) with full
+ * Newton steps (Fisher-scoring Hessian, i.e. the expected Hessian sum_i (dmu/dp)(dmu/dq)/mu),
+ * a 5x5 FP64 solve per step, and parameter clamping (I0, bg > 0; 0.3 < sigma < W/2).
+ * init = {x, y, I0, bg, sigma}; out = same order; fisher (may be NULL) = 5x5 Fisher matrix at
+ * the solution, whose inverse diagonal is the Cramer-Rao bound.
+ */
+ORACLE_API void oracle_gauss5(const double *img, int w, int h, const double *init, int iterations, double *out,
+                              double *fisher)
+{
+    double p[5];
+    for (int i = 0; i < 5; i++) p[i] = init[i];
+    for (int it = 0; it <= iterations; it++) {
+        double H[5][5] = {{0}}, g[5] = {0};
+        for (int y = 0; y < h; y++) {
+            double DY, dDy, dDsy;
+            gauss_pixel(y, 0, p[1], 0, p[4], &DY, &dDy, &dDsy, 1);
+            for (int x = 0; x < w; x++) {
+                double DX, dDx, dDsx;
+                gauss_pixel(x, 0, p[0], 0, p[4], &DX, &dDx, &dDsx, 0);
+                double mu = p[3] + p[2] * DX * DY;
+                double j[5] = {p[2] * dDx * DY, p[2] * DX * dDy, DX * DY, 1.0, p[2] * (dDsx * DY + DX * dDsy)};
+                double f = img[y * w + x] / mu - 1.0;
+                for (int a = 0; a < 5; a++) {
+                    g[a] += j[a] * f;
+                    for (int b = 0; b < 5; b++) H[a][b] += j[a] * j[b] / mu;
+                }
+            }
+        }
+        if (it == iterations) {
+            if (fisher)
+                for (int a = 0; a < 5; a++)
+                    for (int b = 0; b < 5; b++) fisher[a * 5 + b] = H[a][b];
+            break;
+        }
+        double d[5];
+        if (!solve5(H, g, d)) break;
+        for (int a = 0; a < 5; a++) p[a] += d[a];
+        if (p[2] < 1e-3) p[2] = 1e-3;
+        if (p[3] < 1e-3) p[3] = 1e-3;
+        if (p[4] < 0.3) p[4] = 0.3;
+        if (p[4] > w * 0.5) p[4] = w * 0.5;
+    }
+    for (int i = 0; i < 5; i++) out[i] = p[i];
+}
+
+/*
+ * Radial-profile-to-LUT cost and its analytic gradient (the adjoint of the GPU library).
+ * cost(x, y, z, L) = sum_r (w_r (p_r(x, y) - Lz_r))^2 where p is the (unnormalised) radial
+ * profile of utils.cpp:275-320 at (x, y) and Lz is the LUT linearly interpolated between
+ * planes floor(z) and floor(z)+1 (clamped to the table). grad = {dx, dy, dz};
+ * glut (planes*nbins, may be NULL) receives d cost / d L.
+ */
+ORACLE_API double oracle_zcost_grad(const double *img, int w, int h, double mean, double x, double y, double z,
+                                    const float *lut, int planes, int nbins, int angsteps, double minR, double maxR,
+                                    const double *weights, double *grad, double *glut)
+{
+    double rstep = (maxR - minR) / nbins;
+    int iz = (int)floor(z);
+    if (iz < 0) iz = 0;
+    if (iz > planes - 2) iz = planes - 2;
+    double fz = z - iz;
+    double cost = 0, gx = 0, gy = 0, gz = 0;
+    if (glut) memset(glut, 0, sizeof(double) * planes * nbins);
+    for (int i = 0; i < nbins; i++) {
+        double r = minR + rstep * i, sum = 0, sx = 0, sy = 0;
+        int n = 0;
+        for (int a = 0; a < angsteps; a++) {
+            double ang = 2 * REF_PI_F * a / angsteps, ca = cos(ang), sa = sin(ang);
+            double px = x + ca * r, py = y + sa * r;
+            int rx = (int)px, ry = (int)py;
+            if (rx < 0 || ry < 0 || rx + 1 >= w || ry + 1 >= h) continue;
+            double v00 = img[w * ry + rx], v10 = img[w * ry + rx + 1];
+            double v01 = img[w * (ry + 1) + rx], v11 = img[w * (ry + 1) + rx + 1];
+            double fx = px - rx, fy = py - ry;
+            double v0 = v00 + (v10 - v00) * fx, v1 = v01 + (v11 - v01) * fx;
+            sum += v0 + (v1 - v0) * fy;
+            sx += (v10 - v00) * (1 - fy) + (v11 - v01) * fy;
+            sy += v1 - v0;
+            n++;
+        }
+        double p, dpx = 0, dpy = 0;
+        if (n > MIN_RADPROFILE_SMP_COUNT) {
+            p = sum / n;
+            dpx = sx / n;
+            dpy = sy / n;
+        } else
+            p = mean;
+        double l0 = lut[iz * nbins + i], l1 = lut[(iz + 1) * nbins + i];
+        double lz = l0 + (l1 - l0) * fz;
+        double wr = weights ? weights[i] : 1.0;
+        double e = wr * (p - lz);
+        cost += e * e;
+        double de = 2 * e * wr;
+        gx += de * dpx;
+        gy += de * dpy;
+        gz += -de * (l1 - l0);
+        if (glut) {
+            glut[iz * nbins + i] += -de * (1 - fz);
+            glut[(iz + 1) * nbins + i] += -de * fz;
+        }
+    }
+    grad[0] = gx;
+    grad[1] = gy;
+    grad[2] = gz;
+    return cost;
+}
+
+/*
+ * Joint Gauss-Newton refinement of (x, y, z) on the cost above: J^T J from the per-bin
+ * residual Jacobian, a 3x3 solve per step with a Levenberg damping of 1e-9*trace, `steps`
+ * steps, z clamped to [0, planes-1]. io = {x, y, z} in, refined out.
+ */
+ORACLE_API void oracle_joint_refine(const double *img, int w, int h, double mean, double *io, const float *lut,
+                                    int planes, int nbins, int angsteps, double minR, double maxR,
+                                    const double *weights, int steps)
+{
+    double rstep = (maxR - minR) / nbins;
+    for (int s = 0; s < steps; s++) {
+        double x = io[0], y = io[1], z = io[2];
+        int iz = (int)floor(z);
+        if (iz < 0) iz = 0;
+        if (iz > planes - 2) iz = planes - 2;
+        double fz = z - iz;
+        double A[3][3] = {{0}}, g[3] = {0};
+        for (int i = 0; i < nbins; i++) {
+            double r = minR + rstep * i, sum = 0, sx = 0, sy = 0;
+            int n = 0;
+            for (int a = 0; a < angsteps; a++) {
+                double ang = 2 * REF_PI_F * a / angsteps;
+                double px = x + cos(ang) * r, py = y + sin(ang) * r;
+                int rx = (int)px, ry = (int)py;
+                if (rx < 0 || ry < 0 || rx + 1 >= w || ry + 1 >= h) continue;
+                double v00 = img[w * ry + rx], v10 = img[w * ry + rx + 1];
+                double v01 = img[w * (ry + 1) + rx], v11 = img[w * (ry + 1) + rx + 1];
+                double fx = px - rx, fy = py - ry;
+                double v0 = v00 + (v10 - v00) * fx, v1 = v01 + (v11 - v01) * fx;
+                sum += v0 + (v1 - v0) * fy;
+                sx += (v10 - v00) * (1 - fy) + (v11 - v01) * fy;
+                sy += v1 - v0;
+                n++;
+            }
+            double p, J[3] = {0, 0, 0};
+            double l0 = lut[iz * nbins + i], l1 = lut[(iz + 1) * nbins + i];
+            if (n > MIN_RADPROFILE_SMP_COUNT) {
+                p = sum / n;
+                J[0] = sx / n;
+                J[1] = sy / n;
+            } else
+                p = mean;
+            J[2] = -(l1 - l0);
+            double wr = weights ? weights[i] : 1.0;
+            double e = wr * (p - (l0 + (l1 - l0) * fz));
+            for (int a = 0; a < 3; a++) {
+                g[a] += wr * J[a] * e;
+                for (int b = 0; b < 3; b++) A[a][b] += wr * wr * J[a] * J[b];
+            }
+        }
+        double tr = A[0][0] + A[1][1] + A[2][2];
+        for (int a = 0; a < 3; a++) A[a][a] += 1e-9 * tr + 1e-30;
+        /* solve A d = -g by Cramer's rule */
+        double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) -
+                     A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+                     A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+        if (det == 0) break;
+        double d[3];
+        for (int c = 0; c < 3; c++) {
+            double M[3][3];
+            for (int i = 0; i < 3; i++)
+                for (int j = 0; j < 3; j++) M[i][j] = (j == c) ? -g[i] : A[i][j];
+            d[c] = (M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) - M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
+                    M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0])) /
+                   det;
+        }
+        io[0] = x + d[0];
+        io[1] = y + d[1];
+        io[2] = z + d[2];
+        if (io[2] < 0) io[2] = 0;
+        if (io[2] > planes - 1) io[2] = planes - 1;
+    }
+}

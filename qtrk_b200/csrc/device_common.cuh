@@ -1,0 +1,676 @@
+// Device building blocks of the localization kernels (sm_100a).
+//
+// Each function restates one step of the reference CPU tracker for one ROI held in
+// shared memory by one CTA; the reference file:line each follows is given beside it.
+// Thread mappings are chosen for the GPU (one (quadrant, radius) bin per thread or
+// per aligned lane group, warp-shuffle reductions, one warp for the QI FFTs); the
+// discrete decisions (int truncation, the bilinear "outside" rule, sample-count
+// thresholds, the argmax window of the quadratic fit) are those of the reference.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "track_params.h"
+
+namespace qtrk {
+
+// -------------------------------------------------------------------------------------
+// small helpers
+// -------------------------------------------------------------------------------------
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+{
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+__device__ __forceinline__ int ilog2_pow2(int v) { return 31 - __clz(v); }
+
+__device__ __forceinline__ unsigned bitrev(unsigned v, int bits) { return __brev(v) >> (32 - bits); }
+
+// Sum N doubles over the whole CTA; every thread receives the totals.
+// red: shared scratch of at least N * (blockDim.x / 32) doubles (256 doubles cover N <= 32
+// at 256 threads).
+template <int N>
+__device__ __forceinline__ void block_sum(double (&v)[N], double *red)
+{
+#pragma unroll
+    for (int k = 0; k < N; k++)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < N; k++) red[k * nw + warp] = v[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        double s = 0;
+        for (int w = 0; w < nw; w++) s += red[k * nw + w];
+        v[k] = s;
+    }
+}
+
+// Thread groups that process one ROI: the whole CTA, or one warp (small-ROI kernels).
+struct BlockGroup {
+    double *red;  // >= N*32 doubles of shared scratch for sum<N>
+    __device__ __forceinline__ int rank() const { return threadIdx.x; }
+    __device__ __forceinline__ int size() const { return blockDim.x; }
+    __device__ __forceinline__ void sync() const { __syncthreads(); }
+    template <int N>
+    __device__ __forceinline__ void sum(double (&v)[N]) const { block_sum<N>(v, red); }
+};
+
+struct WarpGroup {
+    __device__ __forceinline__ int rank() const { return threadIdx.x & 31; }
+    __device__ __forceinline__ int size() const { return 32; }
+    __device__ __forceinline__ void sync() const { __syncwarp(); }
+    template <int N>
+    __device__ __forceinline__ void sum(double (&v)[N]) const
+    {
+#pragma unroll
+        for (int k = 0; k < N; k++)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    }
+};
+
+// Interpolate, utils.h:40-58: truncating float->int conversion; the sample is outside when
+// rx < 0, ry < 0, rx+1 >= w or ry+1 >= h. Returns false when outside.
+__device__ __forceinline__ bool bilinear(const float *img, int w, int h, float x, float y, float &v)
+{
+    const int rx = __float2int_rz(x), ry = __float2int_rz(y);
+    if ((unsigned)rx >= (unsigned)(w - 1) || (unsigned)ry >= (unsigned)(h - 1)) return false;
+    const float *p = img + ry * w + rx;
+    const float v00 = p[0], v10 = p[1], v01 = p[w], v11 = p[w + 1];
+    const float fx = x - (float)rx, fy = y - (float)ry;
+    const float v0 = v00 + (v10 - v00) * fx;
+    const float v1 = v01 + (v11 - v01) * fx;
+    v = v0 + (v1 - v0) * fy;
+    return true;
+}
+
+// CPUTracker::CheckBoundaries, cpu_tracker.cpp:182-188
+__device__ __forceinline__ bool check_boundaries(float cx, float cy, float radius, int w, int h)
+{
+    return cx + radius >= w || cx - radius < 0 || cy + radius >= h || cy - radius < 0;
+}
+
+// LsqSqQuadFit + ComputeMaxInterp<T,7>::Compute, LsqQuadraticFit.h:8-176, evaluated in FP64.
+// `at(i)` returns element i of the length-`len` array; iMax is the first index of the maximum.
+// The weights are indexed from 0 even when the window is clipped at the array start, as in
+// the reference.
+template <typename Get>
+__device__ double max_interp7(Get at, int len, int iMax, const float (&wts)[7])
+{
+    const int startPos = max(iMax - 3, 0);
+    const int endPos = min(iMax + 4, len);
+    const int np = endPos - startPos;
+    if (np < 3) return (double)iMax;
+    double Sx = 0, Sy = 0, Sx2 = 0, Sx3 = 0, Sx4 = 0, Sxy = 0, Sx2y = 0, Sw = 0;
+    for (int i = 0; i < np; i++) {
+        const double x = (double)(startPos + i - iMax), y = (double)at(startPos + i), wt = (double)wts[i];
+        const double sq = x * x;
+        Sx += x * wt;
+        Sy += y * wt;
+        Sx2 += sq * wt;
+        Sx3 += sq * x * wt;
+        Sx4 += sq * sq * wt;
+        Sxy += x * y * wt;
+        Sx2y += sq * y * wt;
+        Sw += wt;
+    }
+    const double d = Sx4 * (Sx2 * Sw - Sx * Sx) - Sx3 * (Sx3 * Sw - Sx * Sx2) + Sx2 * (Sx3 * Sx - Sx2 * Sx2);
+    const double a = (Sx2y * (Sx2 * Sw - Sx * Sx) - Sxy * (Sx3 * Sw - Sx * Sx2) + Sy * (Sx3 * Sx - Sx2 * Sx2)) / d;
+    const double b = (Sx4 * (Sxy * Sw - Sy * Sx) - Sx3 * (Sx2y * Sw - Sy * Sx2) + Sx2 * (Sx2y * Sx - Sxy * Sx2)) / d;
+    if (fabs(a) < 1e-9) return (double)iMax;
+    return (double)iMax - b / (2 * a);
+}
+
+// First index of the maximum of at(0..len), reduced over one warp (all 32 lanes call).
+// Matches the strict ">" scan of LsqQuadraticFit.h:140-147 (NaN values never win).
+template <typename Get>
+__device__ __forceinline__ int warp_argmax(Get at, int len)
+{
+    using T = decltype(at(0));
+    const int lane = threadIdx.x & 31;
+    T best = 0;
+    int bi = -1;
+    for (int i = lane; i < len; i += 32) {
+        const T v = at(i);
+        if (v == v && (bi < 0 || v > best)) {
+            best = v;
+            bi = i;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const T ov = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (oi >= 0 && (bi < 0 || ov > best || (ov == best && oi < bi))) {
+            best = ov;
+            bi = oi;
+        }
+    }
+    return bi < 0 ? 0 : bi;
+}
+
+// -------------------------------------------------------------------------------------
+// ROI load: u8/u16/f32 -> f32 tile in shared memory, with the clear-first-four-pixels
+// option (QueuedCPUTracker.cpp:280-282) and the per-bead offset/gain step
+// (cpu_tracker.cpp:98-112) fused into the same pass.
+// -------------------------------------------------------------------------------------
+__device__ __forceinline__ float finish_pixel(float v, int i, const TrackParams &P, const float *off,
+                                              const float *gain)
+{
+    if ((P.mode & kLT_ClearFirstFourPixels) && i < 4) v = 0.0f;
+    if (off && !gain) v = v + off[i] * P.offset_factor;
+    if (gain && !off) v = v * gain[i] * P.gain_factor;
+    if (gain && off) v = (v + off[i] * P.offset_factor) * gain[i] * P.gain_factor;
+    return v;
+}
+
+template <class G>
+__device__ void load_roi(const G &g, float *img, const uint8_t *src, int pitch, const TrackParams &P, int bead)
+{
+    const int W = P.width, H = P.height, n = W * H;
+    const int bpp = P.pdt == 0 ? 1 : (P.pdt == 1 ? 2 : 4);
+    const float *off = nullptr, *gain = nullptr;
+    if (bead >= 0 && bead < P.calib_count) {
+        if (P.calib_offset) off = P.calib_offset + (size_t)bead * n;
+        if (P.calib_gain) gain = P.calib_gain + (size_t)bead * n;
+    }
+    const bool contiguous = pitch == W * bpp && ((reinterpret_cast<uintptr_t>(src) & 15) == 0) && ((n * bpp) & 15) == 0;
+    if (contiguous) {
+        // 128-bit streaming loads over the whole ROI (rows are back to back).
+        const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
+        const int nv = (n * bpp) >> 4;
+        for (int v = g.rank(); v < nv; v += g.size()) {
+            const uint4 q = __ldcs(s4 + v);
+            const uint32_t w4[4] = {q.x, q.y, q.z, q.w};
+            if (P.pdt == 0) {
+                const int base = v * 16;
+#pragma unroll
+                for (int j = 0; j < 16; j++)
+                    img[base + j] = finish_pixel((float)((w4[j >> 2] >> ((j & 3) * 8)) & 0xffu), base + j, P, off, gain);
+            } else if (P.pdt == 1) {
+                const int base = v * 8;
+#pragma unroll
+                for (int j = 0; j < 8; j++)
+                    img[base + j] = finish_pixel((float)((w4[j >> 1] >> ((j & 1) * 16)) & 0xffffu), base + j, P, off, gain);
+            } else {
+                const int base = v * 4;
+#pragma unroll
+                for (int j = 0; j < 4; j++) img[base + j] = finish_pixel(__uint_as_float(w4[j]), base + j, P, off, gain);
+            }
+        }
+    } else {
+        for (int i = g.rank(); i < n; i += g.size()) {
+            const int y = i / W, x = i - y * W;
+            const uint8_t *p = src + (size_t)y * pitch + (size_t)x * bpp;
+            float v;
+            if (P.pdt == 0)
+                v = (float)(*p);
+            else if (P.pdt == 1)
+                v = (float)(*reinterpret_cast<const uint16_t *>(p));
+            else
+                v = *reinterpret_cast<const float *>(p);
+            img[i] = finish_pixel(v, i, P, off, gain);
+        }
+    }
+    g.sync();
+}
+
+// -------------------------------------------------------------------------------------
+// CPUTracker::ComputeMeanAndCOM, cpu_tracker.cpp:681-729 (FP64 accumulation as in the
+// reference; mean and stdev rounded to float where the reference stores floats).
+// -------------------------------------------------------------------------------------
+struct ComResult {
+    float x, y, mean, stdev;
+};
+
+template <class G>
+__device__ ComResult compute_com(const G &g, const float *img, int W, int H, float bgcorr)
+{
+    const int n = W * H;
+    double s[2] = {0, 0};
+    for (int i = g.rank(); i < n; i += g.size()) {
+        const float v = img[i];
+        s[0] += v;
+        s[1] += (double)(v * v);
+    }
+    g.sum(s);
+    const float invN = 1.0f / (float)n;
+    ComResult r;
+    r.mean = (float)(s[0] * (double)invN);
+    r.stdev = sqrtf((float)(s[1] * (double)invN - (double)(r.mean * r.mean)));
+    double m[3] = {0, 0, 0};
+    const float thr = bgcorr * r.stdev;
+    for (int i = g.rank(); i < n; i += g.size()) {
+        const int y = i / W, x = i - y * W;
+        const float v = fmaxf(0.0f, fabsf(img[i] - r.mean) - thr);
+        m[0] += v;
+        m[1] += x * (double)v;
+        m[2] += y * (double)v;
+    }
+    g.sum(m);
+    r.x = (float)(m[1] / m[0]);
+    r.y = (float)(m[2] / m[0]);
+    return r;
+}
+
+// Lanes per radial/quadrant bin: the largest power of two with nbins*lanes <= threads, <= 32.
+__device__ __forceinline__ int lanes_per_bin(int nbins)
+{
+    int t = blockDim.x / nbins;
+    if (t < 1) return 1;
+    if (t > 32) t = 32;
+    return 1 << (31 - __clz(t));
+}
+
+// -------------------------------------------------------------------------------------
+// CPUTracker::ComputeQuadrantProfile, cpu_tracker.cpp:631-677, for all four quadrants at
+// once. qprof[q*nr + i] = mean of the in-bounds bilinear samples on the quarter arc of
+// radius minr + rstep*i (the image mean when fewer than 4 are in bounds), times the
+// radial weight. Directions come from the quadrant table at stride `stride`.
+// -------------------------------------------------------------------------------------
+__device__ void qi_quadrant_profiles(const float *img, int W, int H, float cx, float cy, float mean, int nr, int nang,
+                                     int stride, float minr, float rstep, const float2 *dirs, const float *rweights,
+                                     float *qprof)
+{
+    const int nbins = 4 * nr;
+    const int tpb = lanes_per_bin(nbins);
+    const int total = nbins * tpb;
+    for (int base = 0; base < total; base += blockDim.x) {
+        const int t = base + threadIdx.x;
+        const int bin = t / tpb, sub = t - bin * tpb;
+        float sum = 0.0f;
+        int cnt = 0;
+        int i = 0;
+        if (bin < nbins) {
+            const int q = bin / nr;
+            i = bin - q * nr;
+            const float r = minr + rstep * (float)i;
+            // quadrant signs (cpu_tracker.cpp:634-640): q0 (+,+), q1 (-,+), q2 (-,-), q3 (+,-)
+            const float sx = (q == 0 || q == 3) ? r : -r;
+            const float sy = (q < 2) ? r : -r;
+            for (int a = sub; a < nang; a += tpb) {
+                const float2 d = dirs[stride * a];
+                float v;
+                if (bilinear(img, W, H, cx + d.x * sx, cy + d.y * sy, v)) {
+                    sum += v;
+                    cnt++;
+                }
+            }
+        }
+        for (int o = tpb >> 1; o > 0; o >>= 1) {
+            sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        }
+        if (bin < nbins && sub == 0) {
+            float v = cnt >= 4 ? sum / (float)cnt : mean;
+            if (rweights) v *= rweights[i];
+            qprof[bin] = v;
+        }
+    }
+}
+
+// Radix-2 decimation-in-time FFT of length L (power of two, input in bit-reversed order),
+// executed by one warp over shared memory. tw[k] = e^{-2 pi i k / L}, k < L/2.
+__device__ void warp_fft(float2 *buf, int L, int log2L, const float2 *tw, bool inverse)
+{
+    const int lane = threadIdx.x & 31;
+    for (int s = 1; s <= log2L; s++) {
+        const int half = 1 << (s - 1), tstep = L >> s;
+        for (int j = lane; j < (L >> 1); j += 32) {
+            const int grp = j >> (s - 1), pos = j & (half - 1);
+            const int i0 = (grp << s) + pos, i1 = i0 + half;
+            float2 w = tw[pos * tstep];
+            if (inverse) w.y = -w.y;
+            const float2 a = buf[i0], b = cmul(buf[i1], w);
+            buf[i0] = make_float2(a.x + b.x, a.y + b.y);
+            buf[i1] = make_float2(a.x - b.x, a.y - b.y);
+        }
+        __syncwarp();
+    }
+}
+
+// Profile value n (0 <= n < 2nr) of the X (k=0) or Y (k=1) concatenated QI profile,
+// cpu_tracker.cpp:327-343: X = [ (q1+q2) reversed | q0+q3 ], Y = [ (q2+q3) reversed | q0+q1 ].
+__device__ __forceinline__ float2 qi_concat(const float *qprof, int nr, int n)
+{
+    const float *q0 = qprof, *q1 = qprof + nr, *q2 = qprof + 2 * nr, *q3 = qprof + 3 * nr;
+    if (n < nr) {
+        const int r = nr - 1 - n;
+        return make_float2(q1[r] + q2[r], q2[r] + q3[r]);
+    }
+    const int r = n - nr;
+    return make_float2(q0[r] + q3[r], q0[r] + q1[r]);
+}
+
+// The unnormalised correlation of each concatenated profile p with its reverse, as
+// produced by CPUTracker::QI_ComputeOffset (cpu_tracker.cpp:375-401):
+//   out[n] = L * sum_m p[(n+m) mod L] * p[L-1-m].
+// Both axes are packed into one complex signal z = px + i py. Because
+// FFT(reverse(p))* = e^{-2 pi i k/L} FFT(p) for real p, the product the reference forms
+// from two forward FFTs equals e^{-2 pi i k/L} P[k]^2, so one forward and one inverse
+// FFT per iteration give both axes. Result: ac[n] = (out_x[n], out_y[n]). Warp 0 only.
+__device__ void qi_autoconv_fft(const float *qprof, int nr, float2 *A, float2 *ac, const float2 *tw)
+{
+    const int lane = threadIdx.x & 31;
+    const int L = 2 * nr, log2L = ilog2_pow2(L);
+    for (int n = lane; n < L; n += 32) A[bitrev(n, log2L)] = qi_concat(qprof, nr, n);
+    __syncwarp();
+    warp_fft(A, L, log2L, tw, false);
+    for (int k = lane; k < L; k += 32) {
+        const float2 Zk = A[k];
+        const float2 Zc = A[(L - k) & (L - 1)];
+        // split the packed transform: Px = (Z[k] + conj Z[L-k]) / 2, Py = (Z[k] - conj Z[L-k]) / 2i
+        const float2 Px = make_float2(0.5f * (Zk.x + Zc.x), 0.5f * (Zk.y - Zc.y));
+        const float2 Py = make_float2(0.5f * (Zk.y + Zc.y), -0.5f * (Zk.x - Zc.x));
+        float2 e = tw[k & ((L >> 1) - 1)];
+        if (k >= (L >> 1)) e = make_float2(-e.x, -e.y);
+        const float2 Ax = cmul(e, cmul(Px, Px));
+        const float2 Ay = cmul(e, cmul(Py, Py));
+        ac[bitrev(k, log2L)] = make_float2(Ax.x - Ay.y, Ax.y + Ay.x);
+    }
+    __syncwarp();
+    warp_fft(ac, L, log2L, tw, true);
+}
+
+// Same quantity by direct summation (any L; used when 2nr is not a power of two). All threads.
+__device__ void qi_autoconv_direct(const float *qprof, int nr, float2 *A, float2 *ac)
+{
+    const int L = 2 * nr;
+    for (int n = threadIdx.x; n < L; n += blockDim.x) A[n] = qi_concat(qprof, nr, n);
+    __syncthreads();
+    for (int n = threadIdx.x; n < L; n += blockDim.x) {
+        float sx = 0.0f, sy = 0.0f;
+        for (int m = 0; m < L; m++) {
+            int idx = n + m;
+            if (idx >= L) idx -= L;
+            const float2 a = A[idx], b = A[L - 1 - m];
+            sx += a.x * b.x;
+            sy += a.y * b.y;
+        }
+        ac[n] = make_float2(L * sx, L * sy);
+    }
+    __syncthreads();
+}
+
+// -------------------------------------------------------------------------------------
+// ComputeRadialProfile, utils.cpp:275-320: for each bin, the mean of the in-bounds
+// bilinear samples on the full circle (FP64 sum), or `mean` when no more than 4 samples
+// are in bounds; then NormalizeRadialProfile (utils.cpp:230-261) when asked.
+// -------------------------------------------------------------------------------------
+__device__ void radial_profile(const float *img, int W, int H, float cx, float cy, float mean, int nb, int nang,
+                               float minr, float rstep, const float2 *dirs, float *prof, bool normalize,
+                               double *red)
+{
+    const int tpb = lanes_per_bin(nb);
+    const int total = nb * tpb;
+    for (int base = 0; base < total; base += blockDim.x) {
+        const int t = base + threadIdx.x;
+        const int bin = t / tpb, sub = t - bin * tpb;
+        double sum = 0.0;
+        int cnt = 0;
+        if (bin < nb) {
+            const float r = minr + rstep * (float)bin;
+            for (int a = sub; a < nang; a += tpb) {
+                const float2 d = dirs[a];
+                float v;
+                if (bilinear(img, W, H, cx + d.x * r, cy + d.y * r, v)) {
+                    sum += v;
+                    cnt++;
+                }
+            }
+        }
+        for (int o = tpb >> 1; o > 0; o >>= 1) {
+            sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        }
+        if (bin < nb && sub == 0) prof[bin] = cnt > 4 ? (float)(sum / cnt) : mean;
+    }
+    __syncthreads();
+    if (normalize && threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        double s = 0;
+        for (int i = lane; i < nb; i += 32) s += prof[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        const float m = (float)(s / nb);
+        double s2 = 0;
+        for (int i = lane; i < nb; i += 32) {
+            const float p = prof[i] - m;
+            prof[i] = p;
+            s2 += (double)(p * p);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+        const double inv = 1.0 / sqrt(s2 / nb);
+        for (int i = lane; i < nb; i += 32) prof[i] = (float)((double)prof[i] * inv);
+    }
+    __syncthreads();
+}
+
+// CPUTracker::LUTProfileCompare, cpu_tracker.cpp:791-868 (plain form): one warp per plane
+// group, lanes over radial bins. scores[k] = -sum_r (w_r (p_r - L_kr))^2 with the difference
+// p_r - L_kr taken in FP32 and squared/accumulated in FP64, as the reference does.
+__device__ void zlut_scores_plain(const float *prof, const float *lut, int planes, int nb, const float *weights,
+                                  double *scores)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int k = warp; k < planes; k += nw) {
+        const float *row = lut + (size_t)k * nb;
+        double acc = 0.0;
+        for (int r = lane; r < nb; r += 32) {
+            double d = (double)(prof[r] - __ldg(row + r));
+            if (weights) d *= (double)__ldg(weights + r);
+            acc += d * d;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) scores[k] = -acc;
+    }
+    __syncthreads();
+}
+
+// -------------------------------------------------------------------------------------
+// 2D Gaussian MLE, CPUTracker::Compute2DGaussianMLE (cpu_tracker.cpp:514-589):
+// 4 parameters (x, y, I0, bg), fixed sigma, per-parameter Newton steps. The erf is the
+// Abramowitz & Stegun 7.1.26 form the reference binds (utils.h:395-417). Per iteration the
+// erf/exp terms depend only on the column (x) or the row (y), so they are evaluated once
+// per column and per row and combined per pixel.
+// -------------------------------------------------------------------------------------
+__device__ __forceinline__ float erf_as(float x, float e_mx2)
+{
+    // e_mx2 = exp(-x*x)
+    const float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f, a4 = -1.453152027f,
+                a5 = 1.061405429f, p = 0.3275911f;
+    const float sign = x < 0 ? -1.0f : 1.0f;
+    const float ax = fabsf(x);
+    const float t = 1.0f / (1.0f + p * ax);
+    const float y = 1.0f - (((((a5 * t + a4) * t) + a3) * t + a2) * t + a1) * t * e_mx2;
+    return sign * y;
+}
+
+// Column (or row) terms for coordinate c at position p: D = 0.5 erf(c0) - 0.5 erf(c1),
+// g = e^{-c1^2} - e^{-c0^2}, h = (c-p-.5) e^{-c1^2} - (c-p+.5) e^{-c0^2}.
+struct GaussAxisTerms {
+    float D, g, h;
+};
+
+__device__ __forceinline__ GaussAxisTerms gauss_axis_terms(int c, float p, float k1)
+{
+    const float e0 = (c - p + .5f) * k1;
+    const float e1 = (c - p - .5f) * k1;
+    const float x0 = expf(-e0 * e0), x1 = expf(-e1 * e1);
+    GaussAxisTerms t;
+    t.D = 0.5f * erf_as(e0, x0) - 0.5f * erf_as(e1, x1);
+    t.g = x1 - x0;
+    t.h = (c - p - .5f) * x1 - (c - p + .5f) * x0;
+    return t;
+}
+
+
+// CPUTracker::Compute2DGaussianMLE, cpu_tracker.cpp:514-589. col: 3*W floats, row: 3*H floats
+// of shared scratch. px/py enter as the start position (the COM) and leave as the estimate.
+template <class G>
+__device__ void gauss4_mle(const G &g, const float *img, int W, int H, float mean, float &px, float &py, int iters,
+                           float sigma, float *col, float *row)
+{
+    float I0 = mean * 0.5f * (float)W * (float)H;
+    float bg = mean * 0.5f;
+    const float k1 = 1.0f / (sqrtf(2.0f) * sigma);
+    const float k2 = 1.0f / (sqrtf(2 * 3.14159265359f) * sigma);
+    const float k3 = 1.0f / (sqrtf(2 * 3.14159265359f) * sigma * sigma * sigma);
+    for (int it = 0; it < iters; it++) {
+        g.sync();
+        for (int c = g.rank(); c < W; c += g.size()) {
+            const GaussAxisTerms t = gauss_axis_terms(c, px, k1);
+            col[3 * c] = t.D;
+            col[3 * c + 1] = t.g;
+            col[3 * c + 2] = t.h;
+        }
+        for (int r = g.rank(); r < H; r += g.size()) {
+            const GaussAxisTerms t = gauss_axis_terms(r, py, k1);
+            row[3 * r] = t.D;
+            row[3 * r + 1] = t.g;
+            row[3 * r + 2] = t.h;
+        }
+        g.sync();
+        double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int i = g.rank(); i < W * H; i += g.size()) {
+            const int y = i / W, x = i - y * W;
+            const float DX = col[3 * x], gX = col[3 * x + 1], hX = col[3 * x + 2];
+            const float DY = row[3 * y], gY = row[3 * y + 1], hY = row[3 * y + 2];
+            const float mu = bg + I0 * DX * DY;
+            const float dmu_dx = I0 * k2 * gX * DY;
+            const float dmu_dy = I0 * k2 * gY * DX;
+            const float dmu_dI0 = DX * DY;
+            const float smp = img[i];
+            const float f = smp / mu - 1;
+            acc[0] += dmu_dx * f;
+            acc[1] += dmu_dy * f;
+            acc[2] += dmu_dI0 * f;
+            acc[3] += f;
+            const float d2mu_dx = I0 * k3 * hX * DY;
+            const float d2mu_dy = I0 * k3 * hY * DX;
+            const float mu2 = mu * mu;
+            acc[4] += d2mu_dx * f - dmu_dx * dmu_dx * smp / mu2;
+            acc[5] += d2mu_dy * f - dmu_dy * dmu_dy * smp / mu2;
+            acc[6] += -dmu_dI0 * dmu_dI0 * smp / mu2;
+            acc[7] += -smp / mu2;
+        }
+        g.sum(acc);
+        px = (float)((double)px - acc[0] / acc[4]);
+        py = (float)((double)py - acc[1] / acc[5]);
+        I0 = (float)((double)I0 - acc[2] / acc[6]);
+        bg = (float)((double)bg - acc[3] / acc[7]);
+    }
+}
+
+// Solve the symmetric 5x5 system A d = b (Gaussian elimination, partial pivoting, FP64).
+__device__ __forceinline__ bool solve5(double (&A)[5][5], double (&b)[5], double (&d)[5])
+{
+#pragma unroll
+    for (int c = 0; c < 5; c++) {
+        int piv = c;
+#pragma unroll
+        for (int r = c + 1; r < 5; r++)
+            if (fabs(A[r][c]) > fabs(A[piv][c])) piv = r;
+        if (!(fabs(A[piv][c]) > 1e-300)) return false;
+        if (piv != c) {
+#pragma unroll
+            for (int j = 0; j < 5; j++) {
+                const double t = A[c][j];
+                A[c][j] = A[piv][j];
+                A[piv][j] = t;
+            }
+            const double t = b[c];
+            b[c] = b[piv];
+            b[piv] = t;
+        }
+#pragma unroll
+        for (int r = c + 1; r < 5; r++) {
+            const double f = A[r][c] / A[c][c];
+#pragma unroll
+            for (int j = c; j < 5; j++) A[r][j] -= f * A[c][j];
+            b[r] -= f * b[c];
+        }
+    }
+#pragma unroll
+    for (int i = 4; i >= 0; i--) {
+        double s = b[i];
+#pragma unroll
+        for (int j = i + 1; j < 5; j++) s -= A[i][j] * d[j];
+        d[i] = s / A[i][i];
+    }
+    return true;
+}
+
+// Extension (no reference counterpart): 5-parameter (x, y, I0, bg, sigma) Poisson MLE of an
+// integrated Gaussian spot, full Newton (Fisher-scoring) steps. Likelihood terms and
+// gradients in FP32 per pixel, FP64 reduction and an FP64 5x5 solve per step. p[] = {x, y,
+// I0, bg, sigma}; col/row: 5*W and 5*H floats of shared scratch.
+template <class G>
+__device__ void gauss5_mle(const G &g, const float *img, int W, int H, float (&p)[5], int iters, float *col,
+                           float *row)
+{
+    for (int it = 0; it < iters; it++) {
+        const float s = p[4];
+        const float k1 = 1.0f / (sqrtf(2.0f) * s);
+        const float k2 = 1.0f / (sqrtf(2 * 3.14159265359f) * s);
+        g.sync();
+        for (int c = g.rank(); c < W + H; c += g.size()) {
+            const bool is_col = c < W;
+            const int cc = is_col ? c : c - W;
+            const float pc = is_col ? p[0] : p[1];
+            const float a0 = (cc - pc + .5f) * k1, a1 = (cc - pc - .5f) * k1;
+            const float e0 = expf(-a0 * a0), e1 = expf(-a1 * a1);
+            float *t = is_col ? col + 3 * cc : row + 3 * cc;
+            t[0] = 0.5f * (erff(a0) - erff(a1));
+            t[1] = (e1 - e0) * k2;                                                  // dD/dp
+            t[2] = ((cc - pc - .5f) * e1 - (cc - pc + .5f) * e0) * k2 / s;          // dD/dsigma
+        }
+        g.sync();
+        float a[20];
+#pragma unroll
+        for (int k = 0; k < 20; k++) a[k] = 0.0f;
+        for (int i = g.rank(); i < W * H; i += g.size()) {
+            const int y = i / W, x = i - y * W;
+            const float DX = col[3 * x], dX = col[3 * x + 1], sX = col[3 * x + 2];
+            const float DY = row[3 * y], dY = row[3 * y + 1], sY = row[3 * y + 2];
+            const float mu = p[3] + p[2] * DX * DY;
+            const float J[5] = {p[2] * dX * DY, p[2] * DX * dY, DX * DY, 1.0f, p[2] * (sX * DY + DX * sY)};
+            const float f = img[i] / mu - 1.0f;
+            const float imu = 1.0f / mu;
+            int k = 5;
+#pragma unroll
+            for (int u = 0; u < 5; u++) {
+                a[u] += J[u] * f;
+#pragma unroll
+                for (int v = u; v < 5; v++) a[k++] += J[u] * J[v] * imu;
+            }
+        }
+        double acc[20];
+#pragma unroll
+        for (int k = 0; k < 20; k++) acc[k] = a[k];
+        g.sum(acc);
+        double A[5][5], b[5], d[5];
+        int k = 5;
+#pragma unroll
+        for (int u = 0; u < 5; u++) {
+            b[u] = acc[u];
+#pragma unroll
+            for (int v = u; v < 5; v++) A[u][v] = A[v][u] = acc[k++];
+        }
+        if (!solve5(A, b, d)) break;
+#pragma unroll
+        for (int u = 0; u < 5; u++) p[u] = (float)((double)p[u] + d[u]);
+        p[2] = fmaxf(p[2], 1e-3f);
+        p[3] = fmaxf(p[3], 1e-3f);
+        p[4] = fminf(fmaxf(p[4], 0.3f), 0.5f * (float)W);
+    }
+}
+
+}  // namespace qtrk

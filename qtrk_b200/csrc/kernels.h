@@ -1,0 +1,35 @@
+// Host-side entry points of the CUDA kernels (implemented in localize.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "qtrk_c_api.h"
+#include "track_params.h"
+
+namespace qtrk {
+
+// Fill the shared-memory layout fields of P from its sizes.
+void plan_smem(TrackParams &P);
+// Raise the dynamic shared-memory limit of the kernels once per device.
+cudaError_t prepare_kernels(int device);
+// True when the Gaussian-only warp-per-ROI kernel serves P.
+bool use_gauss_warp(const TrackParams &P);
+
+// Localize `count` ROIs: ROI i starts at pixels + (roi_offsets ? roi_offsets[i] : i*roi_stride).
+// jobs may be null (job i = {frame=i}). One kernel launch.
+cudaError_t launch_localize(const TrackParams &P, const uint8_t *pixels, int pitch, int64_t roi_stride,
+                            const int64_t *roi_offsets, const LocalizationJob *jobs, int count,
+                            LocalizationResult *results, cudaStream_t stream);
+
+// One BuildLUT plane: nbeads ROIs stacked at pitch*H; adds each profile to lut[bead][plane].
+cudaError_t launch_build_lut(const TrackParams &P, const uint8_t *pixels, int pitch, int nbeads, int plane,
+                             const float2 *known_pos, bool normalize, float *lut, cudaStream_t stream);
+
+// NormalizeRadialProfile on `rows` rows of nb floats.
+cudaError_t launch_finalize_lut(float *lut, int rows, int nb, cudaStream_t stream);
+
+// Radial profile of one float image (P.width x P.height) around (cx, cy).
+cudaError_t launch_profile(const TrackParams &P, const float *img, float cx, float cy, float mean, bool normalize,
+                           float *out, cudaStream_t stream);
+
+}  // namespace qtrk

@@ -1,0 +1,430 @@
+// Localization kernels for sm_100a.
+//
+// localize_kernel: one CTA per ROI runs the whole per-ROI pipeline of
+//   QueuedCPUTracker::ProcessJob (cputrack/QueuedCPUTracker.cpp:273-361) on a float tile
+//   of the ROI in shared memory: load + convert (+ calibration) -> mean/COM -> QI
+//   iterations (or the 2D Gaussian MLE) -> radial profile -> Z-LUT match -> result.
+//   Pixels are read from HBM exactly once; everything after the load works on-chip.
+// gauss_warp_kernel: one warp per small ROI (<= 32x32) for the Gaussian-only mode.
+// build_lut_kernel / finalize_lut_kernel: QueuedCPUTracker::BuildLUT / FinalizeLUT
+//   (cputrack/QueuedCPUTracker.cpp:580-659) with the accumulation on the device.
+// profile_kernel: ComputeRadialProfile (cputrack/utils.cpp:275-320) for one image.
+#include <cstdint>
+#include <cstdio>
+#include <cuda_runtime.h>
+
+#include "device_common.cuh"
+#include "kernels.h"
+
+namespace qtrk {
+
+// QI / Z-LUT least-squares weights, cputrack/QueuedTracker.h:349,359
+__device__ const float kQIWeights[7] = {0.14f, 0.5f, 0.85f, 1.0f, 0.85f, 0.5f, 0.14f};
+__device__ const float kZLUTWeights[7] = {0.15f, 0.5f, 0.85f, 1.0f, 0.85f, 0.5f, 0.15f};
+
+struct SmemView {
+    float *img, *misc;
+    float2 *qdirs, *tw, *zdirs;
+    uint8_t *work;
+    double *red;
+};
+
+__device__ __forceinline__ SmemView smem_view(uint8_t *smem, const TrackParams &P)
+{
+    SmemView v;
+    v.img = reinterpret_cast<float *>(smem + P.sm_img);
+    v.misc = reinterpret_cast<float *>(smem + P.sm_misc);
+    v.red = reinterpret_cast<double *>(smem + P.sm_red);
+    v.work = smem + P.sm_work;
+    float2 *tab = reinterpret_cast<float2 *>(smem + P.sm_tables);
+    v.qdirs = tab;
+    v.tw = tab + P.qi_angpq;
+    v.zdirs = v.tw + P.qi_nr;  // L/2 = qi_nr twiddles
+    return v;
+}
+
+// Copy the direction / twiddle tables into shared memory (all threads).
+__device__ __forceinline__ void load_tables(const SmemView &s, const TrackParams &P)
+{
+    const float2 *qd = static_cast<const float2 *>(P.qi_dirs);
+    const float2 *tw = static_cast<const float2 *>(P.qi_twiddles);
+    const float2 *zd = static_cast<const float2 *>(P.z_dirs);
+    if (qd)
+        for (int i = threadIdx.x; i < P.qi_angpq; i += blockDim.x) s.qdirs[i] = qd[i];
+    if (tw)
+        for (int i = threadIdx.x; i < P.qi_nr; i += blockDim.x) s.tw[i] = tw[i];
+    if (zd)
+        for (int i = threadIdx.x; i < P.z_angsteps; i += blockDim.x) s.zdirs[i] = zd[i];
+}
+
+// CPUTracker::ComputeQI, cpu_tracker.cpp:285-360. All threads call; returns the position
+// and the boundary flag of the last iteration.
+__device__ void qi_localize(const SmemView &s, const TrackParams &P, float mean, float &cx, float &cy, bool &bhit,
+                            const float *rweights)
+{
+    const int W = P.width, H = P.height, nr = P.qi_nr, L = 2 * nr;
+    const bool pow2 = (L & (L - 1)) == 0 && L >= 2;
+    float *qprof = reinterpret_cast<float *>(s.work);
+    float2 *A = reinterpret_cast<float2 *>(s.work + ((4 * nr * 4 + 15) & ~15));
+    float2 *ac = A + L;
+    const float rstep = (P.qi_maxr - P.qi_minr) / (float)nr;  // also pixelsPerProfLen (cpu_tracker.cpp:311,649)
+    for (int k = 0; k < P.qi_iterations; k++) {
+        bhit = check_boundaries(cx, cy, P.qi_maxr, W, H);
+        qi_quadrant_profiles(s.img, W, H, cx, cy, mean, nr, P.qi_nang[k], P.qi_stride[k], P.qi_minr, rstep, s.qdirs,
+                             rweights, qprof);
+        __syncthreads();
+        if (pow2) {
+            if (threadIdx.x < 32) qi_autoconv_fft(qprof, nr, A, ac, s.tw);
+        } else {
+            qi_autoconv_direct(qprof, nr, A, ac);
+        }
+        if (threadIdx.x < 32) {
+            // autoconv[x] = out[(x + nr) mod L] (cpu_tracker.cpp:400-402)
+            auto atx = [&](int x) {
+                int n = x + nr;
+                if (n >= L) n -= L;
+                return ac[n].x;
+            };
+            auto aty = [&](int x) {
+                int n = x + nr;
+                if (n >= L) n -= L;
+                return ac[n].y;
+            };
+            const int ix = warp_argmax(atx, L);
+            const int iy = warp_argmax(aty, L);
+            if (threadIdx.x == 0) {
+                const float mx = (float)max_interp7(atx, L, ix, kQIWeights);
+                const float my = (float)max_interp7(aty, L, iy, kQIWeights);
+                const float offx = (mx - (float)nr) * (3.14159265359f / 4);
+                const float offy = (my - (float)nr) * (3.14159265359f / 4);
+                s.misc[0] = cx + offx * rstep;
+                s.misc[1] = cy + offy * rstep;
+            }
+        }
+        __syncthreads();
+        cx = s.misc[0];
+        cy = s.misc[1];
+        __syncthreads();
+    }
+}
+
+// Radial profile + Z-LUT compare (QueuedCPUTracker.cpp:319-338). Returns z (0 without a LUT).
+__device__ float z_localize(const SmemView &s, const TrackParams &P, float mean, float x, float y, int bead)
+{
+    const int nb = P.z_nbins;
+    float *prof = reinterpret_cast<float *>(s.work);
+    double *scores = reinterpret_cast<double *>(s.work + (((nb * 4) + 15) & ~15));
+    const float rstep = (P.z_maxr - P.z_minr) / (float)nb;
+    radial_profile(s.img, P.width, P.height, x, y, mean, nb, P.z_angsteps, P.z_minr, rstep, s.zdirs, prof,
+                   (P.mode & kLT_NormalizeProfile) != 0, s.red);
+    if (!P.lut || bead < 0 || bead >= P.lut_count) return 0.0f;
+    const float *lut = P.lut + (size_t)bead * P.lut_planes * nb;
+    zlut_scores_plain(prof, lut, P.lut_planes, nb, P.z_weights, scores);
+    if (P.cmp_scores)
+        for (int k = threadIdx.x; k < P.lut_planes; k += blockDim.x)
+            P.cmp_scores[(size_t)bead * P.lut_planes + k] = (float)scores[k];
+    if (threadIdx.x < 32) {
+        auto at = [&](int i) { return scores[i]; };
+        const int im = warp_argmax(at, P.lut_planes);
+        if (threadIdx.x == 0) s.misc[2] = (float)max_interp7(at, P.lut_planes, im, kZLUTWeights);
+    }
+    __syncthreads();
+    return s.misc[2];
+}
+
+__device__ __forceinline__ void read_job(const LocalizationJob *jobs, int i, uint32_t (&w)[6])
+{
+    if (jobs) {
+        const uint32_t *p = reinterpret_cast<const uint32_t *>(jobs) + (size_t)i * 6;
+#pragma unroll
+        for (int k = 0; k < 6; k++) w[k] = p[k];
+    } else {
+        w[0] = (uint32_t)i;
+#pragma unroll
+        for (int k = 1; k < 6; k++) w[k] = 0;
+    }
+}
+
+__device__ __forceinline__ void write_result(LocalizationResult *results, int i, const uint32_t (&job)[6], float x,
+                                             float y, float z, float gx, float gy, uint32_t err, float mean)
+{
+    uint32_t *o = reinterpret_cast<uint32_t *>(results) + (size_t)i * 13;
+#pragma unroll
+    for (int k = 0; k < 6; k++) o[k] = job[k];
+    o[6] = __float_as_uint(x);
+    o[7] = __float_as_uint(y);
+    o[8] = __float_as_uint(z);
+    o[9] = __float_as_uint(gx);
+    o[10] = __float_as_uint(gy);
+    o[11] = err;
+    o[12] = __float_as_uint(mean);
+}
+
+// kGauss selects the instantiation: false = COM / QI (+ Z), true = 2D Gaussian MLE (+ Z).
+// Separate instantiations keep the QI path's register budget free of the MLE's FP64 solve.
+template <bool kGauss>
+__global__ void __launch_bounds__(kBlockThreads, 3) localize_kernel(TrackParams P, const uint8_t *__restrict__ pixels,
+                                                                    int pitch, int64_t roi_stride,
+                                                                    const int64_t *__restrict__ roi_offsets,
+                                                                    const LocalizationJob *__restrict__ jobs, int count,
+                                                                    LocalizationResult *__restrict__ results)
+{
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int roi = blockIdx.x;
+    if (roi >= count) return;
+    const SmemView s = smem_view(smem, P);
+    uint32_t job[6];
+    read_job(jobs, roi, job);
+    const int bead = (int)job[2];
+    const int64_t off = roi_offsets ? roi_offsets[roi] : (int64_t)roi * roi_stride;
+
+    load_tables(s, P);
+    BlockGroup g{s.red};
+    load_roi(g, s.img, pixels + off, pitch, P, bead);
+
+    const int W = P.width, H = P.height;
+    const ComResult com = compute_com(g, s.img, W, H, P.com_bgcorrection);
+    float comx = com.x, comy = com.y;
+    if (isnan(comx) || isnan(comy)) {  // QueuedCPUTracker.cpp:294-295
+        comx = (float)(W / 2);
+        comy = (float)(H / 2);
+    }
+    float x = comx, y = comy, z = 0.0f;
+    bool bhit = false;
+    if (!kGauss) {
+        if (P.mode & kLT_QI) qi_localize(s, P, com.mean, x, y, bhit, P.qi_rweights);
+    } else {
+        float *col = reinterpret_cast<float *>(s.work);
+        if (P.mode & kLT_Gaussian5P) {
+            float p[5] = {x, y, com.mean * 0.5f * (float)(W * H), com.mean * 0.5f, P.g_sigma};
+            gauss5_mle(g, s.img, W, H, p, P.g_iterations, col, col + 3 * W);
+            x = p[0];
+            y = p[1];
+            z = p[4];
+        } else {
+            gauss4_mle(g, s.img, W, H, com.mean, x, y, P.g_iterations, P.g_sigma, col, col + 3 * W);
+        }
+        __syncthreads();
+    }
+    if (P.mode & kLT_LocalizeZ) {
+        bhit = check_boundaries(x, y, P.z_maxr, W, H);
+        z = z_localize(s, P, com.mean, x, y, bead);
+    }
+    if (threadIdx.x == 0) write_result(results, roi, job, x, y, z, comx, comy, bhit ? 1u : 0u, com.mean);
+}
+
+// Gaussian-only mode for ROIs of at most 32x32 pixels: one warp per ROI, 8 ROIs per CTA.
+__global__ void __launch_bounds__(256) gauss_warp_kernel(TrackParams P, const uint8_t *__restrict__ pixels, int pitch,
+                                                         int64_t roi_stride, const int64_t *__restrict__ roi_offsets,
+                                                         const LocalizationJob *__restrict__ jobs, int count,
+                                                         LocalizationResult *__restrict__ results)
+{
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int warp = threadIdx.x >> 5;
+    const int roi = blockIdx.x * 8 + warp;
+    if (roi >= count) return;  // whole warps exit together
+    const int W = P.width, H = P.height;
+    const int per_warp = ((W * H + 3 * (W + H) + 3) & ~3) * 4;
+    float *img = reinterpret_cast<float *>(smem + warp * per_warp);
+    float *col = img + W * H;
+    float *row = col + 3 * W;
+    uint32_t job[6];
+    read_job(jobs, roi, job);
+    const int64_t off = roi_offsets ? roi_offsets[roi] : (int64_t)roi * roi_stride;
+    WarpGroup g;
+    load_roi(g, img, pixels + off, pitch, P, (int)job[2]);
+    const ComResult com = compute_com(g, img, W, H, P.com_bgcorrection);
+    float comx = com.x, comy = com.y;
+    if (isnan(comx) || isnan(comy)) {
+        comx = (float)(W / 2);
+        comy = (float)(H / 2);
+    }
+    float x = comx, y = comy, z = 0.0f;
+    if (P.mode & kLT_Gaussian5P) {
+        float p[5] = {x, y, com.mean * 0.5f * (float)(W * H), com.mean * 0.5f, P.g_sigma};
+        gauss5_mle(g, img, W, H, p, P.g_iterations, col, row);
+        x = p[0];
+        y = p[1];
+        z = p[4];
+    } else {
+        gauss4_mle(g, img, W, H, com.mean, x, y, P.g_iterations, P.g_sigma, col, row);
+    }
+    if ((threadIdx.x & 31) == 0) write_result(results, roi, job, x, y, z, comx, comy, 0u, com.mean);
+}
+
+// One bead of QueuedCPUTracker::BuildLUT (QueuedCPUTracker.cpp:582-645): ROI i of the stack is
+// at data + pitch*H*i. Position from known_pos, else COM (no background correction) + QI
+// without radial weights (line 603). The profile's fallback value is the tracker's mean,
+// which SetImage resets to 0 when known_pos skips the COM (cpu_tracker.h:135).
+__global__ void __launch_bounds__(kBlockThreads) build_lut_kernel(TrackParams P, const uint8_t *__restrict__ pixels,
+                                                                  int pitch, int nbeads, int plane,
+                                                                  const float2 *__restrict__ known_pos,
+                                                                  int normalize, float *__restrict__ lut)
+{
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int bead = blockIdx.x;
+    if (bead >= nbeads) return;
+    const SmemView s = smem_view(smem, P);
+    load_tables(s, P);
+    BlockGroup g{s.red};
+    load_roi(g, s.img, pixels + (size_t)pitch * P.height * bead, pitch, P, bead);
+    float x, y, mean = 0.0f;
+    if (known_pos) {
+        x = known_pos[bead].x;
+        y = known_pos[bead].y;
+    } else {
+        const ComResult com = compute_com(g, s.img, P.width, P.height, 0.0f);
+        mean = com.mean;
+        x = com.x;
+        y = com.y;
+        bool bhit;
+        qi_localize(s, P, mean, x, y, bhit, nullptr);
+    }
+    const int nb = P.z_nbins;
+    float *prof = reinterpret_cast<float *>(s.work);
+    const float rstep = (P.z_maxr - P.z_minr) / (float)nb;
+    radial_profile(s.img, P.width, P.height, x, y, mean, nb, P.z_angsteps, P.z_minr, rstep, s.zdirs, prof,
+                   normalize != 0, s.red);
+    float *dst = lut + ((size_t)bead * P.lut_planes + plane) * nb;
+    for (int r = threadIdx.x; r < nb; r += blockDim.x) dst[r] += prof[r];
+}
+
+// QueuedCPUTracker::FinalizeLUT (QueuedCPUTracker.cpp:648-659): NormalizeRadialProfile
+// (utils.cpp:230-261) on every (bead, plane) row. One warp per row.
+__global__ void finalize_lut_kernel(float *__restrict__ lut, int rows, int nb)
+{
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (row >= rows) return;
+    const int lane = threadIdx.x & 31;
+    float *p = lut + (size_t)row * nb;
+    double s = 0;
+    for (int i = lane; i < nb; i += 32) s += p[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const float m = (float)(s / nb);
+    double s2 = 0;
+    for (int i = lane; i < nb; i += 32) {
+        const float v = p[i] - m;
+        p[i] = v;
+        s2 += (double)(v * v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    const double inv = 1.0 / sqrt(s2 / nb);
+    for (int i = lane; i < nb; i += 32) p[i] = (float)((double)p[i] * inv);
+}
+
+// ComputeRadialProfile (utils.cpp:275-320) of one float image with a given fallback mean.
+__global__ void __launch_bounds__(kBlockThreads) profile_kernel(TrackParams P, const float *__restrict__ img_in,
+                                                                float cx, float cy, float mean, int normalize,
+                                                                float *__restrict__ out)
+{
+    extern __shared__ __align__(16) uint8_t smem[];
+    const SmemView s = smem_view(smem, P);
+    load_tables(s, P);
+    BlockGroup g{s.red};
+    load_roi(g, s.img, reinterpret_cast<const uint8_t *>(img_in), P.width * 4, P, -1);
+    float *prof = reinterpret_cast<float *>(s.work);
+    const float rstep = (P.z_maxr - P.z_minr) / (float)P.z_nbins;
+    radial_profile(s.img, P.width, P.height, cx, cy, mean, P.z_nbins, P.z_angsteps, P.z_minr, rstep, s.zdirs, prof,
+                   normalize != 0, s.red);
+    for (int r = threadIdx.x; r < P.z_nbins; r += blockDim.x) out[r] = prof[r];
+}
+
+// ------------------------------------------------------------------------------------------
+// host-side launchers
+// ------------------------------------------------------------------------------------------
+static int align16(int v) { return (v + 15) & ~15; }
+
+void plan_smem(TrackParams &P)
+{
+    const int W = P.width, H = P.height;
+    const int nr = P.qi_nr > 0 ? P.qi_nr : 1, L = 2 * nr;
+    P.sm_img = 0;
+    P.sm_tables = align16(W * H * 4);
+    const int tables = (P.qi_angpq + nr + P.z_angsteps) * 8;
+    P.sm_work = P.sm_tables + align16(tables);
+    const int qi_work = align16(4 * nr * 4) + 2 * L * 8;
+    const int z_work = align16(P.z_nbins * 4) + P.lut_planes * 8;
+    const int g_work = (5 * W + 5 * H) * 4;
+    int work = qi_work;
+    if (z_work > work) work = z_work;
+    if (g_work > work) work = g_work;
+    P.sm_red = P.sm_work + align16(work);
+    static_assert(kBlockThreads / 32 * 20 <= 256, "reduction scratch too small for the 5-parameter MLE");
+    P.sm_misc = P.sm_red + 256 * 8;  // block_sum scratch: N * warps doubles, N <= 20
+    P.smem_bytes = P.sm_misc + 64;
+}
+
+int gauss_warp_smem(const TrackParams &P)
+{
+    const int W = P.width, H = P.height;
+    return 8 * ((W * H + 3 * (W + H) + 3) & ~3) * 4;
+}
+
+static bool g_attrs_set[64];
+
+cudaError_t prepare_kernels(int device)
+{
+    if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+    if (g_attrs_set[device]) return cudaSuccess;
+    const int max_smem = 227 * 1024;
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(localize_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)))
+        return e;
+    if ((e = cudaFuncSetAttribute(localize_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)))
+        return e;
+    if ((e = cudaFuncSetAttribute(build_lut_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem))) return e;
+    if ((e = cudaFuncSetAttribute(profile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem))) return e;
+    if ((e = cudaFuncSetAttribute(gauss_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem))) return e;
+    g_attrs_set[device] = true;
+    return cudaSuccess;
+}
+
+bool use_gauss_warp(const TrackParams &P)
+{
+    return (P.mode & kLT_Gaussian2D) && !(P.mode & (kLT_QI | kLT_LocalizeZ)) && P.width <= 32 && P.height <= 32;
+}
+
+cudaError_t launch_localize(const TrackParams &P, const uint8_t *pixels, int pitch, int64_t roi_stride,
+                            const int64_t *roi_offsets, const LocalizationJob *jobs, int count,
+                            LocalizationResult *results, cudaStream_t stream)
+{
+    if (count <= 0) return cudaSuccess;
+    if (use_gauss_warp(P)) {
+        gauss_warp_kernel<<<(count + 7) / 8, 256, gauss_warp_smem(P), stream>>>(P, pixels, pitch, roi_stride,
+                                                                              roi_offsets, jobs, count, results);
+    } else if ((P.mode & kLT_Gaussian2D) && !(P.mode & kLT_QI)) {
+        localize_kernel<true><<<count, kBlockThreads, P.smem_bytes, stream>>>(P, pixels, pitch, roi_stride,
+                                                                              roi_offsets, jobs, count, results);
+    } else {
+        localize_kernel<false><<<count, kBlockThreads, P.smem_bytes, stream>>>(P, pixels, pitch, roi_stride,
+                                                                               roi_offsets, jobs, count, results);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_build_lut(const TrackParams &P, const uint8_t *pixels, int pitch, int nbeads, int plane,
+                             const float2 *known_pos, bool normalize, float *lut, cudaStream_t stream)
+{
+    if (nbeads <= 0) return cudaSuccess;
+    build_lut_kernel<<<nbeads, kBlockThreads, P.smem_bytes, stream>>>(P, pixels, pitch, nbeads, plane, known_pos,
+                                                                      normalize ? 1 : 0, lut);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finalize_lut(float *lut, int rows, int nb, cudaStream_t stream)
+{
+    if (rows <= 0) return cudaSuccess;
+    finalize_lut_kernel<<<(rows + 7) / 8, 256, 0, stream>>>(lut, rows, nb);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_profile(const TrackParams &P, const float *img, float cx, float cy, float mean, bool normalize,
+                           float *out, cudaStream_t stream)
+{
+    profile_kernel<<<1, kBlockThreads, P.smem_bytes, stream>>>(P, img, cx, cy, mean, normalize ? 1 : 0, out);
+    return cudaGetLastError();
+}
+
+}  // namespace qtrk

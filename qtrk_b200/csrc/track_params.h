@@ -1,0 +1,71 @@
+// Parameters shared between the host tracker and the sm_100a kernels.
+//
+// One TrackParams value describes everything a localization launch needs: ROI geometry,
+// mode bits, the derived step counts of QTrkComputedConfig::Update
+// (cputrack/QueuedTracker.cpp:6-21) and device pointers to the read-only tables the
+// host precomputes once per configuration (direction tables, radial weights, FFT
+// twiddles, the Z-LUT). It is passed by value as a kernel parameter.
+#pragma once
+#include <cstdint>
+
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+#else
+struct float2_host { float x, y; };
+#endif
+
+namespace qtrk {
+
+constexpr int kMaxQIIterations = 32;
+constexpr int kBlockThreads = 256;  // threads per localization CTA (one ROI per CTA)
+
+// Mode bits (cputrack/qtrk_c_api.h:5-20 plus the library's extension bits).
+enum : int {
+    kLT_QI = 2,
+    kLT_Gaussian2D = 4,
+    kLT_LocalizeZ = 16,
+    kLT_NormalizeProfile = 64,
+    kLT_ClearFirstFourPixels = 128,
+    kLT_ZMatchBF16 = 1 << 20,
+    kLT_JointRefine = 1 << 21,
+    kLT_Gaussian5P = 1 << 22,
+};
+
+struct TrackParams {
+    int width, height;  // ROI size in pixels
+    int pdt;            // 0 = u8, 1 = u16, 2 = f32
+    int mode;           // LocalizeModeEnum bits
+    float com_bgcorrection;
+
+    // QI (cputrack/cpu_tracker.cpp:285-406)
+    int qi_iterations, qi_nr, qi_angpq;
+    float qi_minr, qi_maxr;
+    int qi_nang[kMaxQIIterations];    // angular samples per quadrant in iteration k (>= 4)
+    int qi_stride[kMaxQIIterations];  // direction-table stride in iteration k (cpu_tracker.cpp:655-657)
+    const void *qi_dirs;              // float2[qi_angpq]: quadrant directions (cos, sin)
+    const float *qi_rweights;         // float[qi_nr] radial bin window or nullptr
+    const void *qi_twiddles;          // float2[L/2], e^{-2 pi i k / L}, L = 2 qi_nr
+
+    // Radial profile + Z-LUT (cputrack/utils.cpp:275-320, cputrack/cpu_tracker.cpp:791-868)
+    int z_nbins, z_angsteps;
+    float z_minr, z_maxr;
+    const void *z_dirs;       // float2[z_angsteps]
+    const float *lut;         // [lut_count][lut_planes][z_nbins]
+    int lut_count, lut_planes;
+    const float *z_weights;   // float[z_nbins] or nullptr
+    float *cmp_scores;        // [lut_count][lut_planes] or nullptr (compare-profile output)
+
+    // 2D Gaussian MLE (cputrack/cpu_tracker.cpp:514-589)
+    int g_iterations;
+    float g_sigma;
+
+    // Per-bead pixel calibration (cputrack/cpu_tracker.cpp:98-112); nullptr when unset
+    const float *calib_offset, *calib_gain;  // [calib_count][height][width]
+    int calib_count;
+    float offset_factor, gain_factor;
+
+    // Dynamic shared-memory layout (byte offsets), filled by the host
+    int sm_img, sm_tables, sm_work, sm_red, sm_misc, smem_bytes;
+};
+
+}  // namespace qtrk

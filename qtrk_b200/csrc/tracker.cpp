@@ -1,0 +1,958 @@
+// Host side of the B200 tracker: configuration, device tables, staging slots, queue.
+// See tracker.h for the design; reference behaviour is cited per method.
+#include "tracker.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <sstream>
+#include <stdexcept>
+#include <thread>
+
+#include "kernels.h"
+
+namespace qtrk {
+
+namespace {
+
+double now_s()
+{
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+int pdt_bytes(int pdt) { return pdt == 0 ? 1 : (pdt == 1 ? 2 : 4); }
+
+// Sets the calling thread's current device for the lifetime of the guard.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+constexpr double kWaitLimitSeconds = 120.0;  // bound on any host wait for the GPU
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------
+// Configuration (cputrack/QueuedTracker.cpp:6-21, cputrack/utils.cpp:644-677)
+// ------------------------------------------------------------------------------------
+int nearest_pow2(int v)
+{
+    int r = 1;
+    while (r < v) r *= 2;
+    if (std::fabs((float)(r - v)) < std::fabs((float)(r / 2 - v))) return r;
+    return r / 2;
+}
+
+QTrkComputedConfig compute_config(const QTrkSettings &s)
+{
+    QTrkComputedConfig c;
+    std::memset(&c, 0, sizeof(c));
+    c.base = s;
+    const int roi = s.width / 2;
+    c.zlut_maxradius = roi * s.zlut_roi_coverage;
+    const float zlut_perimeter = 2 * 3.141593f * c.zlut_maxradius;
+    c.zlut_angularsteps = (int)(zlut_perimeter * s.zlut_angular_coverage);
+    c.zlut_radialsteps = (int)((c.zlut_maxradius - s.zlut_minradius) * s.zlut_radial_coverage);
+    c.qi_maxradius = roi * s.qi_roi_coverage;
+    const float qi_perimeter = 2 * 3.141593f * c.qi_maxradius;
+    c.qi_angstepspq = (int)(qi_perimeter * s.qi_angular_coverage / 4);
+    c.qi_radialsteps = (int)((c.qi_maxradius - s.qi_minradius) * s.qi_radial_coverage);
+    c.qi_radialsteps = nearest_pow2(c.qi_radialsteps);
+    return c;
+}
+
+std::vector<float> radial_bin_window(int rsteps)
+{
+    std::vector<float> w(std::max(rsteps, 0));
+    for (int i = 0; i < rsteps; i++) {
+        const float x = i / (float)rsteps;
+        const float t2 = 0.05f, t1 = 0.01f;
+        const float fall = 1.0f - expf(-((1 - x) * (1 - x)) / t2);
+        const float rise = 1.0f - expf(-(x * x) / t1);
+        w[i] = sqrtf(fall * rise * x * 2);
+    }
+    return w;
+}
+
+// ------------------------------------------------------------------------------------
+// Registry for the instance-less reference entry points
+// ------------------------------------------------------------------------------------
+static std::mutex g_reg_mu;
+static std::vector<Tracker *> g_trackers;
+static float g_default_of = 1.0f, g_default_gf = 1.0f;
+
+void register_tracker(Tracker *t)
+{
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    g_trackers.push_back(t);
+}
+void unregister_tracker(Tracker *t)
+{
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    g_trackers.erase(std::remove(g_trackers.begin(), g_trackers.end(), t), g_trackers.end());
+}
+Tracker *latest_tracker()
+{
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    return g_trackers.empty() ? nullptr : g_trackers.back();
+}
+void for_each_tracker(void (*fn)(Tracker *, void *), void *arg)
+{
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    for (Tracker *t : g_trackers) fn(t, arg);
+}
+float default_offset_factor() { return g_default_of; }
+float default_gain_factor() { return g_default_gf; }
+void set_default_factors(float of, float gf)
+{
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    g_default_of = of;
+    g_default_gf = gf;
+}
+
+// ------------------------------------------------------------------------------------
+// Tracker
+// ------------------------------------------------------------------------------------
+void Tracker::CheckCuda(cudaError_t e, const char *what)
+{
+    if (e != cudaSuccess) {
+        throw std::runtime_error(std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+    }
+}
+
+void Tracker::Warn(const std::string &msg)
+{
+    std::lock_guard<std::mutex> lk(warn_mu_);
+    if (warnings_.size() < 65536) warnings_ += msg + "\n";
+}
+
+Tracker::Tracker(const QTrkSettings &settings)
+{
+    cfg = compute_config(settings);
+    const QTrkSettings &s = cfg.base;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        throw std::runtime_error(std::string("no usable CUDA device: ") + (e ? cudaGetErrorString(e) : "count is 0"));
+    if (s.cuda_device >= 0) {
+        device_ = s.cuda_device;
+    } else {
+        // QTrkCUDA_UseAll / UseBest / UseList: one instance drives one GPU (the current one);
+        // several GPUs are served by one instance per GPU.
+        CheckCuda(cudaGetDevice(&device_), "cudaGetDevice");
+    }
+    if (device_ >= ndev) throw std::runtime_error("cuda_device " + std::to_string(device_) + " does not exist");
+    cudaDeviceProp prop;
+    CheckCuda(cudaGetDeviceProperties(&prop, device_), "cudaGetDeviceProperties");
+    if (prop.major != 10 || prop.minor != 0)
+        throw std::runtime_error("libqtrk_b200 is built for sm_100a (B200); device " + std::to_string(device_) +
+                                 " is sm_" + std::to_string(prop.major) + std::to_string(prop.minor));
+    DeviceGuard dg(device_);
+    CheckCuda(prepare_kernels(device_), "prepare_kernels");
+
+    const int W = s.width, H = s.height;
+    if (W < 4 || H < 4) throw std::runtime_error("ROI width and height must be at least 4");
+    if (s.qi_iterations < 0 || s.qi_iterations > kMaxQIIterations)
+        throw std::runtime_error("qi_iterations must be in [0, " + std::to_string(kMaxQIIterations) + "]");
+    if (cfg.qi_radialsteps < 1 || cfg.qi_angstepspq < 1) throw std::runtime_error("QI step counts must be >= 1");
+    if (cfg.zlut_radialsteps < 1 || cfg.zlut_angularsteps < 1)
+        throw std::runtime_error("Z-LUT step counts must be >= 1");
+
+    // ---- parameters and device tables ----
+    TrackParams &P = base_;
+    std::memset(&P, 0, sizeof(P));
+    P.width = W;
+    P.height = H;
+    P.com_bgcorrection = s.com_bgcorrection;
+    P.qi_iterations = s.qi_iterations;
+    P.qi_nr = cfg.qi_radialsteps;
+    P.qi_angpq = cfg.qi_angstepspq;
+    P.qi_minr = s.qi_minradius;
+    P.qi_maxr = cfg.qi_maxradius;
+    {
+        // angular samples per iteration, cpu_tracker.cpp:314,356 and 642-657
+        float angsteps = cfg.qi_angstepspq / powf(s.qi_angstep_factor, (float)s.qi_iterations);
+        for (int k = 0; k < s.qi_iterations; k++) {
+            int n = (int)angsteps;
+            if (n < 4) n = 4;
+            const float angstepf = (float)cfg.qi_angstepspq / n;
+            P.qi_nang[k] = n;
+            P.qi_stride[k] = (int)angstepf;
+            angsteps *= s.qi_angstep_factor;
+        }
+    }
+    P.z_nbins = cfg.zlut_radialsteps;
+    P.z_angsteps = cfg.zlut_angularsteps;
+    P.z_minr = s.zlut_minradius;
+    P.z_maxr = cfg.zlut_maxradius;
+    P.g_iterations = s.gauss2D_iterations;
+    P.g_sigma = s.gauss2D_sigma;
+    offset_factor_ = default_offset_factor();
+    gain_factor_ = default_gain_factor();
+
+    // quadrant direction table, cpu_tracker.cpp:294-300
+    std::vector<float> qd(2 * P.qi_angpq);
+    for (int j = 0; j < P.qi_angpq; j++) {
+        const float ang = 0.5 * 3.141593f * (j + 0.5f) / (float)P.qi_angpq;
+        qd[2 * j] = cosf(ang);
+        qd[2 * j + 1] = sinf(ang);
+    }
+    // full-circle directions, utils.cpp:278-282
+    std::vector<float> zd(2 * P.z_angsteps);
+    for (int j = 0; j < P.z_angsteps; j++) {
+        const float ang = 2 * 3.141593f * j / (float)P.z_angsteps;
+        zd[2 * j] = cosf(ang);
+        zd[2 * j + 1] = sinf(ang);
+    }
+    // FFT twiddles e^{-2 pi i k / L}, k < L/2, L = 2 nr
+    const int L = 2 * P.qi_nr;
+    std::vector<float> tw(2 * P.qi_nr);
+    for (int k = 0; k < P.qi_nr; k++) {
+        const double a = -2.0 * M_PI * k / L;
+        tw[2 * k] = (float)cos(a);
+        tw[2 * k + 1] = (float)sin(a);
+    }
+    // QI radial bin weights, QueuedCPUTracker.cpp:119
+    const std::vector<float> rw = radial_bin_window(P.qi_nr);
+
+    CheckCuda(cudaMalloc(&d_qdirs_, qd.size() * 4), "cudaMalloc(qi dirs)");
+    CheckCuda(cudaMalloc(&d_zdirs_, zd.size() * 4), "cudaMalloc(z dirs)");
+    CheckCuda(cudaMalloc(&d_tw_, tw.size() * 4), "cudaMalloc(twiddles)");
+    CheckCuda(cudaMalloc(&d_qi_rw_, rw.size() * 4), "cudaMalloc(qi weights)");
+    CheckCuda(cudaMalloc(&d_zw_, P.z_nbins * 4), "cudaMalloc(z weights)");
+    CheckCuda(cudaMemcpy(d_qdirs_, qd.data(), qd.size() * 4, cudaMemcpyHostToDevice), "upload qi dirs");
+    CheckCuda(cudaMemcpy(d_zdirs_, zd.data(), zd.size() * 4, cudaMemcpyHostToDevice), "upload z dirs");
+    CheckCuda(cudaMemcpy(d_tw_, tw.data(), tw.size() * 4, cudaMemcpyHostToDevice), "upload twiddles");
+    CheckCuda(cudaMemcpy(d_qi_rw_, rw.data(), rw.size() * 4, cudaMemcpyHostToDevice), "upload qi weights");
+    P.qi_dirs = d_qdirs_;
+    P.z_dirs = d_zdirs_;
+    P.qi_twiddles = d_tw_;
+    P.qi_rweights = d_qi_rw_;
+
+    TrackParams probe = Params(2);
+    if (probe.smem_bytes > 227 * 1024)
+        throw std::runtime_error("ROI of " + std::to_string(W) + "x" + std::to_string(H) +
+                                 " pixels does not fit in one CTA's shared memory");
+
+    CheckCuda(cudaStreamCreateWithFlags(&lut_stream_, cudaStreamNonBlocking), "cudaStreamCreate(lut)");
+    CheckCuda(cudaEventCreateWithFlags(&lut_ready_, cudaEventDisableTiming), "cudaEventCreate");
+    for (int b = 0; b < 2; b++)
+        CheckCuda(cudaEventCreateWithFlags(&lut_stage_free_[b], cudaEventDisableTiming), "cudaEventCreate");
+    CheckCuda(cudaEventRecord(lut_ready_, lut_stream_), "cudaEventRecord");
+    AllocateSlots();
+    register_tracker(this);
+}
+
+Tracker::~Tracker()
+{
+    unregister_tracker(this);
+    DeviceGuard dg(device_);
+    {
+        std::unique_lock<std::mutex> lk(mu_);
+        try {
+            DrainAllLocked(lk);
+        } catch (...) {
+        }
+    }
+    if (lut_stream_) cudaStreamSynchronize(lut_stream_);
+    for (Slot &s : slots_) {
+        if (s.stream) cudaStreamSynchronize(s.stream);
+        cudaFreeHost(s.h_pix);
+        cudaFreeHost(s.h_jobs);
+        cudaFreeHost(s.h_res);
+        cudaFreeHost(s.h_off);
+        cudaFree(s.d_pix);
+        cudaFree(s.d_jobs);
+        cudaFree(s.d_res);
+        cudaFree(s.d_off);
+        if (s.ev_start) cudaEventDestroy(s.ev_start);
+        if (s.ev_done) cudaEventDestroy(s.ev_done);
+        if (s.stream) cudaStreamDestroy(s.stream);
+    }
+    for (int b = 0; b < 2; b++) {
+        cudaFreeHost(h_lut_stage_[b]);
+        cudaFree(d_lut_stage_[b]);
+        if (lut_stage_free_[b]) cudaEventDestroy(lut_stage_free_[b]);
+    }
+    cudaFree(d_qdirs_);
+    cudaFree(d_zdirs_);
+    cudaFree(d_tw_);
+    cudaFree(d_qi_rw_);
+    cudaFree(d_zw_);
+    cudaFree(d_lut_);
+    cudaFree(d_cmp_);
+    cudaFree(d_calib_off_);
+    cudaFree(d_calib_gain_);
+    if (lut_ready_) cudaEventDestroy(lut_ready_);
+    if (lut_stream_) cudaStreamDestroy(lut_stream_);
+}
+
+TrackParams Tracker::Params(int pdt) const
+{
+    TrackParams P = base_;
+    P.pdt = pdt;
+    P.mode = mode_;
+    P.lut = d_lut_;
+    P.lut_count = lut_count_;
+    P.lut_planes = lut_planes_;
+    P.z_weights = have_zw_ ? d_zw_ : nullptr;
+    P.cmp_scores = cmp_enabled_ ? d_cmp_ : nullptr;
+    P.calib_offset = d_calib_off_;
+    P.calib_gain = d_calib_gain_;
+    P.calib_count = (d_calib_off_ || d_calib_gain_) ? calib_count_ : 0;
+    P.offset_factor = offset_factor_;
+    P.gain_factor = gain_factor_;
+    plan_smem(P);
+    return P;
+}
+
+void Tracker::AllocateSlots()
+{
+    const QTrkSettings &s = cfg.base;
+    const int nslots = s.numThreads < 1 ? 4 : std::min(s.numThreads, 16);
+    const size_t roi_f32 = (size_t)s.width * s.height * 4;
+    const size_t budget = 64u << 20;  // pixel bytes per slot
+    batch_ = (int)std::max<size_t>(16, std::min<size_t>(4096, budget / roi_f32));
+    slot_bytes_ = (size_t)batch_ * roi_f32;
+    slots_.resize(nslots);
+    for (int i = 0; i < nslots; i++) {
+        Slot &sl = slots_[i];
+        CheckCuda(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        CheckCuda(cudaEventCreate(&sl.ev_start), "cudaEventCreate");
+        CheckCuda(cudaEventCreate(&sl.ev_done), "cudaEventCreate");
+        CheckCuda(cudaHostAlloc(&sl.h_pix, slot_bytes_, cudaHostAllocDefault), "cudaHostAlloc(pixels)");
+        CheckCuda(cudaMalloc(&sl.d_pix, slot_bytes_), "cudaMalloc(pixels)");
+        CheckCuda(cudaHostAlloc(&sl.h_jobs, sizeof(LocalizationJob) * batch_, cudaHostAllocDefault), "cudaHostAlloc");
+        CheckCuda(cudaMalloc(&sl.d_jobs, sizeof(LocalizationJob) * batch_), "cudaMalloc");
+        CheckCuda(cudaHostAlloc(&sl.h_res, sizeof(LocalizationResult) * batch_, cudaHostAllocDefault), "cudaHostAlloc");
+        CheckCuda(cudaMalloc(&sl.d_res, sizeof(LocalizationResult) * batch_), "cudaMalloc");
+        CheckCuda(cudaHostAlloc(&sl.h_off, sizeof(int64_t) * batch_, cudaHostAllocDefault), "cudaHostAlloc");
+        CheckCuda(cudaMalloc(&sl.d_off, sizeof(int64_t) * batch_), "cudaMalloc");
+        free_.push_back(i);
+    }
+}
+
+bool Tracker::IsPinned(const void *p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+void Tracker::CollectLocked()
+{
+    while (!inflight_.empty()) {
+        const int idx = inflight_.front();
+        Slot &s = slots_[idx];
+        const cudaError_t q = cudaEventQuery(s.ev_done);
+        if (q == cudaErrorNotReady) break;
+        if (q != cudaSuccess) {
+            Warn(std::string("batch of ") + std::to_string(s.count) + " ROIs failed: " + cudaGetErrorString(q));
+        } else {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, s.ev_start, s.ev_done) == cudaSuccess) stats_.gpu_ms += ms;
+            stats_.batches++;
+            stats_.rois += s.count;
+            if (stats_.latency_ms.size() < (1u << 20)) stats_.latency_ms.push_back((float)((now_s() - s.t_submit) * 1e3));
+            std::lock_guard<std::mutex> rl(res_mu_);
+            for (int i = 0; i < s.count; i++) results_.push_back(s.h_res[i]);
+        }
+        inflight_.pop_front();
+        s.count = 0;
+        s.frame = false;
+        free_.push_back(idx);
+    }
+}
+
+int Tracker::AcquireSlotLocked(std::unique_lock<std::mutex> &lk)
+{
+    const double deadline = now_s() + kWaitLimitSeconds;
+    for (;;) {
+        CollectLocked();
+        if (!free_.empty()) {
+            const int i = free_.front();
+            free_.pop_front();
+            Slot &s = slots_[i];
+            s.count = 0;
+            s.frame = false;
+            return i;
+        }
+        if (now_s() > deadline) return -1;
+        lk.unlock();
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+        lk.lock();
+    }
+}
+
+void Tracker::SubmitLocked(int idx)
+{
+    Slot &s = slots_[idx];
+    const TrackParams P = Params(s.pdt);
+    const size_t roib = (size_t)cfg.base.width * cfg.base.height * pdt_bytes(s.pdt);
+    CheckCuda(cudaStreamWaitEvent(s.stream, lut_ready_, 0), "cudaStreamWaitEvent");
+    if (!s.frame) {
+        CheckCuda(cudaEventRecord(s.ev_start, s.stream), "cudaEventRecord");
+        CheckCuda(cudaMemcpyAsync(s.d_pix, s.h_pix, roib * s.count, cudaMemcpyHostToDevice, s.stream), "H2D pixels");
+    }
+    CheckCuda(cudaMemcpyAsync(s.d_jobs, s.h_jobs, sizeof(LocalizationJob) * s.count, cudaMemcpyHostToDevice, s.stream),
+              "H2D jobs");
+    if (s.frame)
+        CheckCuda(cudaMemcpyAsync(s.d_off, s.h_off, sizeof(int64_t) * s.count, cudaMemcpyHostToDevice, s.stream),
+                  "H2D offsets");
+    CheckCuda(launch_localize(P, s.d_pix, s.pitch, (int64_t)roib, s.frame ? s.d_off : nullptr, s.d_jobs, s.count,
+                              s.d_res, s.stream),
+              "localize kernel launch");
+    launches_++;
+    CheckCuda(cudaMemcpyAsync(s.h_res, s.d_res, sizeof(LocalizationResult) * s.count, cudaMemcpyDeviceToHost, s.stream),
+              "D2H results");
+    CheckCuda(cudaEventRecord(s.ev_done, s.stream), "cudaEventRecord");
+    s.t_submit = now_s();
+    inflight_.push_back(idx);
+}
+
+void Tracker::DrainAllLocked(std::unique_lock<std::mutex> &lk)
+{
+    if (filling_ >= 0) {
+        if (slots_[filling_].count > 0) {
+            SubmitLocked(filling_);
+        } else {
+            free_.push_back(filling_);
+        }
+        filling_ = -1;
+    }
+    const double deadline = now_s() + kWaitLimitSeconds;
+    for (;;) {
+        CollectLocked();
+        if (inflight_.empty()) return;
+        if (now_s() > deadline) throw std::runtime_error("timed out waiting for the GPU to finish queued batches");
+        lk.unlock();
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+        lk.lock();
+    }
+}
+
+void Tracker::WaitIdleForReconfigure()
+{
+    std::unique_lock<std::mutex> lk(mu_);
+    DrainAllLocked(lk);
+    CheckCuda(cudaStreamSynchronize(lut_stream_), "cudaStreamSynchronize(lut)");
+}
+
+// QueuedCPUTracker::SetLocalizationMode waits for idle (QueuedCPUTracker.cpp:513-517).
+void Tracker::SetLocalizationMode(LocMode_t mode)
+{
+    DeviceGuard dg(device_);
+    const int unsupported = LT_XCor1D | LT_ZLUTAlign | LT_FourierLUT | LT_LocalizeZWeighted;
+    if (mode & unsupported)
+        Warn("localization mode bits 0x" + [&] {
+            std::ostringstream o;
+            o << std::hex << (mode & unsupported);
+            return o.str();
+        }() + " (XCor1D/ZLUTAlign/FourierLUT/LocalizeZWeighted) are not supported and were ignored");
+    WaitIdleForReconfigure();
+    std::lock_guard<std::mutex> lk(mu_);
+    mode_ = mode & ~unsupported;
+}
+
+// QueuedCPUTracker::SetPixelCalibrationImages, QueuedCPUTracker.cpp:165-196: per-bead images of
+// width*height*zlut_count floats; a null pointer removes that image.
+void Tracker::SetPixelCalibrationImages(const float *offset, const float *gain)
+{
+    DeviceGuard dg(device_);
+    WaitIdleForReconfigure();
+    std::lock_guard<std::mutex> lk(mu_);
+    if (lut_count_ <= 0) {
+        Warn("SetPixelCalibrationImages needs a Z-LUT (its bead count sizes the images); ignored");
+        return;
+    }
+    const size_t n = (size_t)cfg.base.width * cfg.base.height * lut_count_;
+    auto upd = [&](float *&dptr, const float *src) {
+        if (src) {
+            if (!dptr) CheckCuda(cudaMalloc(&dptr, n * 4), "cudaMalloc(calibration)");
+            CheckCuda(cudaMemcpy(dptr, src, n * 4, cudaMemcpyHostToDevice), "upload calibration");
+        } else if (dptr) {
+            cudaFree(dptr);
+            dptr = nullptr;
+        }
+    };
+    upd(d_calib_off_, offset);
+    upd(d_calib_gain_, gain);
+    calib_count_ = lut_count_;
+}
+
+void Tracker::SetPixelCalibrationFactors(float offsetFactor, float gainFactor)
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    offset_factor_ = offsetFactor;
+    gain_factor_ = gainFactor;
+}
+
+// QueuedCPUTracker::ScheduleLocalization, QueuedCPUTracker.cpp:435-456: the ROI rows are copied
+// before returning, so the caller may reuse its buffer at once.
+void Tracker::ScheduleLocalization(const void *data, int pitch, int pdt, const LocalizationJob *job)
+{
+    if (!data || !job) throw std::invalid_argument("ScheduleLocalization: null data or job");
+    if (pdt < 0 || pdt > 2) throw std::invalid_argument("ScheduleLocalization: unknown pixel data type");
+    DeviceGuard dg(device_);
+    const int W = cfg.base.width, H = cfg.base.height;
+    const size_t rowb = (size_t)W * pdt_bytes(pdt), roib = rowb * H;
+    std::unique_lock<std::mutex> lk(mu_);
+    if (filling_ >= 0) {
+        Slot &s = slots_[filling_];
+        if (s.count > 0 && s.pdt != pdt) {
+            SubmitLocked(filling_);
+            filling_ = -1;
+        }
+    }
+    if (filling_ < 0) {
+        filling_ = AcquireSlotLocked(lk);
+        if (filling_ < 0) {
+            Warn("ScheduleLocalization: timed out waiting for a free batch slot; job dropped");
+            return;
+        }
+        Slot &s = slots_[filling_];
+        s.pdt = pdt;
+        s.frame = false;
+        s.pitch = (int)rowb;
+    }
+    Slot &s = slots_[filling_];
+    uint8_t *dst = s.h_pix + (size_t)s.count * roib;
+    const uint8_t *src = static_cast<const uint8_t *>(data);
+    if ((size_t)pitch == rowb) {
+        std::memcpy(dst, src, roib);
+    } else {
+        for (int y = 0; y < H; y++) std::memcpy(dst + y * rowb, src + (size_t)y * pitch, rowb);
+    }
+    s.h_jobs[s.count] = *job;
+    s.count++;
+    if (s.count == batch_) {
+        SubmitLocked(filling_);
+        filling_ = -1;
+    }
+}
+
+// QueuedTracker::ScheduleFrame, QueuedTracker.cpp:91-111: ROIs outside the frame are skipped,
+// zlutIndex = i + job.zlutIndex. Here the frame rows are copied to the device once and the
+// kernel crops the ROIs from them (no host-side cropping).
+int Tracker::ScheduleFrame(const void *img, int pitch, int width, int height, const ROIPosition *pos, int n, int pdt,
+                           const LocalizationJob *job)
+{
+    if (!img || !job || (n > 0 && !pos)) throw std::invalid_argument("ScheduleFrame: null argument");
+    if (pdt < 0 || pdt > 2) throw std::invalid_argument("ScheduleFrame: unknown pixel data type");
+    DeviceGuard dg(device_);
+    const int W = cfg.base.width, H = cfg.base.height, bpp = pdt_bytes(pdt);
+    std::vector<int> idx;
+    idx.reserve(n);
+    int skipped = 0;
+    for (int i = 0; i < n; i++) {
+        const ROIPosition &p = pos[i];
+        if (p.x < 0 || p.y < 0 || p.x + W > width || p.y + H > height) {
+            skipped++;
+            continue;
+        }
+        idx.push_back(i);
+    }
+    if (skipped) Warn("ScheduleFrame: skipped " + std::to_string(skipped) + " ROI(s) outside the frame");
+    if (idx.empty()) return 0;
+
+    // Group ROIs into row bands that fit a slot; one band keeps the caller's order.
+    int minx = width, maxx = 0;
+    for (int i : idx) {
+        minx = std::min(minx, pos[i].x);
+        maxx = std::max(maxx, pos[i].x + W);
+    }
+    const size_t dpitch = (((size_t)(maxx - minx) * bpp) + 15) & ~(size_t)15;
+    auto span_bytes = [&](int y0, int y1) { return (size_t)(y1 - y0) * dpitch; };
+    std::vector<std::vector<int>> bands;
+    {
+        int y0 = height, y1 = 0;
+        for (int i : idx) {
+            y0 = std::min(y0, pos[i].y);
+            y1 = std::max(y1, pos[i].y + H);
+        }
+        if (span_bytes(y0, y1) <= slot_bytes_ && (int)idx.size() <= batch_) {
+            bands.push_back(idx);
+        } else {
+            std::vector<int> sorted = idx;
+            std::stable_sort(sorted.begin(), sorted.end(), [&](int a, int b) { return pos[a].y < pos[b].y; });
+            std::vector<int> cur;
+            int by0 = 0, by1 = 0;
+            for (int i : sorted) {
+                if (cur.empty()) {
+                    by0 = pos[i].y;
+                    by1 = pos[i].y + H;
+                    cur.push_back(i);
+                    continue;
+                }
+                const int ny1 = std::max(by1, pos[i].y + H);
+                if (span_bytes(by0, ny1) <= slot_bytes_ && (int)cur.size() < batch_) {
+                    by1 = ny1;
+                    cur.push_back(i);
+                } else {
+                    bands.push_back(cur);
+                    cur.assign(1, i);
+                    by0 = pos[i].y;
+                    by1 = pos[i].y + H;
+                }
+            }
+            if (!cur.empty()) bands.push_back(cur);
+        }
+    }
+    if (span_bytes(0, H) > slot_bytes_) {
+        // A single ROI row span does not fit a slot (very wide frame): crop on the host.
+        int count = 0;
+        for (int i : idx) {
+            LocalizationJob j = *job;
+            j.zlutIndex = i + job->zlutIndex;
+            ScheduleLocalization(static_cast<const uint8_t *>(img) + (size_t)pitch * pos[i].y + (size_t)pos[i].x * bpp,
+                                 pitch, pdt, &j);
+            count++;
+        }
+        return count;
+    }
+
+    const bool pinned = IsPinned(img);
+    std::vector<cudaEvent_t> copies;
+    std::unique_lock<std::mutex> lk(mu_);
+    if (filling_ >= 0) {  // keep FIFO order with earlier single-ROI jobs
+        if (slots_[filling_].count > 0)
+            SubmitLocked(filling_);
+        else
+            free_.push_back(filling_);
+        filling_ = -1;
+    }
+    int count = 0;
+    for (const std::vector<int> &band : bands) {
+        int y0 = height, y1 = 0;
+        for (int i : band) {
+            y0 = std::min(y0, pos[i].y);
+            y1 = std::max(y1, pos[i].y + H);
+        }
+        const int si = AcquireSlotLocked(lk);
+        if (si < 0) {
+            Warn("ScheduleFrame: timed out waiting for a free batch slot; ROIs dropped");
+            break;
+        }
+        Slot &s = slots_[si];
+        s.frame = true;
+        s.pdt = pdt;
+        s.pitch = (int)dpitch;
+        s.count = (int)band.size();
+        for (int k = 0; k < s.count; k++) {
+            const int i = band[k];
+            s.h_off[k] = (int64_t)(pos[i].y - y0) * (int64_t)dpitch + (int64_t)(pos[i].x - minx) * bpp;
+            s.h_jobs[k] = *job;
+            s.h_jobs[k].zlutIndex = i + job->zlutIndex;
+        }
+        CheckCuda(cudaEventRecord(s.ev_start, s.stream), "cudaEventRecord");
+        const uint8_t *src = static_cast<const uint8_t *>(img) + (size_t)y0 * pitch + (size_t)minx * bpp;
+        CheckCuda(cudaMemcpy2DAsync(s.d_pix, dpitch, src, (size_t)pitch, (size_t)(maxx - minx) * bpp, (size_t)(y1 - y0),
+                                    cudaMemcpyHostToDevice, s.stream),
+                  "H2D frame rows");
+        if (pinned) {
+            cudaEvent_t ev;
+            CheckCuda(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+            CheckCuda(cudaEventRecord(ev, s.stream), "cudaEventRecord");
+            copies.push_back(ev);
+        }
+        SubmitLocked(si);
+        count += s.count;
+    }
+    lk.unlock();
+    // A pinned source is read by DMA after cudaMemcpy2DAsync returns: wait until it has been
+    // read so the caller may reuse the frame buffer (pageable sources are staged before return).
+    for (cudaEvent_t ev : copies) {
+        cudaEventSynchronize(ev);
+        cudaEventDestroy(ev);
+    }
+    return count;
+}
+
+void Tracker::ClearResults()
+{
+    std::lock_guard<std::mutex> rl(res_mu_);
+    results_.clear();
+}
+
+void Tracker::Flush()
+{
+    DeviceGuard dg(device_);
+    std::lock_guard<std::mutex> lk(mu_);
+    if (filling_ >= 0 && slots_[filling_].count > 0) {
+        SubmitLocked(filling_);
+        filling_ = -1;
+    }
+}
+
+// QueuedCPUTracker::SetRadialZLUT, QueuedCPUTracker.cpp:364-391: [count][planes][zlut_radialsteps]
+// floats, zero-filled when data is null.
+void Tracker::SetRadialZLUT(const float *data, int count, int planes)
+{
+    DeviceGuard dg(device_);
+    WaitIdleForReconfigure();
+    std::lock_guard<std::mutex> lk(mu_);
+    cudaFree(d_lut_);
+    cudaFree(d_cmp_);
+    d_lut_ = nullptr;
+    d_cmp_ = nullptr;
+    const int res = cfg.zlut_radialsteps;
+    const size_t total = (size_t)std::max(count, 0) * std::max(planes, 0) * res;
+    if (total > 0) {
+        CheckCuda(cudaMalloc(&d_lut_, total * 4), "cudaMalloc(Z-LUT)");
+        if (data)
+            CheckCuda(cudaMemcpy(d_lut_, data, total * 4, cudaMemcpyHostToDevice), "upload Z-LUT");
+        else
+            CheckCuda(cudaMemset(d_lut_, 0, total * 4), "clear Z-LUT");
+        CheckCuda(cudaMalloc(&d_cmp_, (size_t)count * planes * 4), "cudaMalloc(compare profiles)");
+        CheckCuda(cudaMemset(d_cmp_, 0, (size_t)count * planes * 4), "clear compare profiles");
+        lut_count_ = count;
+        lut_planes_ = planes;
+        if (Params(2).smem_bytes > 227 * 1024) {
+            cudaFree(d_lut_);
+            cudaFree(d_cmp_);
+            d_lut_ = nullptr;
+            d_cmp_ = nullptr;
+            lut_count_ = lut_planes_ = 0;
+            throw std::invalid_argument("Z-LUT with " + std::to_string(planes) +
+                                        " planes does not fit the per-CTA score buffer");
+        }
+    } else {
+        lut_count_ = lut_planes_ = 0;
+    }
+    CheckCuda(cudaEventRecord(lut_ready_, lut_stream_), "cudaEventRecord");
+}
+
+void Tracker::GetRadialZLUT(float *dst)
+{
+    if (!dst) throw std::invalid_argument("GetRadialZLUT: null destination");
+    DeviceGuard dg(device_);
+    std::lock_guard<std::mutex> lk(mu_);
+    CheckCuda(cudaStreamSynchronize(lut_stream_), "cudaStreamSynchronize(lut)");
+    const size_t total = (size_t)lut_count_ * lut_planes_ * cfg.zlut_radialsteps;
+    if (total) CheckCuda(cudaMemcpy(dst, d_lut_, total * 4, cudaMemcpyDeviceToHost), "download Z-LUT");
+}
+
+void Tracker::GetRadialZLUTSize(int &count, int &planes, int &radialsteps) const
+{
+    count = lut_count_;
+    planes = lut_planes_;
+    radialsteps = cfg.zlut_radialsteps;
+}
+
+// QueuedCPUTracker::SetRadialWeights, QueuedCPUTracker.cpp:393-406 (null clears them).
+void Tracker::SetRadialWeights(const float *w)
+{
+    DeviceGuard dg(device_);
+    WaitIdleForReconfigure();
+    std::lock_guard<std::mutex> lk(mu_);
+    if (w) {
+        CheckCuda(cudaMemcpy(d_zw_, w, (size_t)cfg.zlut_radialsteps * 4, cudaMemcpyHostToDevice), "upload weights");
+        have_zw_ = true;
+    } else {
+        have_zw_ = false;
+    }
+}
+
+void Tracker::EnableRadialZLUTCompareProfile(bool enabled)
+{
+    DeviceGuard dg(device_);
+    WaitIdleForReconfigure();
+    std::lock_guard<std::mutex> lk(mu_);
+    cmp_enabled_ = enabled;
+}
+
+void Tracker::GetRadialZLUTCompareProfile(float *dst)
+{
+    if (!dst) throw std::invalid_argument("GetRadialZLUTCompareProfile: null destination");
+    DeviceGuard dg(device_);
+    WaitIdleForReconfigure();
+    std::lock_guard<std::mutex> lk(mu_);
+    if (d_cmp_ && lut_count_ * lut_planes_ > 0)
+        CheckCuda(cudaMemcpy(dst, d_cmp_, (size_t)lut_count_ * lut_planes_ * 4, cudaMemcpyDeviceToHost),
+                  "download compare profiles");
+}
+
+void Tracker::BeginLUT(uint32_t flags)
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    if (flags & (BUILDLUT_IMAGELUT | BUILDLUT_FOURIER))
+        Warn("BeginLUT: BUILDLUT_IMAGELUT and BUILDLUT_FOURIER are not supported and were ignored");
+    if (flags & BUILDLUT_BIASCORRECT) Warn("BeginLUT: BUILDLUT_BIASCORRECT is not supported and was ignored");
+    lut_flags_ = flags;
+}
+
+// QueuedCPUTracker::BuildLUT, QueuedCPUTracker.cpp:580-646: `data` holds one ROI per bead,
+// bead i at data + pitch*height*i. The rows are staged (double-buffered) and the profiles are
+// accumulated into the device LUT by one kernel launch per plane.
+void Tracker::BuildLUT(const void *data, int pitch, int pdt, int plane, const vector2f *known_pos)
+{
+    if (!data) throw std::invalid_argument("BuildLUT: null data");
+    if (pdt < 0 || pdt > 2) throw std::invalid_argument("BuildLUT: unknown pixel data type");
+    DeviceGuard dg(device_);
+    std::lock_guard<std::mutex> lk(mu_);
+    if (!d_lut_ || lut_count_ <= 0) {
+        Warn("BuildLUT: no Z-LUT allocated (call SetRadialZLUT first); ignored");
+        return;
+    }
+    if (plane < 0 || plane >= lut_planes_) {
+        Warn("BuildLUT: plane " + std::to_string(plane) + " out of range; ignored");
+        return;
+    }
+    const int W = cfg.base.width, H = cfg.base.height, nb = lut_count_;
+    const size_t rowb = (size_t)W * pdt_bytes(pdt);
+    if ((size_t)pitch < rowb) throw std::invalid_argument("BuildLUT: pitch smaller than a row");
+    const size_t bytes = (size_t)pitch * ((size_t)H * nb - 1) + rowb;
+    const size_t kp_off = (bytes + 15) & ~(size_t)15;
+    const size_t need = kp_off + sizeof(float2) * nb;
+    if (need > lut_stage_bytes_) {
+        CheckCuda(cudaStreamSynchronize(lut_stream_), "cudaStreamSynchronize(lut)");
+        for (int b = 0; b < 2; b++) {
+            cudaFreeHost(h_lut_stage_[b]);
+            cudaFree(d_lut_stage_[b]);
+            h_lut_stage_[b] = d_lut_stage_[b] = nullptr;
+            CheckCuda(cudaHostAlloc(&h_lut_stage_[b], need, cudaHostAllocDefault), "cudaHostAlloc(LUT stage)");
+            CheckCuda(cudaMalloc(&d_lut_stage_[b], need), "cudaMalloc(LUT stage)");
+        }
+        lut_stage_bytes_ = need;
+    }
+    const int b = lut_stage_next_;
+    lut_stage_next_ ^= 1;
+    CheckCuda(cudaEventSynchronize(lut_stage_free_[b]), "cudaEventSynchronize");
+    std::memcpy(h_lut_stage_[b], data, bytes);
+    if (known_pos) std::memcpy(h_lut_stage_[b] + kp_off, known_pos, sizeof(float2) * nb);
+    CheckCuda(cudaMemcpyAsync(d_lut_stage_[b], h_lut_stage_[b], known_pos ? need : bytes, cudaMemcpyHostToDevice,
+                              lut_stream_),
+              "H2D LUT stack");
+    TrackParams P = Params(pdt);
+    P.mode = 0;  // BuildLUT runs COM/QI/profile without the per-job mode bits
+    CheckCuda(launch_build_lut(P, d_lut_stage_[b], pitch, nb, plane,
+                               known_pos ? reinterpret_cast<const float2 *>(d_lut_stage_[b] + kp_off) : nullptr,
+                               (lut_flags_ & BUILDLUT_NORMALIZE) != 0, d_lut_, lut_stream_),
+              "BuildLUT kernel launch");
+    launches_++;
+    CheckCuda(cudaEventRecord(lut_stage_free_[b], lut_stream_), "cudaEventRecord");
+    CheckCuda(cudaEventRecord(lut_ready_, lut_stream_), "cudaEventRecord");
+}
+
+// QueuedCPUTracker::FinalizeLUT, QueuedCPUTracker.cpp:648-659.
+void Tracker::FinalizeLUT()
+{
+    DeviceGuard dg(device_);
+    std::lock_guard<std::mutex> lk(mu_);
+    if (d_lut_) {
+        CheckCuda(launch_finalize_lut(d_lut_, lut_count_ * lut_planes_, cfg.zlut_radialsteps, lut_stream_),
+                  "FinalizeLUT kernel launch");
+        launches_++;
+    }
+    CheckCuda(cudaEventRecord(lut_ready_, lut_stream_), "cudaEventRecord");
+    CheckCuda(cudaStreamSynchronize(lut_stream_), "cudaStreamSynchronize(lut)");
+}
+
+int Tracker::GetResultCount()
+{
+    DeviceGuard dg(device_);
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        CollectLocked();
+    }
+    std::lock_guard<std::mutex> rl(res_mu_);
+    return (int)results_.size();
+}
+
+// FIFO order, like QueuedCUDATracker::FetchResults (cudatrack/QueuedCUDATracker.cu:726-737).
+int Tracker::FetchResults(LocalizationResult *dst, int maxResults)
+{
+    if (!dst || maxResults <= 0) return 0;
+    DeviceGuard dg(device_);
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        CollectLocked();
+    }
+    std::lock_guard<std::mutex> rl(res_mu_);
+    int n = 0;
+    while (n < maxResults && !results_.empty()) {
+        dst[n++] = results_.front();
+        results_.pop_front();
+    }
+    return n;
+}
+
+int Tracker::GetQueueLength(int *maxQueueLen)
+{
+    DeviceGuard dg(device_);
+    std::lock_guard<std::mutex> lk(mu_);
+    CollectLocked();
+    int n = filling_ >= 0 ? slots_[filling_].count : 0;
+    for (int i : inflight_) n += slots_[i].count;
+    if (maxQueueLen) *maxQueueLen = (int)slots_.size() * batch_;
+    return n;
+}
+
+bool Tracker::IsIdle() { return GetQueueLength(nullptr) == 0; }
+
+std::string Tracker::GetProfileReport()
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    std::ostringstream o;
+    o << "B200 tracker (device " << device_ << "): " << stats_.batches << " batches, " << stats_.rois << " ROIs";
+    if (stats_.gpu_ms > 0) o << ", " << stats_.gpu_ms << " ms on the GPU streams";
+    if (!stats_.latency_ms.empty()) {
+        std::vector<float> l = stats_.latency_ms;
+        std::sort(l.begin(), l.end());
+        auto pct = [&](double p) { return l[std::min(l.size() - 1, (size_t)(p * (l.size() - 1) + 0.5))]; };
+        o << "; batch latency p50 " << pct(0.5) << " ms, p99 " << pct(0.99) << " ms";
+    }
+    o << "; batch size " << batch_ << ", " << slots_.size() << " streams, " << launches_.load() << " kernel launches";
+    return o.str();
+}
+
+std::string Tracker::GetWarnings()
+{
+    std::lock_guard<std::mutex> lk(warn_mu_);
+    std::string w;
+    w.swap(warnings_);
+    return w;
+}
+
+int Tracker::LocalizeDevice(const void *d_pixels, int pitch, int64_t roi_stride, int pdt, int count,
+                            const LocalizationJob *d_jobs, LocalizationResult *d_results, cudaStream_t stream)
+{
+    if (!d_pixels || !d_results || count < 0 || pdt < 0 || pdt > 2) {
+        Warn("QTrkB200LocalizeDevice: invalid argument");
+        return -1;
+    }
+    if (pitch < cfg.base.width * pdt_bytes(pdt)) {
+        Warn("QTrkB200LocalizeDevice: pitch smaller than a row");
+        return -2;
+    }
+    DeviceGuard dg(device_);
+    TrackParams P;
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        P = Params(pdt);
+    }
+    CheckCuda(cudaStreamWaitEvent(stream, lut_ready_, 0), "cudaStreamWaitEvent");
+    CheckCuda(launch_localize(P, static_cast<const uint8_t *>(d_pixels), pitch, roi_stride, nullptr, d_jobs, count,
+                              d_results, stream),
+              "localize kernel launch");
+    launches_++;
+    return 0;
+}
+
+}  // namespace qtrk

@@ -1,0 +1,165 @@
+"""Seeded synthetic bead images for the five benchmark configurations.
+
+No public dataset is involved: the reference measures on its own generated images
+(cputrack-test/SharedTests.h:343-416 renders ROIs from a LUT and adds Poisson noise).
+Here the radial bead profile is the analytic family
+
+    p_z(r) = exp(-r^2 / (2 (4 + 0.1 z)^2)) * cos(2 pi r / (6 + 0.05 z))
+
+rendered at pixel centres (r measured from the bead centre in pixel coordinates, the
+convention of the reference's samplers), scaled, clamped at zero and Poisson-sampled
+with numpy's PCG64 generator seeded per configuration. The Z-LUT is built through the
+tracker's own BeginLUT/BuildLUT/FinalizeLUT from noise-free images clamped the same way
+(cputrack-test/SharedTests.h:35-65 builds its LUTs the same way).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import abi
+
+
+def profile(r: np.ndarray, zp: np.ndarray | float) -> np.ndarray:
+    s = 4.0 + 0.1 * zp
+    per = 6.0 + 0.05 * zp
+    return np.exp(-r * r / (2 * s * s)) * np.cos(2 * np.pi * r / per)
+
+
+def render(w: int, h: int, cx: np.ndarray, cy: np.ndarray, zp: np.ndarray, bg: float, amp: float) -> np.ndarray:
+    """Noise-free expected pixel values, shape (n, h, w), float64, clamped at 0."""
+    ys = np.arange(h, dtype=np.float64)[None, :, None]
+    xs = np.arange(w, dtype=np.float64)[None, None, :]
+    r = np.sqrt((xs - cx[:, None, None]) ** 2 + (ys - cy[:, None, None]) ** 2)
+    lam = bg + amp * profile(r, np.asarray(zp, np.float64)[:, None, None])
+    return np.maximum(lam, 0.0)
+
+
+@dataclass
+class Workload:
+    name: str
+    settings: abi.QTrkSettings
+    mode: int
+    rois: np.ndarray            # (n, h, w) u8/u16/f32
+    true_xyz: np.ndarray        # (n, 3): x, y in pixels, z in LUT planes
+    lut_stack: np.ndarray | None = None   # (planes, 1, h, w) noise-free images for BuildLUT
+    lut_known_pos: np.ndarray | None = None
+    extra: dict = field(default_factory=dict)
+
+
+def settings_config1(**kw) -> abi.QTrkSettings:
+    """60x60 ROIs, QI radius 3-28 px, 64 angular steps per quadrant, 40 radial steps
+    (rounded to 32 by QTrkComputedConfig::Update, cputrack/QueuedTracker.cpp:20), Z-LUT
+    40 bins over radius 3-28, 4 QI iterations."""
+    s = abi.settings(width=60, height=60, qi_iterations=4, qi_minradius=3.0, qi_roi_coverage=28 / 30,
+                     qi_radial_coverage=1.6, qi_angular_coverage=64.5 * 4 / (2 * np.pi * 28),
+                     zlut_minradius=3.0, zlut_roi_coverage=28 / 30, zlut_radial_coverage=1.6 + 1e-4,
+                     zlut_angular_coverage=0.7, cuda_device=-2, numThreads=-1)
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
+
+
+def settings_config2(**kw) -> abi.QTrkSettings:
+    """100x100 ROIs, radius 3-47 px: QI 64 radial steps x 51 angular steps per quadrant,
+    Z-LUT 64 bins x 206 angles, 4 QI iterations."""
+    s = abi.settings(width=100, height=100, qi_iterations=4, qi_minradius=3.0, qi_roi_coverage=0.94,
+                     qi_radial_coverage=1.4, qi_angular_coverage=0.7, zlut_minradius=3.0, zlut_roi_coverage=0.94,
+                     zlut_radial_coverage=64.5 / 44.0, zlut_angular_coverage=0.7, cuda_device=-2, numThreads=-1)
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
+
+
+MODE_QI_Z = abi.LT_QI | abi.LT_LocalizeZ | abi.LT_NormalizeProfile
+
+
+def config1(n: int = 1000, seed: int = 1) -> Workload:
+    """1,000 ROIs 60x60 f32: centre (30,30)+U(+-3), z ~ U[5,45] planes, 10 + 100 p_z(r) + Poisson;
+    Z-LUT 50 planes, plane k <-> z = k."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    w = h = 60
+    cx = 30 + rng.uniform(-3, 3, n)
+    cy = 30 + rng.uniform(-3, 3, n)
+    z = rng.uniform(5, 45, n)
+    rois = np.empty((n, h, w), np.float32)
+    for a in range(0, n, 2048):
+        b = min(n, a + 2048)
+        lam = render(w, h, cx[a:b], cy[a:b], z[a:b], 10.0, 100.0)
+        rois[a:b] = rng.poisson(lam).astype(np.float32)
+    planes = 50
+    kz = np.arange(planes, dtype=np.float64)
+    stack = render(w, h, np.full(planes, w / 2), np.full(planes, h / 2), kz, 10.0, 100.0).astype(np.float32)
+    return Workload("config1-60x60-f32", settings_config1(), MODE_QI_Z, rois, np.stack([cx, cy, z], 1),
+                    stack[:, None], np.array([[w / 2, h / 2]], np.float32))
+
+
+def config2(n: int = 10000, seed: int = 2) -> Workload:
+    """10,000 ROIs 100x100 u16 (12-bit): 200 + 2000 p(r; 0.25 z) + Poisson, clipped to 4095;
+    centre (50,50)+U(+-3), z ~ U[10,190] planes; Z-LUT 200 planes x 64 bins, plane k <-> 0.25 k."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    w = h = 100
+    cx = 50 + rng.uniform(-3, 3, n)
+    cy = 50 + rng.uniform(-3, 3, n)
+    z = rng.uniform(10, 190, n)
+    rois = np.empty((n, h, w), np.uint16)
+    for a in range(0, n, 1024):
+        b = min(n, a + 1024)
+        lam = render(w, h, cx[a:b], cy[a:b], 0.25 * z[a:b], 200.0, 2000.0)
+        rois[a:b] = np.minimum(rng.poisson(lam), 4095).astype(np.uint16)
+    planes = 200
+    kz = 0.25 * np.arange(planes, dtype=np.float64)
+    stack = render(w, h, np.full(planes, w / 2), np.full(planes, h / 2), kz, 200.0, 2000.0).astype(np.float32)
+    return Workload("config2-100x100-u16", settings_config2(), MODE_QI_Z, rois, np.stack([cx, cy, z], 1),
+                    stack[:, None], np.array([[w / 2, h / 2]], np.float32))
+
+
+def gaussian_spots(n: int, w: int, cx, cy, sigma: float, photons, bg: float) -> np.ndarray:
+    """Integrated Gaussian spot (GenerateGaussianSpotImage, cputrack/utils.cpp:393-402) in FP64."""
+    from math import sqrt
+
+    from scipy.special import erf  # scipy is present in this image
+
+    xs = np.arange(w, dtype=np.float64)
+    k = 1.0 / sqrt(2.0) / sigma
+    dx = 0.5 * (erf((xs[None, :] - cx[:, None] + 0.5) * k) - erf((xs[None, :] - cx[:, None] - 0.5) * k))
+    dy = 0.5 * (erf((xs[None, :] - cy[:, None] + 0.5) * k) - erf((xs[None, :] - cy[:, None] - 0.5) * k))
+    return bg + photons[:, None, None] * dy[:, :, None] * dx[:, None, :]
+
+
+def config3(n: int = 100000, seed: int = 3) -> Workload:
+    """100,000 ROIs 16x16 f32: integrated Gaussian sigma 1.5, photons log-U[500,5000],
+    background 10 photons/px, Poisson; centre 8 + U(+-2)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    w = 16
+    cx = 8 + rng.uniform(-2, 2, n)
+    cy = 8 + rng.uniform(-2, 2, n)
+    ph = np.exp(rng.uniform(np.log(500), np.log(5000), n))
+    rois = np.empty((n, w, w), np.float32)
+    for a in range(0, n, 8192):
+        b = min(n, a + 8192)
+        rois[a:b] = rng.poisson(gaussian_spots(b - a, w, cx[a:b], cy[a:b], 1.5, ph[a:b], 10.0)).astype(np.float32)
+    s = abi.settings(width=16, height=16, gauss2D_sigma=1.5, gauss2D_iterations=8, cuda_device=-2, numThreads=-1,
+                     qi_minradius=1, zlut_minradius=1)
+    return Workload("config3-16x16-gauss", s, abi.LT_Gaussian2D, rois,
+                    np.stack([cx, cy, np.zeros(n)], 1), extra={"photons": ph, "bg": 10.0, "sigma": 1.5})
+
+
+def config4_stack(nbeads: int = 256, planes: int = 200, seed: int = 4, noise: bool = True) -> tuple:
+    """Calibration stack: nbeads x planes ROIs of 80x80 u16, bead b at 40 + U(+-2) (fixed over z),
+    plane k <-> profile parameter 0.25 k; 200 + 2000 p + Poisson, clipped to 4095.
+    Returns (settings, stack (planes, nbeads, 80, 80) u16, centres (nbeads, 2))."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    w = 80
+    cx = 40 + rng.uniform(-2, 2, nbeads)
+    cy = 40 + rng.uniform(-2, 2, nbeads)
+    stack = np.empty((planes, nbeads, w, w), np.uint16)
+    for k in range(planes):
+        lam = render(w, w, cx, cy, np.full(nbeads, 0.25 * k), 200.0, 2000.0)
+        img = rng.poisson(lam) if noise else np.rint(lam)
+        stack[k] = np.minimum(img, 4095).astype(np.uint16)
+    s = abi.settings(width=80, height=80, qi_iterations=4, qi_minradius=3.0, qi_roi_coverage=0.9,
+                     qi_radial_coverage=1.4, qi_angular_coverage=0.7, zlut_minradius=3.0, zlut_roi_coverage=0.9,
+                     zlut_radial_coverage=48.5 / 33.0, zlut_angular_coverage=0.7, cuda_device=-2, numThreads=-1)
+    return s, stack, np.stack([cx, cy], 1).astype(np.float32)

@@ -1,0 +1,312 @@
+"""GPU parity: libqtrk_b200 (through its C ABI) against the reference CPU tracker.
+
+The oracle is the reference's own QueuedCPUTracker (oracle/_ref, when built) and the
+committed golden fixtures it produced (tests/golden/). Tolerances (north star):
+COM 1e-4 px, QI x/y 1e-3 px, Z 0.01 plane; error flags must be identical.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from golden_io import load
+from qtrk_b200 import abi, synth
+from qtrk_b200.tracker import QTrkInstance
+
+pytestmark = pytest.mark.gpu
+
+TOL_COM = 1e-4
+TOL_QI = 1e-3
+TOL_Z = 0.01
+
+
+def make_tracker(settings, mode, lut=None):
+    t = QTrkInstance(settings)
+    if lut is not None:
+        t.SetRadialZLUT(lut)
+    t.SetLocalizationMode(mode)
+    return t
+
+
+def check_results(gpu, pos, com, err, mean=None, tol_xy=TOL_QI, tol_z=TOL_Z):
+    assert np.abs(gpu["pos"][:, 0] - pos[:, 0]).max() < tol_xy
+    assert np.abs(gpu["pos"][:, 1] - pos[:, 1]).max() < tol_xy
+    assert np.abs(gpu["pos"][:, 2] - pos[:, 2]).max() < tol_z
+    assert np.abs(gpu["firstGuess"] - com).max() < TOL_COM
+    assert (gpu["error"] == err).all()
+    if mean is not None:
+        np.testing.assert_allclose(gpu["imageMean"], mean, rtol=1e-6)
+
+
+def test_golden_config1_qi_z():
+    g = load("config1_60x60_f32.npz")
+    with make_tracker(g["settings"], int(g["mode"]), g["lut"]) as t:
+        r = t.Localize(g["rois"].astype(np.float32))
+        assert t.KernelLaunchCount() >= 1
+    check_results(r, g["pos"], g["com"], g["error"], g["mean"])
+
+
+def test_golden_config1_com_and_qi_only():
+    g = load("config1_60x60_f32.npz")
+    rois = g["rois"].astype(np.float32)
+    with make_tracker(g["settings"], abi.LT_OnlyCOM) as t:
+        r = t.Localize(rois)
+    assert np.abs(r["pos"][:, :2] - g["com_only_pos"][:, :2]).max() < TOL_COM
+    assert (r["pos"][:, 2] == 0).all()
+    with make_tracker(g["settings"], abi.LT_QI) as t:
+        r = t.Localize(rois)
+    check_results(r, g["qi_only_pos"], g["qi_only_com"], g["qi_only_error"])
+
+
+def test_golden_config2_u16():
+    g = load("config2_100x100_u16.npz")
+    with make_tracker(g["settings"], int(g["mode"]), g["lut"]) as t:
+        r = t.Localize(g["rois"])
+    check_results(r, g["pos"], g["com"], g["error"], g["mean"])
+
+
+def test_golden_gaussian_4p():
+    g = load("config3_16x16_gauss.npz")
+    with make_tracker(g["settings"], int(g["mode"])) as t:
+        r = t.Localize(g["rois"].astype(np.float32))
+    assert np.abs(r["pos"][:, :2] - g["pos"][:, :2]).max() < TOL_QI
+    assert np.abs(r["firstGuess"] - g["com"]).max() < TOL_COM
+
+
+def test_golden_buildlut_com_qi_path():
+    g = load("buildlut_80x80_u16.npz")
+    stack = g["stack"]
+    planes, nbeads = stack.shape[:2]
+    with QTrkInstance(g["settings"]) as t:
+        t.SetRadialZLUTSize(nbeads, planes)
+        t.BeginLUT(abi.BUILDLUT_NORMALIZE)
+        for p in range(planes):
+            t.BuildLUT(stack[p], p)
+        t.FinalizeLUT()
+        lut = t.GetRadialZLUT()
+    assert lut.shape == g["lut"].shape
+    assert np.abs(lut - g["lut"]).max() < 2e-3
+
+
+def test_reference_pipeline_config1(ref):
+    wl = synth.config1(300, seed=21)
+    lut = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
+    r_ref = ref.track(wl.settings, wl.mode, wl.rois, lut)
+    with make_tracker(wl.settings, wl.mode, lut) as t:
+        r = t.Localize(wl.rois)
+    check_results(r, r_ref["pos"], r_ref["firstGuess"], r_ref["error"], r_ref["imageMean"])
+
+
+def test_reference_pipeline_config2(ref):
+    wl = synth.config2(150, seed=22)
+    lut = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
+    r_ref = ref.track(wl.settings, wl.mode, wl.rois, lut)
+    with make_tracker(wl.settings, wl.mode, lut) as t:
+        r = t.Localize(wl.rois)
+    check_results(r, r_ref["pos"], r_ref["firstGuess"], r_ref["error"], r_ref["imageMean"])
+
+
+def test_buildlut_known_pos_matches_reference(ref):
+    wl = synth.config2(1, seed=23)
+    lut_ref = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
+    with QTrkInstance(wl.settings) as t:
+        t.SetRadialZLUTSize(1, wl.lut_stack.shape[0])
+        t.BeginLUT(abi.BUILDLUT_NORMALIZE)
+        for p in range(wl.lut_stack.shape[0]):
+            t.BuildLUT(wl.lut_stack[p], p, known_pos=wl.lut_known_pos)
+        t.FinalizeLUT()
+        lut = t.GetRadialZLUT()
+    assert np.abs(lut - lut_ref).max() < 1e-4
+
+
+def test_modes_and_options_match_reference(ref):
+    """com_bgcorrection, ClearFirstFourPixels, radial weights, unnormalised profiles, u8 input."""
+    wl = synth.config1(64, seed=24)
+    lut = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
+    s = synth.settings_config1(com_bgcorrection=0.7)
+    w = np.linspace(0.3, 1.0, lut.shape[2]).astype(np.float32)
+    u8 = np.clip(wl.rois, 0, 255).astype(np.uint8)
+    for mode, rois, weights in [
+        (abi.LT_QI | abi.LT_LocalizeZ | abi.LT_NormalizeProfile | abi.LT_ClearFirstFourPixels, wl.rois, None),
+        (abi.LT_QI | abi.LT_LocalizeZ | abi.LT_NormalizeProfile, u8, w),
+        (abi.LT_QI | abi.LT_LocalizeZ, wl.rois, None),
+    ]:
+        r_ref = ref.track(s, mode, rois, lut, weights=weights)
+        with make_tracker(s, mode, lut) as t:
+            if weights is not None:
+                t.SetRadialWeights(weights)
+            r = t.Localize(rois)
+        check_results(r, r_ref["pos"], r_ref["firstGuess"], r_ref["error"])
+
+
+def test_per_bead_luts_and_zlut_index(ref):
+    wl = synth.config1(40, seed=25)
+    lut1 = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
+    lut = np.concatenate([lut1, lut1[:, ::-1].copy(), lut1 * 0.5], axis=0)
+    idx = np.arange(40) % 3
+    r_ref = ref.track(wl.settings, wl.mode, wl.rois, lut, zlut_index=idx)
+    with make_tracker(wl.settings, wl.mode, lut) as t:
+        r = t.Localize(wl.rois, zlut_index=idx)
+    check_results(r, r_ref["pos"], r_ref["firstGuess"], r_ref["error"])
+    assert (r["zlutIndex"] == idx).all()
+
+
+def test_schedule_frame_matches_crops(ref):
+    """QTrkScheduleFrame crops on the device; results equal per-ROI scheduling; out-of-frame ROIs skipped."""
+    wl = synth.config1(12, seed=26)
+    lut1 = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
+    lut = np.ascontiguousarray(np.concatenate([lut1] * 12))  # ScheduleFrame sets zlutIndex = i
+    frame = np.zeros((200, 260), np.float32)
+    pos = []
+    for i in range(12):
+        x, y = 5 + (i % 4) * 62, 3 + (i // 4) * 63
+        frame[y:y + 60, x:x + 60] = wl.rois[i]
+        pos.append((x, y))
+    pos += [(-1, 0), (250, 10), (0, 190)]  # outside: skipped (QueuedTracker.cpp:99-102)
+    pos = np.array(pos, np.int32)
+    job = abi.LocalizationJob()
+    nref = ref.lib.QTrkScheduleFrame  # reference return value for the same call
+    trk = ref.lib.QTrkCreateInstance(C.byref(wl.settings))
+    try:
+        ref.lib.QTrkSetRadialZLUT(trk, lut.ctypes.data_as(C.c_void_p), 12, lut.shape[1])
+        ref.lib.QTrkSetLocalizationMode(trk, wl.mode)
+        n_expected = nref(trk, frame.ctypes.data_as(C.c_void_p), frame.strides[0], 260, 200,
+                          pos.ctypes.data_as(C.c_void_p), len(pos), abi.QTrkFloat, C.byref(job))
+        import time
+        while ref.lib.QTrkGetResultCount(trk) < n_expected:
+            time.sleep(0.001)
+        buf = (abi.LocalizationResult * n_expected)()
+        ref.lib.QTrkFetchResults(trk, buf, n_expected)
+        r_ref = abi.results_to_numpy(buf, n_expected)
+        while not ref.lib.QTrkIsIdle(trk):
+            time.sleep(0.001)
+    finally:
+        ref.lib.QTrkFreeInstance(trk)
+    r_ref = r_ref[np.argsort(r_ref["zlutIndex"])]
+    with make_tracker(wl.settings, wl.mode, lut) as t:
+        n = t.ScheduleFrame(frame, pos)
+        assert n == n_expected == 12
+        r = t.WaitForResults(n)
+        assert "skipped 3" in t.GetWarnings()
+    r = r[np.argsort(r["zlutIndex"])]
+    assert (r["zlutIndex"] == np.arange(12)).all()
+    check_results(r, r_ref["pos"], r_ref["firstGuess"], r_ref["error"])
+
+
+def test_schedule_frame_pinned_and_large(ref):
+    """A frame larger than one staging slot is split into row bands; pinned frames are DMA'd directly."""
+    import torch
+
+    wl = synth.config2(8, seed=27)
+    lut = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
+    n_side = 60
+    frame = torch.empty((n_side * 100, n_side * 100), dtype=torch.int16).pin_memory().numpy().view(np.uint16)
+    pos = []
+    for i in range(n_side):
+        for j in range(n_side):
+            k = (i * n_side + j) % 8
+            frame[i * 100:(i + 1) * 100, j * 100:(j + 1) * 100] = wl.rois[k]
+            pos.append((j * 100, i * 100))
+    pos = np.array(pos, np.int32)
+    with make_tracker(wl.settings, wl.mode, lut) as t:
+        n = t.ScheduleFrame(frame, pos)
+        assert n == n_side * n_side
+        r = t.WaitForResults(n, timeout_s=300)
+    r = r[np.argsort(r["zlutIndex"])]
+    with make_tracker(wl.settings, wl.mode, lut) as t:
+        r8 = t.Localize(wl.rois)
+    k = np.arange(n) % 8
+    assert np.array_equal(r["pos"], r8["pos"][k])
+
+
+def test_queue_semantics():
+    """FIFO results, queue length, idle state, ClearResults, batches larger than one slot."""
+    wl = synth.config1(5000, seed=28)
+    with make_tracker(wl.settings, abi.LT_QI) as t:
+        assert t.IsIdle() and t.GetQueueLength() == 0
+        t.ScheduleStack(wl.rois[:10])
+        assert t.GetQueueLength() == 10 and not t.IsIdle()   # not flushed yet
+        t.Flush()
+        r = t.WaitForResults(10)
+        assert t.IsIdle()
+        t.ScheduleStack(wl.rois, first_frame=100)
+        t.Flush()
+        import time
+        t0 = time.monotonic()
+        while t.GetResultCount() < 5000 and time.monotonic() - t0 < 60:
+            time.sleep(0.001)
+        res = t.GetResults(5000)
+        assert len(res) == 5000
+        assert (np.diff(res["frame"].astype(np.int64)) == 1).all()   # FIFO
+        t.ScheduleStack(wl.rois[:3])
+        t.Flush()
+        while not t.IsIdle():
+            time.sleep(0.001)
+        t.ClearResults()
+        assert t.GetResultCount() == 0
+        assert t.GetMaxQueueLength() > 0
+        assert "ROIs" in t.GetProfileReport()
+
+
+def test_edge_cases():
+    s = synth.settings_config1()
+    rois = np.zeros((4, 60, 60), np.float32)
+    rois[1] = 7.0                       # flat: COM is NaN -> ROI centre (QueuedCPUTracker.cpp:294-295)
+    rois[2, 0:10, 0:10] = 1000.0        # bright corner: QI walks into the boundary
+    rois[3] = np.random.default_rng(0).poisson(20, (60, 60))
+    lut = np.random.default_rng(1).normal(size=(1, 50, 40)).astype(np.float32)
+    with make_tracker(s, abi.LT_QI | abi.LT_LocalizeZ | abi.LT_NormalizeProfile, lut) as t:
+        t.Flush()                       # nothing queued
+        r = t.Localize(rois, zlut_index=np.array([0, 0, 0, 5]))
+        assert np.all(r["firstGuess"][1] == 30.0)
+        assert r["error"][2] == 1
+        assert r["pos"][3, 2] == 0.0    # zlutIndex outside the LUT: no Z
+    with make_tracker(s, abi.LT_QI | abi.LT_LocalizeZ) as t:   # no LUT set: z = 0 (cpu_tracker.cpp:793-794)
+        r = t.Localize(rois[3:])
+        assert r["pos"][0, 2] == 0.0
+
+
+def test_device_resident_entry_matches_host_path():
+    import torch
+
+    g = load("config2_100x100_u16.npz")
+    rois = g["rois"]
+    with make_tracker(g["settings"], int(g["mode"]), g["lut"]) as t:
+        host = t.Localize(rois)
+        d = torch.from_numpy(rois.view(np.int16).copy()).cuda()
+        out = torch.zeros(rois.shape[0] * 52, dtype=torch.uint8, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        t.LocalizeDevice(d.data_ptr(), 200, 20000, abi.QTrkU16, rois.shape[0], out.data_ptr(), stream=stream)
+        torch.cuda.synchronize()
+        dev = np.frombuffer(out.cpu().numpy().tobytes(), dtype=abi.RESULT_DTYPE)
+    np.testing.assert_array_equal(dev["pos"], host["pos"])
+    np.testing.assert_array_equal(dev["frame"], np.arange(rois.shape[0]))
+
+
+def test_compute_radial_profile_export_matches_reference(qlib, ref):
+    g = load("config2_100x100_u16.npz")
+    img = g["rois"][0].astype(np.float32)
+    for norm in (False, True):
+        a = np.zeros(64, np.float32)
+        b = np.zeros(64, np.float32)
+        im = abi.ImageData(img.ctypes.data_as(C.POINTER(C.c_float)), 100, 100)
+        qlib.ComputeRadialProfile(a.ctypes.data_as(C.c_void_p), 64, 206, 3.0, 47.0, abi.vector2f(50.2, 49.6),
+                                  C.byref(im), 321.0, norm)
+        ref.lib.ComputeRadialProfile(b.ctypes.data_as(C.c_void_p), 64, 206, 3.0, 47.0, abi.vector2f(50.2, 49.6),
+                                     C.byref(im), 321.0, norm)
+        np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-4)
+
+
+@pytest.mark.slow
+def test_full_size_config2_properties(ref):
+    """10,000 ROIs of 100x100 u16: every result present, FIFO, parity on a sample, accuracy vs truth."""
+    wl = synth.config2(10000, seed=2)
+    lut = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
+    with make_tracker(wl.settings, wl.mode, lut) as t:
+        r = t.Localize(wl.rois, timeout_s=300)
+    assert len(r) == 10000 and (r["frame"] == np.arange(10000)).all()
+    sample = np.arange(0, 10000, 97)
+    r_ref = ref.track(wl.settings, wl.mode, wl.rois[sample], lut)
+    check_results(r[sample], r_ref["pos"], r_ref["firstGuess"], r_ref["error"])
+    assert np.median(np.abs(r["pos"][:, 0] - wl.true_xyz[:, 0])) < 0.1
+    assert np.median(np.abs(r["pos"][:, 2] - wl.true_xyz[:, 2])) < 1.0
