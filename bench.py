@@ -1,0 +1,404 @@
+"""Benchmark: COM + QI + Z-LUT localization of 100x100 ROIs on B200.
+
+Workload (one step): 10,000 ROIs of 100x100 uint16 (12-bit; background 200, amplitude
+2000, Poisson noise; seeded synthetic images in place of camera data), COM, then QI
+with 4 iterations (64 radial x 51 angular steps per quadrant, radius 3-47 px), then the
+radial profile (64 bins x 206 angles) matched against a 200-plane Z-LUT (plain form:
+FP32 profiles, FP64-accumulated scores) and the 7-point quadratic fit.
+
+* value   — ROIs/s with the ROI stack resident in HBM: one QTrkB200LocalizeDevice call
+            (one kernel launch) per step, timed with CUDA events on the launching stream.
+            The stack (200 MB) is larger than L2 (126 MB), so every step streams from HBM.
+* e2e     — ROIs/s through the public C ABI with host buffers: per step QTrkScheduleFrame
+            of a pinned 10000x10000 u16 frame holding the 10,000 ROIs (host->device copy
+            inside the timed region), QTrkFlush, and QTrkFetchResults of all results
+            (device->host copy inside).
+* roofline — the localization kernel's algorithmic bytes (20,081 B per ROI: pixels +
+            job + result + LUT share) per launch / its mean launch time, against the
+            measured HBM copy bandwidth.
+* cpu_baseline — the reference's own CPU tracker (oracle/_ref, QueuedCPUTracker with
+            all host threads) on a bounded sample of the same workload.
+
+`--impl reference` times the reference CPU tracker alone and prints its line.
+Multi-GPU (torchrun): replicas; every rank localizes its own 10,000 ROIs, no collective
+in the data path; time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "ROIs/s (COM+QI+ZLUT, 100^2 ROI) plain vs chosen at <=1 nm err; p99 frame latency"
+UNIT = "ROIs/s"
+N_ROIS = 10000
+BYTES_PER_ROI = 100 * 100 * 2 + 52 + 24 + (200 * 64 * 4) / N_ROIS  # algorithmic bytes (20,081 B)
+PIXEL_NM = 100.0  # stated pixel size for nm error reporting
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def measured_peaks() -> tuple[dict, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling while the timed regions run."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.active = False
+        self.marks: list[tuple[float, float]] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            if self.active:
+                self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload(n: int, seed: int):
+    from qtrk_b200 import synth
+
+    return synth.config2(n, seed=seed)
+
+
+def build_lut_on_gpu(wl):
+    from qtrk_b200.tracker import QTrkInstance
+
+    with QTrkInstance(wl.settings) as t:
+        planes = wl.lut_stack.shape[0]
+        t.SetRadialZLUTSize(1, planes)
+        t.BeginLUT(True)
+        for p in range(planes):
+            t.BuildLUT(wl.lut_stack[p], p, known_pos=wl.lut_known_pos)
+        t.FinalizeLUT()
+        return t.GetRadialZLUT()
+
+
+def cpu_reference_run(wl, lut, n_sample: int, threads: int = -1):
+    """The reference CPU tracker (oracle/_ref) on the first n_sample ROIs; returns (ROIs/s, results, cores)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from oracle import RefOracle, cpu_count, ref_available
+
+    if not ref_available():
+        return None
+    ref = RefOracle()
+    s = wl.settings
+    s.numThreads = threads
+    cores = cpu_count() if threads < 0 else threads
+    res, dt = ref.track(s, wl.mode, wl.rois[:n_sample], lut, return_seconds=True)
+    s.numThreads = -1
+    return n_sample / dt, res, cores
+
+
+def cpu_port_run(wl, lut, n_sample: int):
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from oracle import PortOracle
+
+    port = PortOracle()
+    cc = port.computed_config(wl.settings)
+    t0 = time.perf_counter()
+    p = port.localize(cc, wl.mode, wl.rois[:n_sample], lut)
+    return n_sample / (time.perf_counter() - t0), p
+
+
+def run_reference_arm(args) -> int:
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    wl = make_workload(args.sample, seed=2)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from oracle import RefOracle, cpu_count, ref_available
+
+    kind = "reference" if ref_available() else "port"
+    if kind == "reference":
+        ref = RefOracle()
+        lut = ref.build_lut(wl.settings, wl.lut_stack, 4, known_pos=wl.lut_known_pos)
+    else:
+        from oracle import PortOracle
+
+        port = PortOracle()
+        lut = port.build_lut(port.computed_config(wl.settings), wl.lut_stack, 4,
+                             known_pos=wl.lut_known_pos).astype(np.float32)
+    rates = []
+    for step in range(args.warmup + args.steps):
+        if kind == "reference":
+            r = cpu_reference_run(wl, lut, args.sample)
+            rate = r[0]
+        else:
+            rate = cpu_port_run(wl, lut, min(args.sample, 200))[0]
+        if step >= args.warmup:
+            rates.append(rate)
+    value = float(np.mean(rates))
+    cores = cpu_count() if kind == "reference" else 1
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * args.sample / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "config2: 100x100 u16 ROIs, COM + QI(4 it, 64x51/quadrant) + Z-LUT 200x64 (206 angles)",
+                   "rois_per_step": args.sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{args.sample} ROIs per step of the same seeded workload, QueuedCPUTracker "
+                                   f"with numThreads=-1"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--sample", type=int, default=2000, help="ROIs per CPU-baseline step")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ncu", action="store_true", help="short run for the profiler (no e2e / baseline)")
+    args = ap.parse_args(argv)
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    from qtrk_b200 import abi
+    from qtrk_b200.tracker import QTrkInstance
+
+    wl = make_workload(N_ROIS, seed=2 + 1000 * rank)
+    lut = build_lut_on_gpu(wl)
+    s = wl.settings
+    s.cuda_device = dev.index
+    trk = QTrkInstance(s)
+    # One LUT per bead: QTrkScheduleFrame gives ROI i the LUT of bead i (QueuedTracker.cpp:105),
+    # so the e2e frame path needs N_ROIS LUT rows; all are copies of the config's 200x64 LUT. The
+    # device-resident path passes no jobs (zlutIndex 0) and reads the first copy.
+    if args.ncu:
+        trk.SetRadialZLUT(lut)  # profiler runs use the device path only: keep the capture small
+    else:
+        trk.SetRadialZLUT(np.ascontiguousarray(np.broadcast_to(lut, (N_ROIS,) + lut.shape[1:])))
+    trk.SetLocalizationMode(wl.mode)
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident path (value) ----
+    d_rois = torch.from_numpy(wl.rois.view(np.int16)).to(dev)
+    d_res = torch.empty(N_ROIS * 52, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    launches0 = trk.KernelLaunchCount()
+
+    def device_step():
+        trk.LocalizeDevice(d_rois.data_ptr(), 200, 20000, abi.QTrkU16, N_ROIS, d_res.data_ptr(),
+                           stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        device_step()
+    torch.cuda.synchronize(dev)
+    sampler = ClockSampler(dev.index)
+    sampler.start()
+    time.sleep(0.3)
+    sampler.active = True
+    barrier()
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        device_step()
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    dev_ms = ev0.elapsed_time(ev1)
+    dev_ms_max = max_over_ranks(dev_ms)
+    value = ws * N_ROIS * args.steps / (dev_ms_max / 1e3)
+    launches_value = trk.KernelLaunchCount() - launches0
+    # per-launch duration of the localization kernel (one launch per step on this stream)
+    kernel_ms = dev_ms / args.steps
+
+    res_dev = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=abi.RESULT_DTYPE)
+
+    # ---- end-to-end path through the C ABI with a pinned host frame ----
+    e2e = None
+    launches_e2e = 0
+    if not args.ncu:
+        side = int(np.sqrt(N_ROIS))
+        frame_t = torch.empty((side * 100, side * 100), dtype=torch.int16).pin_memory()
+        frame = frame_t.numpy().view(np.uint16)
+        frame[:] = wl.rois.reshape(side, side, 100, 100).transpose(0, 2, 1, 3).reshape(side * 100, side * 100)
+        ys, xs = np.meshgrid(np.arange(side) * 100, np.arange(side) * 100, indexing="ij")
+        positions = np.ascontiguousarray(np.stack([xs.ravel(), ys.ravel()], 1).astype(np.int32))
+        buf = (abi.LocalizationResult * N_ROIS)()
+        job = abi.LocalizationJob()
+
+        def e2e_step():
+            n = trk.lib.QTrkScheduleFrame(trk.handle, frame.ctypes.data_as(C.c_void_p), frame.strides[0],
+                                          frame.shape[1], frame.shape[0], positions.ctypes.data_as(C.c_void_p),
+                                          N_ROIS, abi.QTrkU16, C.byref(job))
+            assert n == N_ROIS
+            trk.lib.QTrkFlush(trk.handle)
+            got = 0
+            deadline = time.monotonic() + 60
+            while got < N_ROIS:
+                got += trk.lib.QTrkFetchResults(trk.handle, C.byref(buf, got * 52), N_ROIS - got)
+                if time.monotonic() > deadline:
+                    raise TimeoutError("e2e step did not complete")
+
+        for _ in range(2):
+            e2e_step()
+        barrier()
+        l0 = trk.KernelLaunchCount()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        t1 = time.perf_counter()
+        barrier()
+        launches_e2e = trk.KernelLaunchCount() - l0
+        e2e_s = max_over_ranks(t1 - t0)
+        e2e = {"value": ws * N_ROIS * args.e2e_steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(frame.nbytes + N_ROIS * (24 + 8)),
+               "d2h_bytes_per_step": int(N_ROIS * 52),
+               "path": "QTrkScheduleFrame(pinned 10000x10000 u16 frame, one LUT copy per bead) + QTrkFlush + "
+                       "QTrkFetchResults"}
+        res_e2e = abi.results_to_numpy(buf, N_ROIS)
+        res_e2e = res_e2e[np.argsort(res_e2e["zlutIndex"])]
+        assert np.array_equal(res_e2e["pos"], res_dev["pos"]), "e2e and device-resident results differ"
+    sampler.active = False
+    clocks = sampler.stop()
+
+    # ---- roofline of the localization kernel ----
+    peaks, peak_kind = measured_peaks()
+    achieved = BYTES_PER_ROI * N_ROIS / (kernel_ms / 1e3) / 1e9
+    traffic = None
+    tfile = ROOT / "profiles" / "localize_config2_traffic.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get("dram_bytes_per_launch")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_kind": peak_kind,
+                "kernel": "qtrk::localize_kernel<false>", "kernel_ms": kernel_ms,
+                "bytes_per_roi": BYTES_PER_ROI}
+
+    # ---- accuracy vs truth (stated pixel size) ----
+    err_xy = np.hypot(res_dev["pos"][:, 0] - wl.true_xyz[:, 0], res_dev["pos"][:, 1] - wl.true_xyz[:, 1])
+    accuracy = {"median_xy_err_nm_vs_truth": float(np.median(err_xy) * PIXEL_NM),
+                "median_z_err_planes_vs_truth": float(np.median(np.abs(res_dev["pos"][:, 2] - wl.true_xyz[:, 2]))),
+                "pixel_nm": PIXEL_NM}
+
+    # ---- CPU baseline: the reference tracker on the host cores (rank 0, N=1) ----
+    cpu_baseline = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and not args.ncu:
+        r = cpu_reference_run(wl, lut, args.sample)
+        if r is not None:
+            rate, ref_res, cores = r
+            cpu_baseline = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
+                            "sample": f"first {args.sample} ROIs of the same workload, reference QueuedCPUTracker "
+                                      f"(oracle/_ref) with numThreads=-1"}
+            d = res_dev[: args.sample]
+            accuracy["vs_reference_max_dxy_px"] = float(np.abs(d["pos"][:, :2] - ref_res["pos"][:, :2]).max())
+            accuracy["vs_reference_max_dz_planes"] = float(np.abs(d["pos"][:, 2] - ref_res["pos"][:, 2]).max())
+            accuracy["vs_reference_max_dxy_nm"] = accuracy["vs_reference_max_dxy_px"] * PIXEL_NM
+        else:
+            rate, _ = cpu_port_run(wl, lut, 100)
+            cpu_baseline = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+                            "sample": "first 100 ROIs, FP64 restatement (oracle/qtrk_oracle.c), 1 thread"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded Poisson bead images, config2 shapes)",
+        "config": {"workload": "config2: 10,000 ROIs/step of 100x100 u16; COM + QI (4 it, 64 radial x 51 angular "
+                               "per quadrant) + Z-LUT 200 planes x 64 bins (206 angles), plain FP32 match",
+                   "rois_per_step": N_ROIS, "lut_planes": 200, "l2": "inputs larger than L2 (200 MB per step)",
+                   "parallelism": f"replicas x{ws}"},
+        "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu_baseline,
+        "gpu_launches": int(launches_value + launches_e2e), "clocks": clocks, "accuracy": accuracy,
+    }
+    trk.Destroy()
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

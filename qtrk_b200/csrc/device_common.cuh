@@ -12,7 +12,13 @@
 
 #include "track_params.h"
 
+#ifndef QTRK_SAMPLE_UNROLL
+#define QTRK_SAMPLE_UNROLL 2
+#endif
+
 namespace qtrk {
+
+constexpr int kSampleUnroll = QTRK_SAMPLE_UNROLL;  // angular samples per unrolled step
 
 // -------------------------------------------------------------------------------------
 // small helpers
@@ -74,15 +80,21 @@ struct WarpGroup {
     }
 };
 
-// Interpolate, utils.h:40-58: truncating float->int conversion; the sample is outside when
-// rx < 0, ry < 0, rx+1 >= w or ry+1 >= h. Returns false when outside.
+// Interpolate, utils.h:40-58: rx = (int)x (C truncation); the sample is outside when rx < 0,
+// ry < 0, rx+1 >= w or ry+1 >= h. Returns false when outside.
+// Without float->int conversions: truncation keeps a sample inside exactly when -1 < x < w-1,
+// and for those x, (int)x == floor(max(x, 0)), which a round-toward-zero add of 2^23 puts in
+// the low mantissa bits. The fraction x - rx is formed from the same exact float as the
+// reference's x - (float)rx, so the interpolated value is unchanged.
 __device__ __forceinline__ bool bilinear(const float *img, int w, int h, float x, float y, float &v)
 {
-    const int rx = __float2int_rz(x), ry = __float2int_rz(y);
-    if ((unsigned)rx >= (unsigned)(w - 1) || (unsigned)ry >= (unsigned)(h - 1)) return false;
+    if (!(x > -1.0f && x < (float)(w - 1) && y > -1.0f && y < (float)(h - 1))) return false;
+    const float kMagic = 8388608.0f;  // 2^23
+    const float tx = __fadd_rz(fmaxf(x, 0.0f), kMagic), ty = __fadd_rz(fmaxf(y, 0.0f), kMagic);
+    const int rx = __float_as_int(tx) - 0x4B000000, ry = __float_as_int(ty) - 0x4B000000;
     const float *p = img + ry * w + rx;
     const float v00 = p[0], v10 = p[1], v01 = p[w], v11 = p[w + 1];
-    const float fx = x - (float)rx, fy = y - (float)ry;
+    const float fx = x - (tx - kMagic), fy = y - (ty - kMagic);
     const float v0 = v00 + (v10 - v00) * fx;
     const float v1 = v01 + (v11 - v01) * fx;
     v = v0 + (v1 - v0) * fy;
@@ -293,6 +305,7 @@ __device__ void qi_quadrant_profiles(const float *img, int W, int H, float cx, f
             // quadrant signs (cpu_tracker.cpp:634-640): q0 (+,+), q1 (-,+), q2 (-,-), q3 (+,-)
             const float sx = (q == 0 || q == 3) ? r : -r;
             const float sy = (q < 2) ? r : -r;
+#pragma unroll kSampleUnroll
             for (int a = sub; a < nang; a += tpb) {
                 const float2 d = dirs[stride * a];
                 float v;
@@ -415,6 +428,7 @@ __device__ void radial_profile(const float *img, int W, int H, float cx, float c
         int cnt = 0;
         if (bin < nb) {
             const float r = minr + rstep * (float)bin;
+#pragma unroll kSampleUnroll
             for (int a = sub; a < nang; a += tpb) {
                 const float2 d = dirs[a];
                 float v;

@@ -38,21 +38,28 @@ __device__ __forceinline__ SmemView smem_view(uint8_t *smem, const TrackParams &
     v.work = smem + P.sm_work;
     float2 *tab = reinterpret_cast<float2 *>(smem + P.sm_tables);
     v.qdirs = tab;
-    v.tw = tab + P.qi_angpq;
-    v.zdirs = v.tw + P.qi_nr;  // L/2 = qi_nr twiddles
+    v.tw = tab + P.qi_angpq;  // L/2 = qi_nr twiddles
+    v.zdirs = tab;            // loaded over the QI tables once QI is done (load_z_tables)
     return v;
 }
 
-// Copy the direction / twiddle tables into shared memory (all threads).
-__device__ __forceinline__ void load_tables(const SmemView &s, const TrackParams &P)
+// Copy the QI direction / twiddle tables into shared memory (all threads; a barrier must
+// follow before use).
+__device__ __forceinline__ void load_qi_tables(const SmemView &s, const TrackParams &P)
 {
     const float2 *qd = static_cast<const float2 *>(P.qi_dirs);
     const float2 *tw = static_cast<const float2 *>(P.qi_twiddles);
-    const float2 *zd = static_cast<const float2 *>(P.z_dirs);
     if (qd)
         for (int i = threadIdx.x; i < P.qi_angpq; i += blockDim.x) s.qdirs[i] = qd[i];
     if (tw)
         for (int i = threadIdx.x; i < P.qi_nr; i += blockDim.x) s.tw[i] = tw[i];
+}
+
+// Copy the full-circle direction table over the QI tables (all threads; the QI stage must
+// be finished, and a barrier must follow before use).
+__device__ __forceinline__ void load_z_tables(const SmemView &s, const TrackParams &P)
+{
+    const float2 *zd = static_cast<const float2 *>(P.z_dirs);
     if (zd)
         for (int i = threadIdx.x; i < P.z_angsteps; i += blockDim.x) s.zdirs[i] = zd[i];
 }
@@ -64,9 +71,11 @@ __device__ void qi_localize(const SmemView &s, const TrackParams &P, float mean,
 {
     const int W = P.width, H = P.height, nr = P.qi_nr, L = 2 * nr;
     const bool pow2 = (L & (L - 1)) == 0 && L >= 2;
+    // qprof (4 nr floats) is dead once the concatenated profile A is built, so the
+    // autoconvolution ac (L = 2 nr complex) reuses its space: [ qprof | ac ] [ A ].
     float *qprof = reinterpret_cast<float *>(s.work);
-    float2 *A = reinterpret_cast<float2 *>(s.work + ((4 * nr * 4 + 15) & ~15));
-    float2 *ac = A + L;
+    float2 *ac = reinterpret_cast<float2 *>(s.work);
+    float2 *A = reinterpret_cast<float2 *>(s.work + L * 8);
     const float rstep = (P.qi_maxr - P.qi_minr) / (float)nr;  // also pixelsPerProfLen (cpu_tracker.cpp:311,649)
     for (int k = 0; k < P.qi_iterations; k++) {
         bhit = check_boundaries(cx, cy, P.qi_maxr, W, H);
@@ -78,27 +87,21 @@ __device__ void qi_localize(const SmemView &s, const TrackParams &P, float mean,
         } else {
             qi_autoconv_direct(qprof, nr, A, ac);
         }
-        if (threadIdx.x < 32) {
+        if (pow2) __syncthreads();  // the FFT ran on warp 0 only
+        if (threadIdx.x < 64) {
+            // warp 0 fits the X profile, warp 1 the Y profile, concurrently.
             // autoconv[x] = out[(x + nr) mod L] (cpu_tracker.cpp:400-402)
-            auto atx = [&](int x) {
+            const bool yaxis = threadIdx.x >= 32;
+            auto at = [&](int x) {
                 int n = x + nr;
                 if (n >= L) n -= L;
-                return ac[n].x;
+                return yaxis ? ac[n].y : ac[n].x;
             };
-            auto aty = [&](int x) {
-                int n = x + nr;
-                if (n >= L) n -= L;
-                return ac[n].y;
-            };
-            const int ix = warp_argmax(atx, L);
-            const int iy = warp_argmax(aty, L);
-            if (threadIdx.x == 0) {
-                const float mx = (float)max_interp7(atx, L, ix, kQIWeights);
-                const float my = (float)max_interp7(aty, L, iy, kQIWeights);
-                const float offx = (mx - (float)nr) * (3.14159265359f / 4);
-                const float offy = (my - (float)nr) * (3.14159265359f / 4);
-                s.misc[0] = cx + offx * rstep;
-                s.misc[1] = cy + offy * rstep;
+            const int im = warp_argmax(at, L);
+            if ((threadIdx.x & 31) == 0) {
+                const float m = (float)max_interp7(at, L, im, kQIWeights);
+                const float off = (m - (float)nr) * (3.14159265359f / 4);
+                s.misc[yaxis ? 1 : 0] = (yaxis ? cy : cx) + off * rstep;
             }
         }
         __syncthreads();
@@ -115,6 +118,8 @@ __device__ float z_localize(const SmemView &s, const TrackParams &P, float mean,
     float *prof = reinterpret_cast<float *>(s.work);
     double *scores = reinterpret_cast<double *>(s.work + (((nb * 4) + 15) & ~15));
     const float rstep = (P.z_maxr - P.z_minr) / (float)nb;
+    load_z_tables(s, P);
+    __syncthreads();
     radial_profile(s.img, P.width, P.height, x, y, mean, nb, P.z_angsteps, P.z_minr, rstep, s.zdirs, prof,
                    (P.mode & kLT_NormalizeProfile) != 0, s.red);
     if (!P.lut || bead < 0 || bead >= P.lut_count) return 0.0f;
@@ -162,8 +167,12 @@ __device__ __forceinline__ void write_result(LocalizationResult *results, int i,
 
 // kGauss selects the instantiation: false = COM / QI (+ Z), true = 2D Gaussian MLE (+ Z).
 // Separate instantiations keep the QI path's register budget free of the MLE's FP64 solve.
+#ifndef QTRK_MIN_BLOCKS
+#define QTRK_MIN_BLOCKS 4
+#endif
+
 template <bool kGauss>
-__global__ void __launch_bounds__(kBlockThreads, 3) localize_kernel(TrackParams P, const uint8_t *__restrict__ pixels,
+__global__ void __launch_bounds__(kBlockThreads, QTRK_MIN_BLOCKS) localize_kernel(TrackParams P, const uint8_t *__restrict__ pixels,
                                                                     int pitch, int64_t roi_stride,
                                                                     const int64_t *__restrict__ roi_offsets,
                                                                     const LocalizationJob *__restrict__ jobs, int count,
@@ -178,7 +187,7 @@ __global__ void __launch_bounds__(kBlockThreads, 3) localize_kernel(TrackParams 
     const int bead = (int)job[2];
     const int64_t off = roi_offsets ? roi_offsets[roi] : (int64_t)roi * roi_stride;
 
-    load_tables(s, P);
+    load_qi_tables(s, P);
     BlockGroup g{s.red};
     load_roi(g, s.img, pixels + off, pitch, P, bead);
 
@@ -265,7 +274,7 @@ __global__ void __launch_bounds__(kBlockThreads) build_lut_kernel(TrackParams P,
     const int bead = blockIdx.x;
     if (bead >= nbeads) return;
     const SmemView s = smem_view(smem, P);
-    load_tables(s, P);
+    load_qi_tables(s, P);
     BlockGroup g{s.red};
     load_roi(g, s.img, pixels + (size_t)pitch * P.height * bead, pitch, P, bead);
     float x, y, mean = 0.0f;
@@ -283,6 +292,9 @@ __global__ void __launch_bounds__(kBlockThreads) build_lut_kernel(TrackParams P,
     const int nb = P.z_nbins;
     float *prof = reinterpret_cast<float *>(s.work);
     const float rstep = (P.z_maxr - P.z_minr) / (float)nb;
+    __syncthreads();
+    load_z_tables(s, P);
+    __syncthreads();
     radial_profile(s.img, P.width, P.height, x, y, mean, nb, P.z_angsteps, P.z_minr, rstep, s.zdirs, prof,
                    normalize != 0, s.red);
     float *dst = lut + ((size_t)bead * P.lut_planes + plane) * nb;
@@ -321,7 +333,7 @@ __global__ void __launch_bounds__(kBlockThreads) profile_kernel(TrackParams P, c
 {
     extern __shared__ __align__(16) uint8_t smem[];
     const SmemView s = smem_view(smem, P);
-    load_tables(s, P);
+    load_z_tables(s, P);
     BlockGroup g{s.red};
     load_roi(g, s.img, reinterpret_cast<const uint8_t *>(img_in), P.width * 4, P, -1);
     float *prof = reinterpret_cast<float *>(s.work);
@@ -342,17 +354,17 @@ void plan_smem(TrackParams &P)
     const int nr = P.qi_nr > 0 ? P.qi_nr : 1, L = 2 * nr;
     P.sm_img = 0;
     P.sm_tables = align16(W * H * 4);
-    const int tables = (P.qi_angpq + nr + P.z_angsteps) * 8;
-    P.sm_work = P.sm_tables + align16(tables);
-    const int qi_work = align16(4 * nr * 4) + 2 * L * 8;
+    const int qi_tables = (P.qi_angpq + nr) * 8, z_tables = P.z_angsteps * 8;
+    P.sm_work = P.sm_tables + align16(qi_tables > z_tables ? qi_tables : z_tables);
+    const int qi_work = 2 * L * 8;  // [ qprof | ac ] [ A ], qprof (16 nr bytes) fits in ac (8 L bytes)
     const int z_work = align16(P.z_nbins * 4) + P.lut_planes * 8;
-    const int g_work = (5 * W + 5 * H) * 4;
+    const int g_work = (P.mode & kLT_Gaussian2D) ? (3 * W + 3 * H) * 4 : 0;
     int work = qi_work;
     if (z_work > work) work = z_work;
     if (g_work > work) work = g_work;
     P.sm_red = P.sm_work + align16(work);
-    static_assert(kBlockThreads / 32 * 20 <= 256, "reduction scratch too small for the 5-parameter MLE");
-    P.sm_misc = P.sm_red + 256 * 8;  // block_sum scratch: N * warps doubles, N <= 20
+    constexpr int kRed = kBlockThreads / 32 * 20;  // block_sum scratch: N * warps doubles, N <= 20
+    P.sm_misc = P.sm_red + kRed * 8;
     P.smem_bytes = P.sm_misc + 64;
 }
 
