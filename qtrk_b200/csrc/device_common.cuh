@@ -101,6 +101,29 @@ __device__ __forceinline__ bool bilinear(const float *img, int w, int h, float x
     return true;
 }
 
+// bilinear() for a sample known to lie strictly inside (0 < x < w-1, 0 < y < h-1): the same
+// arithmetic without the range test. Callers prove the range for a whole bin at once.
+__device__ __forceinline__ float bilinear_inside(const float *img, int w, float x, float y)
+{
+    const float kMagic = 8388608.0f;
+    const float tx = __fadd_rz(x, kMagic), ty = __fadd_rz(y, kMagic);
+    const float *p = img + ((__float_as_int(ty) - 0x4B000000) * w + (__float_as_int(tx) - 0x4B000000));
+    const float v00 = p[0], v10 = p[1], v01 = p[w], v11 = p[w + 1];
+    const float fx = x - (tx - kMagic), fy = y - (ty - kMagic);
+    const float v0 = v00 + (v10 - v00) * fx;
+    const float v1 = v01 + (v11 - v01) * fx;
+    return v0 + (v1 - v0) * fy;
+}
+
+// True when every point cx + a*r, cy + b*r with |a|, |b| <= 1 (any sample of a circle of radius
+// r around (cx, cy)) lies strictly inside (0, w-1) x (0, h-1), rounding of the sample
+// coordinates included (margin 1e-3 px, far above one ulp of the coordinates).
+__device__ __forceinline__ bool circle_inside(float cx, float cy, float r, int w, int h)
+{
+    const float m = 1e-3f;
+    return cx - r > m && cy - r > m && cx + r < (float)(w - 1) - m && cy + r < (float)(h - 1) - m;
+}
+
 // CPUTracker::CheckBoundaries, cpu_tracker.cpp:182-188
 __device__ __forceinline__ bool check_boundaries(float cx, float cy, float radius, int w, int h)
 {
@@ -138,6 +161,44 @@ __device__ double max_interp7(Get at, int len, int iMax, const float (&wts)[7])
     return (double)iMax - b / (2 * a);
 }
 
+// The same fit with the eight weighted sums formed by lanes 0..6 of one warp (all 32 lanes
+// call; every lane returns the result). maxPos = iMax - b/(2a) with a = A/d, b = B/d, so the
+// determinant d cancels and one division remains; |a| < 1e-9 is tested as |A| < 1e-9 |d|.
+template <typename Get>
+__device__ double max_interp7_warp(Get at, int len, int iMax, const float (&wts)[7])
+{
+    const int lane = threadIdx.x & 31;
+    const int startPos = max(iMax - 3, 0);
+    const int endPos = min(iMax + 4, len);
+    const int np = endPos - startPos;
+    if (np < 3) return (double)iMax;
+    double t[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (lane < np) {
+        const double x = (double)(startPos + lane - iMax), y = (double)at(startPos + lane), wt = (double)wts[lane];
+        const double sq = x * x;
+        t[0] = x * wt;        // Sx
+        t[1] = y * wt;        // Sy
+        t[2] = sq * wt;       // Sx2
+        t[3] = sq * x * wt;   // Sx3
+        t[4] = sq * sq * wt;  // Sx4
+        t[5] = x * y * wt;    // Sxy
+        t[6] = sq * y * wt;   // Sx2y
+        t[7] = wt;            // Sw
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) t[k] += __shfl_xor_sync(0xffffffffu, t[k], o);
+#pragma unroll
+    for (int k = 0; k < 8; k++) t[k] = __shfl_sync(0xffffffffu, t[k], 0);
+    const double Sx = t[0], Sy = t[1], Sx2 = t[2], Sx3 = t[3], Sx4 = t[4], Sxy = t[5], Sx2y = t[6], Sw = t[7];
+    const double d = Sx4 * (Sx2 * Sw - Sx * Sx) - Sx3 * (Sx3 * Sw - Sx * Sx2) + Sx2 * (Sx3 * Sx - Sx2 * Sx2);
+    const double A = Sx2y * (Sx2 * Sw - Sx * Sx) - Sxy * (Sx3 * Sw - Sx * Sx2) + Sy * (Sx3 * Sx - Sx2 * Sx2);
+    const double B = Sx4 * (Sxy * Sw - Sy * Sx) - Sx3 * (Sx2y * Sw - Sy * Sx2) + Sx2 * (Sx2y * Sx - Sxy * Sx2);
+    if (fabs(A) < 1e-9 * fabs(d)) return (double)iMax;
+    return (double)iMax - B / (2 * A);
+}
+
 // First index of the maximum of at(0..len), reduced over one warp (all 32 lanes call).
 // Matches the strict ">" scan of LsqQuadraticFit.h:140-147 (NaN values never win).
 template <typename Get>
@@ -171,6 +232,10 @@ __device__ __forceinline__ int warp_argmax(Get at, int len)
 // option (QueuedCPUTracker.cpp:280-282) and the per-bead offset/gain step
 // (cpu_tracker.cpp:98-112) fused into the same pass.
 // -------------------------------------------------------------------------------------
+// Exact conversion of an unsigned integer below 2^23 to float without the conversion pipe:
+// placing it in the mantissa of 2^23 and subtracting 2^23.
+__device__ __forceinline__ float u_to_float(uint32_t u) { return __uint_as_float(0x4B000000u | u) - 8388608.0f; }
+
 __device__ __forceinline__ float finish_pixel(float v, int i, const TrackParams &P, const float *off,
                                               const float *gain)
 {
@@ -193,26 +258,39 @@ __device__ void load_roi(const G &g, float *img, const uint8_t *src, int pitch, 
     }
     const bool contiguous = pitch == W * bpp && ((reinterpret_cast<uintptr_t>(src) & 15) == 0) && ((n * bpp) & 15) == 0;
     if (contiguous) {
-        // 128-bit streaming loads over the whole ROI (rows are back to back).
+        // 128-bit streaming loads over the whole ROI (rows are back to back). Each thread
+        // issues up to kLoadBatch independent loads before converting any of them, so the
+        // HBM latency is paid about once per ROI rather than once per load.
+        constexpr int kLoadBatch = 4;
         const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
         const int nv = (n * bpp) >> 4;
-        for (int v = g.rank(); v < nv; v += g.size()) {
-            const uint4 q = __ldcs(s4 + v);
-            const uint32_t w4[4] = {q.x, q.y, q.z, q.w};
-            if (P.pdt == 0) {
-                const int base = v * 16;
+        for (int v0 = g.rank(); v0 < nv; v0 += kLoadBatch * g.size()) {
+            uint4 q[kLoadBatch];
 #pragma unroll
-                for (int j = 0; j < 16; j++)
-                    img[base + j] = finish_pixel((float)((w4[j >> 2] >> ((j & 3) * 8)) & 0xffu), base + j, P, off, gain);
-            } else if (P.pdt == 1) {
-                const int base = v * 8;
+            for (int k = 0; k < kLoadBatch; k++) {
+                const int v = v0 + k * g.size();
+                if (v < nv) q[k] = __ldcs(s4 + v);
+            }
 #pragma unroll
-                for (int j = 0; j < 8; j++)
-                    img[base + j] = finish_pixel((float)((w4[j >> 1] >> ((j & 1) * 16)) & 0xffffu), base + j, P, off, gain);
-            } else {
-                const int base = v * 4;
+            for (int k = 0; k < kLoadBatch; k++) {
+                const int v = v0 + k * g.size();
+                if (v >= nv) break;
+                const uint32_t w4[4] = {q[k].x, q[k].y, q[k].z, q[k].w};
+                if (P.pdt == 0) {
+                    const int base = v * 16;
 #pragma unroll
-                for (int j = 0; j < 4; j++) img[base + j] = finish_pixel(__uint_as_float(w4[j]), base + j, P, off, gain);
+                    for (int j = 0; j < 16; j++)
+                        img[base + j] = finish_pixel(u_to_float((w4[j >> 2] >> ((j & 3) * 8)) & 0xffu), base + j, P, off, gain);
+                } else if (P.pdt == 1) {
+                    const int base = v * 8;
+#pragma unroll
+                    for (int j = 0; j < 8; j++)
+                        img[base + j] = finish_pixel(u_to_float((w4[j >> 1] >> ((j & 1) * 16)) & 0xffffu), base + j, P, off, gain);
+                } else {
+                    const int base = v * 4;
+#pragma unroll
+                    for (int j = 0; j < 4; j++) img[base + j] = finish_pixel(__uint_as_float(w4[j]), base + j, P, off, gain);
+                }
             }
         }
     } else {
@@ -243,27 +321,45 @@ struct ComResult {
 template <class G>
 __device__ ComResult compute_com(const G &g, const float *img, int W, int H, float bgcorr)
 {
-    const int n = W * H;
-    double s[2] = {0, 0};
-    for (int i = g.rank(); i < n; i += g.size()) {
+    // Each thread walks a fixed set of pixels with its column/row as float counters, keeps
+    // FP32 partial sums over its few dozen pixels, and the partials are added in FP64 across
+    // the group (the reference accumulates the whole image in FP64; the partial sums keep
+    // its result to ~1e-7 relative, far inside the 1e-4 px COM tolerance).
+    const int n = W * H, stride = g.size();
+    const int dx = stride % W, dy = stride / W;
+    float p0 = 0.0f, p1 = 0.0f;
+    for (int i = g.rank(); i < n; i += stride) {
         const float v = img[i];
-        s[0] += v;
-        s[1] += (double)(v * v);
+        p0 += v;
+        p1 += v * v;
     }
+    double s[2] = {p0, p1};
     g.sum(s);
     const float invN = 1.0f / (float)n;
     ComResult r;
     r.mean = (float)(s[0] * (double)invN);
     r.stdev = sqrtf((float)(s[1] * (double)invN - (double)(r.mean * r.mean)));
-    double m[3] = {0, 0, 0};
     const float thr = bgcorr * r.stdev;
-    for (int i = g.rank(); i < n; i += g.size()) {
-        const int y = i / W, x = i - y * W;
-        const float v = fmaxf(0.0f, fabsf(img[i] - r.mean) - thr);
-        m[0] += v;
-        m[1] += x * (double)v;
-        m[2] += y * (double)v;
+    float q0 = 0.0f, qx = 0.0f, qy = 0.0f;
+    {
+        int x = g.rank() % W, y = g.rank() / W;
+        float fx = (float)x, fy = (float)y;
+        for (int i = g.rank(); i < n; i += stride) {
+            const float v = fmaxf(0.0f, fabsf(img[i] - r.mean) - thr);
+            q0 += v;
+            qx += fx * v;
+            qy += fy * v;
+            x += dx;
+            fx += (float)dx;
+            fy += (float)dy;
+            if (x >= W) {
+                x -= W;
+                fx -= (float)W;
+                fy += 1.0f;
+            }
+        }
     }
+    double m[3] = {q0, qx, qy};
     g.sum(m);
     r.x = (float)(m[1] / m[0]);
     r.y = (float)(m[2] / m[0]);
@@ -305,13 +401,22 @@ __device__ void qi_quadrant_profiles(const float *img, int W, int H, float cx, f
             // quadrant signs (cpu_tracker.cpp:634-640): q0 (+,+), q1 (-,+), q2 (-,-), q3 (+,-)
             const float sx = (q == 0 || q == 3) ? r : -r;
             const float sy = (q < 2) ? r : -r;
+            if (circle_inside(cx, cy, fabsf(r), W, H)) {
 #pragma unroll kSampleUnroll
-            for (int a = sub; a < nang; a += tpb) {
-                const float2 d = dirs[stride * a];
-                float v;
-                if (bilinear(img, W, H, cx + d.x * sx, cy + d.y * sy, v)) {
-                    sum += v;
-                    cnt++;
+                for (int a = sub; a < nang; a += tpb) {
+                    const float2 d = dirs[stride * a];
+                    sum += bilinear_inside(img, W, cx + d.x * sx, cy + d.y * sy);
+                }
+                cnt = (nang - sub + tpb - 1) / tpb;
+            } else {
+#pragma unroll kSampleUnroll
+                for (int a = sub; a < nang; a += tpb) {
+                    const float2 d = dirs[stride * a];
+                    float v;
+                    if (bilinear(img, W, H, cx + d.x * sx, cy + d.y * sy, v)) {
+                        sum += v;
+                        cnt++;
+                    }
                 }
             }
         }
@@ -329,19 +434,50 @@ __device__ void qi_quadrant_profiles(const float *img, int W, int H, float cx, f
 
 // Radix-2 decimation-in-time FFT of length L (power of two, input in bit-reversed order),
 // executed by one warp over shared memory. tw[k] = e^{-2 pi i k / L}, k < L/2.
+// Stage s pairs (i, i + 2^(s-1)) with twiddle tw[(i mod 2^(s-1)) * (L >> s)]. Two consecutive
+// stages are done together in registers on groups of four elements, which halves the
+// shared-memory round trips and warp barriers without changing any butterfly.
+__device__ __forceinline__ float2 fft_tw(const float2 *tw, int k, bool inverse)
+{
+    float2 w = tw[k];
+    if (inverse) w.y = -w.y;
+    return w;
+}
+
 __device__ void warp_fft(float2 *buf, int L, int log2L, const float2 *tw, bool inverse)
 {
     const int lane = threadIdx.x & 31;
-    for (int s = 1; s <= log2L; s++) {
-        const int half = 1 << (s - 1), tstep = L >> s;
+    int s = 1;
+    if (log2L & 1) {  // a single radix-2 stage first (twiddle 1)
         for (int j = lane; j < (L >> 1); j += 32) {
-            const int grp = j >> (s - 1), pos = j & (half - 1);
-            const int i0 = (grp << s) + pos, i1 = i0 + half;
-            float2 w = tw[pos * tstep];
-            if (inverse) w.y = -w.y;
-            const float2 a = buf[i0], b = cmul(buf[i1], w);
-            buf[i0] = make_float2(a.x + b.x, a.y + b.y);
-            buf[i1] = make_float2(a.x - b.x, a.y - b.y);
+            const float2 a = buf[2 * j], b = buf[2 * j + 1];
+            buf[2 * j] = make_float2(a.x + b.x, a.y + b.y);
+            buf[2 * j + 1] = make_float2(a.x - b.x, a.y - b.y);
+        }
+        __syncwarp();
+        s = 2;
+    }
+    for (; s < log2L; s += 2) {
+        const int h = 1 << (s - 1);
+        for (int j = lane; j < (L >> 2); j += 32) {
+            const int pos = j & (h - 1);
+            const int i0 = ((j >> (s - 1)) << (s + 1)) + pos;
+            float2 a0 = buf[i0], a1 = buf[i0 + h], a2 = buf[i0 + 2 * h], a3 = buf[i0 + 3 * h];
+            const float2 w1 = fft_tw(tw, pos * (L >> s), inverse);
+            float2 b = cmul(a1, w1);
+            a1 = make_float2(a0.x - b.x, a0.y - b.y);
+            a0 = make_float2(a0.x + b.x, a0.y + b.y);
+            b = cmul(a3, w1);
+            a3 = make_float2(a2.x - b.x, a2.y - b.y);
+            a2 = make_float2(a2.x + b.x, a2.y + b.y);
+            const float2 w2 = fft_tw(tw, pos * (L >> (s + 1)), inverse);
+            const float2 w3 = fft_tw(tw, (pos + h) * (L >> (s + 1)), inverse);
+            b = cmul(a2, w2);
+            buf[i0] = make_float2(a0.x + b.x, a0.y + b.y);
+            buf[i0 + 2 * h] = make_float2(a0.x - b.x, a0.y - b.y);
+            b = cmul(a3, w3);
+            buf[i0 + h] = make_float2(a1.x + b.x, a1.y + b.y);
+            buf[i0 + 3 * h] = make_float2(a1.x - b.x, a1.y - b.y);
         }
         __syncwarp();
     }
@@ -428,14 +564,33 @@ __device__ void radial_profile(const float *img, int W, int H, float cx, float c
         int cnt = 0;
         if (bin < nb) {
             const float r = minr + rstep * (float)bin;
-#pragma unroll kSampleUnroll
-            for (int a = sub; a < nang; a += tpb) {
-                const float2 d = dirs[a];
-                float v;
-                if (bilinear(img, W, H, cx + d.x * r, cy + d.y * r, v)) {
-                    sum += v;
-                    cnt++;
+            // FP32 sums over groups of 8 samples, folded into an FP64 total (the reference
+            // adds every sample in FP64; 8-sample FP32 groups stay within ~1e-7 of it).
+            const bool inside = circle_inside(cx, cy, fabsf(r), W, H);
+            for (int a0 = sub; a0 < nang; a0 += 8 * tpb) {
+                float part = 0.0f;
+                if (inside) {
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        const int a = a0 + k * tpb;
+                        if (a < nang) {
+                            const float2 d = dirs[a];
+                            part += bilinear_inside(img, W, cx + d.x * r, cy + d.y * r);
+                            cnt++;
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        const int a = a0 + k * tpb;
+                        float v;
+                        if (a < nang && bilinear(img, W, H, cx + dirs[a].x * r, cy + dirs[a].y * r, v)) {
+                            part += v;
+                            cnt++;
+                        }
+                    }
                 }
+                sum += (double)part;
             }
         }
         for (int o = tpb >> 1; o > 0; o >>= 1) {
@@ -468,7 +623,7 @@ __device__ void radial_profile(const float *img, int W, int H, float cx, float c
 
 // CPUTracker::LUTProfileCompare, cpu_tracker.cpp:791-868 (plain form): one warp per plane
 // group, lanes over radial bins. scores[k] = -sum_r (w_r (p_r - L_kr))^2 with the difference
-// p_r - L_kr taken in FP32 and squared/accumulated in FP64, as the reference does.
+// taken in FP32 and squared/accumulated in FP64, as the reference does.
 __device__ void zlut_scores_plain(const float *prof, const float *lut, int planes, int nb, const float *weights,
                                   double *scores)
 {

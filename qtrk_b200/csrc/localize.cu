@@ -98,8 +98,8 @@ __device__ void qi_localize(const SmemView &s, const TrackParams &P, float mean,
                 return yaxis ? ac[n].y : ac[n].x;
             };
             const int im = warp_argmax(at, L);
+            const float m = (float)max_interp7_warp(at, L, im, kQIWeights);
             if ((threadIdx.x & 31) == 0) {
-                const float m = (float)max_interp7(at, L, im, kQIWeights);
                 const float off = (m - (float)nr) * (3.14159265359f / 4);
                 s.misc[yaxis ? 1 : 0] = (yaxis ? cy : cx) + off * rstep;
             }
@@ -131,7 +131,8 @@ __device__ float z_localize(const SmemView &s, const TrackParams &P, float mean,
     if (threadIdx.x < 32) {
         auto at = [&](int i) { return scores[i]; };
         const int im = warp_argmax(at, P.lut_planes);
-        if (threadIdx.x == 0) s.misc[2] = (float)max_interp7(at, P.lut_planes, im, kZLUTWeights);
+        const float z = (float)max_interp7_warp(at, P.lut_planes, im, kZLUTWeights);
+        if (threadIdx.x == 0) s.misc[2] = z;
     }
     __syncthreads();
     return s.misc[2];
