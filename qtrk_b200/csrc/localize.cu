@@ -13,6 +13,8 @@
 #include <cstdio>
 #include <cuda_runtime.h>
 
+#include <cuda_bf16.h>
+
 #include "device_common.cuh"
 #include "kernels.h"
 
@@ -112,7 +114,8 @@ __device__ void qi_localize(const SmemView &s, const TrackParams &P, float mean,
 }
 
 // Radial profile + Z-LUT compare (QueuedCPUTracker.cpp:319-338). Returns z (0 without a LUT).
-__device__ float z_localize(const SmemView &s, const TrackParams &P, float mean, float x, float y, int bead)
+// With P.zprof_f32 set, the profile is written out for the tensor-core match instead.
+__device__ float z_localize(const SmemView &s, const TrackParams &P, float mean, float x, float y, int bead, int roi)
 {
     const int nb = P.z_nbins;
     float *prof = reinterpret_cast<float *>(s.work);
@@ -122,6 +125,22 @@ __device__ float z_localize(const SmemView &s, const TrackParams &P, float mean,
     __syncthreads();
     radial_profile(s.img, P.width, P.height, x, y, mean, nb, P.z_angsteps, P.z_minr, rstep, s.zdirs, prof,
                    (P.mode & kLT_NormalizeProfile) != 0, s.red);
+    if (P.zprof_f32) {
+        // [hi | lo] BF16 split of the weighted profile: v = hi + lo + O(2^-16 v)
+        __nv_bfloat16 *pb = static_cast<__nv_bfloat16 *>(P.zprof_bf16) + (size_t)roi * 2 * P.zprof_nbp;
+        for (int r = threadIdx.x; r < P.zprof_nbp; r += blockDim.x) {
+            float v = 0.0f;
+            if (r < nb) {
+                v = prof[r];
+                P.zprof_f32[(size_t)roi * nb + r] = v;
+                if (P.z_weights) v *= P.z_weights[r];
+            }
+            const __nv_bfloat16 h = __float2bfloat16_rn(v);
+            pb[r] = h;
+            pb[P.zprof_nbp + r] = __float2bfloat16_rn(v - __bfloat162float(h));
+        }
+        return 0.0f;
+    }
     if (!P.lut || bead < 0 || bead >= P.lut_count) return 0.0f;
     const float *lut = P.lut + (size_t)bead * P.lut_planes * nb;
     zlut_scores_plain(prof, lut, P.lut_planes, nb, P.z_weights, scores);
@@ -218,7 +237,7 @@ __global__ void __launch_bounds__(kBlockThreads, QTRK_MIN_BLOCKS) localize_kerne
     }
     if (P.mode & kLT_LocalizeZ) {
         bhit = check_boundaries(x, y, P.z_maxr, W, H);
-        z = z_localize(s, P, com.mean, x, y, bead);
+        z = z_localize(s, P, com.mean, x, y, bead, roi);
     }
     if (threadIdx.x == 0) write_result(results, roi, job, x, y, z, comx, comy, bhit ? 1u : 0u, com.mean);
 }

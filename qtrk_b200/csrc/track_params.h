@@ -54,6 +54,12 @@ struct TrackParams {
     int lut_count, lut_planes;
     const float *z_weights;   // float[z_nbins] or nullptr
     float *cmp_scores;        // [lut_count][lut_planes] or nullptr (compare-profile output)
+    // Tensor-core match: when zprof_f32 is set the localization kernel writes each ROI's
+    // normalised profile (FP32) and its weighted BF16 copy (zprof_nbp bins, zero padded)
+    // instead of scoring it; the Z-match kernel then fills in z.
+    float *zprof_f32;
+    void *zprof_bf16;
+    int zprof_nbp;
 
     // 2D Gaussian MLE (cputrack/cpu_tracker.cpp:514-589)
     int g_iterations;

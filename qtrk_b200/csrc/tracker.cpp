@@ -247,6 +247,10 @@ Tracker::Tracker(const QTrkSettings &settings)
         throw std::runtime_error("ROI of " + std::to_string(W) + "x" + std::to_string(H) +
                                  " pixels does not fit in one CTA's shared memory");
 
+    CheckCuda(zmatch_prepare_kernel_attrs(), "zmatch kernel attributes");
+    CheckCuda(cudaHostAlloc((void **)&h_err_, sizeof(unsigned), cudaHostAllocMapped), "cudaHostAlloc(error word)");
+    *h_err_ = 0;
+    CheckCuda(cudaHostGetDevicePointer((void **)&d_err_, h_err_, 0), "cudaHostGetDevicePointer");
     CheckCuda(cudaStreamCreateWithFlags(&lut_stream_, cudaStreamNonBlocking), "cudaStreamCreate(lut)");
     CheckCuda(cudaEventCreateWithFlags(&lut_ready_, cudaEventDisableTiming), "cudaEventCreate");
     for (int b = 0; b < 2; b++)
@@ -278,6 +282,12 @@ Tracker::~Tracker()
         cudaFree(s.d_jobs);
         cudaFree(s.d_res);
         cudaFree(s.d_off);
+        cudaFree(s.d_zprof);
+        cudaFree(s.d_zprof_bf16);
+        cudaFreeHost(s.h_perm);
+        cudaFree(s.d_perm);
+        cudaFreeHost(s.h_tiles);
+        cudaFree(s.d_tiles);
         if (s.ev_start) cudaEventDestroy(s.ev_start);
         if (s.ev_done) cudaEventDestroy(s.ev_done);
         if (s.stream) cudaStreamDestroy(s.stream);
@@ -296,6 +306,11 @@ Tracker::~Tracker()
     cudaFree(d_cmp_);
     cudaFree(d_calib_off_);
     cudaFree(d_calib_gain_);
+    cudaFree(d_lut_bf16_);
+    cudaFree(d_lut_norm_);
+    cudaFree(d_dev_zprof_);
+    cudaFree(d_dev_zprof_bf16_);
+    cudaFreeHost(h_err_);
     if (lut_ready_) cudaEventDestroy(lut_ready_);
     if (lut_stream_) cudaStreamDestroy(lut_stream_);
 }
@@ -357,6 +372,10 @@ bool Tracker::IsPinned(const void *p)
 
 void Tracker::CollectLocked()
 {
+    if (h_err_ && *h_err_) {
+        *h_err_ = 0;
+        Warn("tensor-core Z match: an MMA completion wait timed out; z of the affected ROIs is NaN");
+    }
     while (!inflight_.empty()) {
         const int idx = inflight_.front();
         Slot &s = slots_[idx];
@@ -403,9 +422,33 @@ int Tracker::AcquireSlotLocked(std::unique_lock<std::mutex> &lk)
 void Tracker::SubmitLocked(int idx)
 {
     Slot &s = slots_[idx];
-    const TrackParams P = Params(s.pdt);
+    TrackParams P = Params(s.pdt);
     const size_t roib = (size_t)cfg.base.width * cfg.base.height * pdt_bytes(s.pdt);
+    const bool tc = UseTensorCoreMatch();
+    int ntiles = 0;
+    if (tc) {
+        const int nb = cfg.zlut_radialsteps, nbp = zmatch_padded_bins(nb);
+        if (!s.d_zprof) {
+            CheckCuda(cudaMalloc(&s.d_zprof, sizeof(float) * batch_ * nb), "cudaMalloc(profiles)");
+            CheckCuda(cudaMalloc(&s.d_zprof_bf16, sizeof(__nv_bfloat16) * batch_ * 2 * nbp), "cudaMalloc(profiles)");
+            CheckCuda(cudaHostAlloc(&s.h_perm, sizeof(int) * batch_, cudaHostAllocDefault), "cudaHostAlloc");
+            CheckCuda(cudaMalloc(&s.d_perm, sizeof(int) * batch_), "cudaMalloc");
+            CheckCuda(cudaHostAlloc(&s.h_tiles, sizeof(int4) * batch_, cudaHostAllocDefault), "cudaHostAlloc");
+            CheckCuda(cudaMalloc(&s.d_tiles, sizeof(int4) * batch_), "cudaMalloc");
+        }
+        PrepareTensorCoreLUT();
+        ntiles = BuildTiles(s.h_jobs, s.count, s.h_perm, s.h_tiles);
+        P.zprof_f32 = s.d_zprof;
+        P.zprof_bf16 = s.d_zprof_bf16;
+        P.zprof_nbp = nbp;
+    }
     CheckCuda(cudaStreamWaitEvent(s.stream, lut_ready_, 0), "cudaStreamWaitEvent");
+    if (tc) {
+        CheckCuda(cudaMemcpyAsync(s.d_perm, s.h_perm, sizeof(int) * s.count, cudaMemcpyHostToDevice, s.stream),
+                  "H2D perm");
+        CheckCuda(cudaMemcpyAsync(s.d_tiles, s.h_tiles, sizeof(int4) * ntiles, cudaMemcpyHostToDevice, s.stream),
+                  "H2D tiles");
+    }
     if (!s.frame) {
         CheckCuda(cudaEventRecord(s.ev_start, s.stream), "cudaEventRecord");
         CheckCuda(cudaMemcpyAsync(s.d_pix, s.h_pix, roib * s.count, cudaMemcpyHostToDevice, s.stream), "H2D pixels");
@@ -419,11 +462,88 @@ void Tracker::SubmitLocked(int idx)
                               s.d_res, s.stream),
               "localize kernel launch");
     launches_++;
+    if (tc) {
+        ZMatchParams Q = TensorCoreParams();
+        Q.prof_f32 = s.d_zprof;
+        Q.prof_bf16 = s.d_zprof_bf16;
+        Q.perm = s.d_perm;
+        Q.tiles = s.d_tiles;
+        Q.count = s.count;
+        Q.results = s.d_res;
+        CheckCuda(launch_zmatch_tc(Q, ntiles, s.stream), "Z-match kernel launch");
+        launches_++;
+    }
     CheckCuda(cudaMemcpyAsync(s.h_res, s.d_res, sizeof(LocalizationResult) * s.count, cudaMemcpyDeviceToHost, s.stream),
               "D2H results");
     CheckCuda(cudaEventRecord(s.ev_done, s.stream), "cudaEventRecord");
     s.t_submit = now_s();
     inflight_.push_back(idx);
+}
+
+bool Tracker::UseTensorCoreMatch() const
+{
+    return (mode_ & LT_B200_ZMatchBF16) && (mode_ & LT_LocalizeZ) && d_lut_ && lut_count_ > 0 &&
+           lut_planes_ > 0 && zmatch_supported(cfg.zlut_radialsteps) && !cmp_enabled_;
+}
+
+void Tracker::PrepareTensorCoreLUT()
+{
+    if (!tc_lut_stale_ && d_lut_bf16_) return;
+    const int nb = cfg.zlut_radialsteps, nbp = zmatch_padded_bins(nb), pp = zmatch_padded_planes(lut_planes_);
+    CheckCuda(cudaStreamSynchronize(lut_stream_), "cudaStreamSynchronize(lut)");
+    cudaFree(d_lut_bf16_);
+    cudaFree(d_lut_norm_);
+    d_lut_bf16_ = nullptr;
+    d_lut_norm_ = nullptr;
+    CheckCuda(cudaMalloc(&d_lut_bf16_, sizeof(__nv_bfloat16) * (size_t)lut_count_ * 2 * pp * nbp),
+              "cudaMalloc(BF16 LUT)");
+    CheckCuda(cudaMalloc(&d_lut_norm_, sizeof(float) * (size_t)lut_count_ * pp), "cudaMalloc(LUT norms)");
+    CheckCuda(zmatch_prepare_lut(d_lut_, have_zw_ ? d_zw_ : nullptr, lut_count_, lut_planes_, nb, d_lut_bf16_,
+                                 d_lut_norm_, lut_stream_),
+              "BF16 LUT preparation");
+    launches_++;
+    CheckCuda(cudaEventRecord(lut_ready_, lut_stream_), "cudaEventRecord");
+    tc_lut_stale_ = false;
+}
+
+ZMatchParams Tracker::TensorCoreParams() const
+{
+    ZMatchParams Q;
+    std::memset(&Q, 0, sizeof(Q));
+    Q.nb = cfg.zlut_radialsteps;
+    Q.nbp = zmatch_padded_bins(Q.nb);
+    Q.planes = lut_planes_;
+    Q.planes_pad = zmatch_padded_planes(lut_planes_);
+    Q.lut_count = lut_count_;
+    Q.lut_bf16 = d_lut_bf16_;
+    Q.lut_norm = d_lut_norm_;
+    Q.lut = d_lut_;
+    Q.weights = have_zw_ ? d_zw_ : nullptr;
+    Q.error_flag = d_err_;
+    return Q;
+}
+
+// ROIs grouped by bead (stable), cut into tiles of at most 128 ROIs of one bead. ROIs whose
+// bead has no LUT form tiles of bead -1 (z = 0, as in the plain path).
+int Tracker::BuildTiles(const LocalizationJob *jobs, int count, int *perm, int4 *tiles) const
+{
+    std::vector<int> order(count);
+    for (int i = 0; i < count; i++) order[i] = i;
+    auto bead_of = [&](int i) {
+        const int b = jobs[i].zlutIndex;
+        return (b >= 0 && b < lut_count_) ? b : -1;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return bead_of(a) < bead_of(b); });
+    int nt = 0;
+    for (int i = 0; i < count;) {
+        const int b = bead_of(order[i]);
+        int j = i;
+        while (j < count && bead_of(order[j]) == b && j - i < 128) j++;
+        tiles[nt++] = make_int4(i, j - i, b, 0);
+        i = j;
+    }
+    std::memcpy(perm, order.data(), sizeof(int) * count);
+    return nt;
 }
 
 void Tracker::DrainAllLocked(std::unique_lock<std::mutex> &lk)
@@ -723,6 +843,7 @@ void Tracker::SetRadialZLUT(const float *data, int count, int planes)
         CheckCuda(cudaMemset(d_cmp_, 0, (size_t)count * planes * 4), "clear compare profiles");
         lut_count_ = count;
         lut_planes_ = planes;
+        tc_lut_stale_ = true;
         if (Params(2).smem_bytes > 227 * 1024) {
             cudaFree(d_lut_);
             cudaFree(d_cmp_);
@@ -767,6 +888,7 @@ void Tracker::SetRadialWeights(const float *w)
     } else {
         have_zw_ = false;
     }
+    tc_lut_stale_ = true;
 }
 
 void Tracker::EnableRadialZLUTCompareProfile(bool enabled)
@@ -848,6 +970,7 @@ void Tracker::BuildLUT(const void *data, int pitch, int pdt, int plane, const ve
     launches_++;
     CheckCuda(cudaEventRecord(lut_stage_free_[b], lut_stream_), "cudaEventRecord");
     CheckCuda(cudaEventRecord(lut_ready_, lut_stream_), "cudaEventRecord");
+    tc_lut_stale_ = true;
 }
 
 // QueuedCPUTracker::FinalizeLUT, QueuedCPUTracker.cpp:648-659.
@@ -862,6 +985,7 @@ void Tracker::FinalizeLUT()
     }
     CheckCuda(cudaEventRecord(lut_ready_, lut_stream_), "cudaEventRecord");
     CheckCuda(cudaStreamSynchronize(lut_stream_), "cudaStreamSynchronize(lut)");
+    tc_lut_stale_ = true;
 }
 
 int Tracker::GetResultCount()
@@ -943,15 +1067,56 @@ int Tracker::LocalizeDevice(const void *d_pixels, int pitch, int64_t roi_stride,
     }
     DeviceGuard dg(device_);
     TrackParams P;
+    ZMatchParams Q;
+    bool tc;
     {
         std::lock_guard<std::mutex> lk(mu_);
         P = Params(pdt);
+        tc = UseTensorCoreMatch();
+        if (tc && d_jobs) {
+            // the bead of each ROI is only known on the device here: score with the plain path
+            static bool warned = false;
+            if (!warned) Warn("QTrkB200LocalizeDevice: device-side jobs use the plain Z match");
+            warned = true;
+            tc = false;
+        }
+        if (tc) {
+            const int nb = cfg.zlut_radialsteps, nbp = zmatch_padded_bins(nb);
+            if (dev_scratch_rois_ < count) {
+                CheckCuda(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+                cudaFree(d_dev_zprof_);
+                cudaFree(d_dev_zprof_bf16_);
+                d_dev_zprof_ = nullptr;
+                d_dev_zprof_bf16_ = nullptr;
+                dev_scratch_rois_ = 0;
+                CheckCuda(cudaMalloc(&d_dev_zprof_, sizeof(float) * (size_t)count * nb), "cudaMalloc(profiles)");
+                CheckCuda(cudaMalloc(&d_dev_zprof_bf16_, sizeof(__nv_bfloat16) * (size_t)count * 2 * nbp),
+                          "cudaMalloc(profiles)");
+                dev_scratch_rois_ = count;
+            }
+            PrepareTensorCoreLUT();
+            P.zprof_f32 = d_dev_zprof_;
+            P.zprof_bf16 = d_dev_zprof_bf16_;
+            P.zprof_nbp = nbp;
+            Q = TensorCoreParams();
+            Q.prof_f32 = d_dev_zprof_;
+            Q.prof_bf16 = d_dev_zprof_bf16_;
+            Q.perm = nullptr;
+            Q.tiles = nullptr;
+            Q.count = count;
+            Q.uniform_bead = 0;
+            Q.results = d_results;
+        }
     }
     CheckCuda(cudaStreamWaitEvent(stream, lut_ready_, 0), "cudaStreamWaitEvent");
     CheckCuda(launch_localize(P, static_cast<const uint8_t *>(d_pixels), pitch, roi_stride, nullptr, d_jobs, count,
                               d_results, stream),
               "localize kernel launch");
     launches_++;
+    if (tc) {
+        CheckCuda(launch_zmatch_tc(Q, (count + 127) / 128, stream), "Z-match kernel launch");
+        launches_++;
+    }
     return 0;
 }
 

@@ -18,6 +18,7 @@
 
 #include "qtrk_c_api.h"
 #include "track_params.h"
+#include "zmatch_tc.h"
 
 // The opaque handle type of the C ABI.
 struct QueuedTracker {
@@ -86,6 +87,12 @@ class Tracker : public QueuedTracker {
         LocalizationJob *h_jobs = nullptr, *d_jobs = nullptr;
         LocalizationResult *h_res = nullptr, *d_res = nullptr;
         int64_t *h_off = nullptr, *d_off = nullptr;
+        // tensor-core Z match scratch (allocated on first use): profiles between the two
+        // kernels, the bead-grouped ROI order and the tile list
+        float *d_zprof = nullptr;
+        __nv_bfloat16 *d_zprof_bf16 = nullptr;
+        int *h_perm = nullptr, *d_perm = nullptr;
+        int4 *h_tiles = nullptr, *d_tiles = nullptr;
         int count = 0, pdt = -1;
         bool frame = false;   // pixels hold frame rows addressed through d_off
         int pitch = 0;
@@ -100,6 +107,10 @@ class Tracker : public QueuedTracker {
     void WaitIdleForReconfigure();
     void CheckCuda(cudaError_t e, const char *what);
     static bool IsPinned(const void *p);
+    bool UseTensorCoreMatch() const;     // mode asks for it and the LUT shape allows it
+    void PrepareTensorCoreLUT();         // BF16 weighted LUT + norms when stale (LUT stream)
+    ZMatchParams TensorCoreParams() const;
+    int BuildTiles(const LocalizationJob *jobs, int count, int *perm, int4 *tiles) const;
 
     int device_ = 0;
     LocMode_t mode_ = 0;
@@ -130,6 +141,16 @@ class Tracker : public QueuedTracker {
     cudaEvent_t lut_stage_free_[2] = {nullptr, nullptr};
     size_t lut_stage_bytes_ = 0;
     int lut_stage_next_ = 0;
+
+    // tensor-core Z match state
+    __nv_bfloat16 *d_lut_bf16_ = nullptr;
+    float *d_lut_norm_ = nullptr;
+    bool tc_lut_stale_ = true;
+    unsigned *h_err_ = nullptr, *d_err_ = nullptr;  // mapped pinned word set by the Z-match kernel
+    float *d_dev_zprof_ = nullptr;                  // scratch of the device-resident entry point
+    __nv_bfloat16 *d_dev_zprof_bf16_ = nullptr;
+    int4 *d_dev_tiles_ = nullptr;
+    int dev_scratch_rois_ = 0;
 
     // pixel calibration
     float *d_calib_off_ = nullptr, *d_calib_gain_ = nullptr;
