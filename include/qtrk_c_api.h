@@ -230,4 +230,29 @@ QTRK_API int QTRK_CALLCONV QTrkB200LocalizeDevice(struct QueuedTracker *qtrk, co
                                                   const LocalizationJob *d_jobs, LocalizationResult *d_results,
                                                   void *stream);
 
+/*
+ * QTrkB200LocalizeDevice without any device-memory allocation. No counterpart in the
+ * reference. For callers that cannot allocate while they run: real-time acquisition threads
+ * (camera callbacks, LabVIEW timed loops) that must keep each call's latency bounded, since
+ * cudaMalloc/cudaFree take the driver's allocation lock and can synchronize the device, and
+ * processes whose device-memory budget is fixed at start-up. Same arguments, results and
+ * kernels as QTrkB200LocalizeDevice; the intermediate profiles of the tensor-core Z match
+ * (LT_B200_ZMatchBF16) go to one fixed 16 MiB array inside the library, which every GPU that
+ * loads the library holds until the process exits.
+ * Limit: count * (4 * zlut_radialsteps + 4 * zlut_radialsteps rounded up to 16) bytes (plus up
+ * to 255 bytes of alignment) must fit in 16 MiB: 32,768 ROIs of 64 radial bins. Larger counts
+ * return -3 and launch nothing. The instance's BF16 copy of the Z-LUT is made by its first
+ * allocating call in this mode (QTrkB200LocalizeDevice or a queued batch); until then this call
+ * returns -4 and launches nothing. With device-side jobs (d_jobs != NULL) Z uses the plain match,
+ * which needs no scratch.
+ * The first call on each device looks up the array's device address; make that first call
+ * before any stream capture. All calls share the array and each overwrites what it reads, so
+ * nothing needs clearing; calls whose GPU work overlaps (other streams, other instances on the
+ * same GPU) race on it.
+ */
+QTRK_API int QTRK_CALLCONV QTrkB200LocalizeDeviceNoAlloc(struct QueuedTracker *qtrk, const void *d_pixels, int pitch,
+                                                         int64_t roi_stride_bytes, QTRK_PixelDataType_t pdt,
+                                                         int count, const LocalizationJob *d_jobs,
+                                                         LocalizationResult *d_results, void *stream);
+
 #endif /* QTRK_B200_C_API_H */

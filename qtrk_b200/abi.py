@@ -170,6 +170,7 @@ B200_PROTOTYPES = {
     "QTrkB200GetLastError": (C.c_int, [C.c_char_p, C.c_int]),
     "QTrkB200GetKernelLaunchCount": (C.c_int64, [_TRK]),
     "QTrkB200LocalizeDevice": (C.c_int, [_TRK, _P, C.c_int, C.c_int64, C.c_int, C.c_int, _P, _P, _P]),
+    "QTrkB200LocalizeDeviceNoAlloc": (C.c_int, [_TRK, _P, C.c_int, C.c_int64, C.c_int, C.c_int, _P, _P, _P]),
 }
 
 

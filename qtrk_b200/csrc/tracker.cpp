@@ -1120,4 +1120,77 @@ int Tracker::LocalizeDevice(const void *d_pixels, int pitch, int64_t roi_stride,
     return 0;
 }
 
+// The allocation-free variant of LocalizeDevice: the tensor-core match's profiles go to
+// `scratch` (a fixed device array owned by the caller of this method), and the instance's
+// BF16 LUT must already exist (it is created by the first allocating call in this mode);
+// refreshing a stale BF16 LUT is a kernel launch only. Nothing here calls cudaMalloc/cudaFree.
+int Tracker::LocalizeDeviceNoAlloc(const void *d_pixels, int pitch, int64_t roi_stride, int pdt, int count,
+                                   const LocalizationJob *d_jobs, LocalizationResult *d_results, cudaStream_t stream,
+                                   void *scratch, size_t scratch_bytes)
+{
+    if (!d_pixels || !d_results || !scratch || count < 0 || pdt < 0 || pdt > 2) {
+        Warn("QTrkB200LocalizeDeviceNoAlloc: invalid argument");
+        return -1;
+    }
+    if (pitch < cfg.base.width * pdt_bytes(pdt)) {
+        Warn("QTrkB200LocalizeDeviceNoAlloc: pitch smaller than a row");
+        return -2;
+    }
+    DeviceGuard dg(device_);
+    TrackParams P;
+    ZMatchParams Q;
+    bool tc;
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        P = Params(pdt);
+        tc = UseTensorCoreMatch() && !d_jobs;  // device-side jobs: plain match, as LocalizeDevice
+        if (tc) {
+            if (!d_lut_bf16_ || !d_lut_norm_) {
+                Warn("QTrkB200LocalizeDeviceNoAlloc: the instance has no tensor-core LUT yet; it is created by the "
+                     "first QTrkB200LocalizeDevice call or queued batch in this mode");
+                return -4;
+            }
+            const int nb = cfg.zlut_radialsteps, nbp = zmatch_padded_bins(nb);
+            const size_t prof_bytes = ((sizeof(float) * (size_t)count * nb) + 255) & ~(size_t)255;
+            const size_t need = prof_bytes + sizeof(__nv_bfloat16) * (size_t)count * 2 * nbp;
+            if (need > scratch_bytes) {
+                Warn("QTrkB200LocalizeDeviceNoAlloc: " + std::to_string(count) + " ROIs need " + std::to_string(need) +
+                     " bytes of profile scratch; the fixed array holds " + std::to_string(scratch_bytes));
+                return -3;
+            }
+            float *zprof = static_cast<float *>(scratch);
+            __nv_bfloat16 *zbf = reinterpret_cast<__nv_bfloat16 *>(static_cast<uint8_t *>(scratch) + prof_bytes);
+            if (tc_lut_stale_) {  // refresh in place: one kernel launch, the buffers keep their size
+                CheckCuda(zmatch_prepare_lut(d_lut_, have_zw_ ? d_zw_ : nullptr, lut_count_, lut_planes_, nb,
+                                             d_lut_bf16_, d_lut_norm_, lut_stream_),
+                          "BF16 LUT preparation");
+                launches_++;
+                CheckCuda(cudaEventRecord(lut_ready_, lut_stream_), "cudaEventRecord");
+                tc_lut_stale_ = false;
+            }
+            P.zprof_f32 = zprof;
+            P.zprof_bf16 = zbf;
+            P.zprof_nbp = nbp;
+            Q = TensorCoreParams();
+            Q.prof_f32 = zprof;
+            Q.prof_bf16 = zbf;
+            Q.perm = nullptr;
+            Q.tiles = nullptr;
+            Q.count = count;
+            Q.uniform_bead = 0;
+            Q.results = d_results;
+        }
+    }
+    CheckCuda(cudaStreamWaitEvent(stream, lut_ready_, 0), "cudaStreamWaitEvent");
+    CheckCuda(launch_localize(P, static_cast<const uint8_t *>(d_pixels), pitch, roi_stride, nullptr, d_jobs, count,
+                              d_results, stream),
+              "localize kernel launch");
+    launches_++;
+    if (tc) {
+        CheckCuda(launch_zmatch_tc(Q, (count + 127) / 128, stream), "Z-match kernel launch");
+        launches_++;
+    }
+    return 0;
+}
+
 }  // namespace qtrk

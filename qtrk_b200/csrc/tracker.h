@@ -74,6 +74,10 @@ class Tracker : public QueuedTracker {
     // Extensions
     int LocalizeDevice(const void *d_pixels, int pitch, int64_t roi_stride, int pdt, int count,
                        const LocalizationJob *d_jobs, LocalizationResult *d_results, cudaStream_t stream);
+    // LocalizeDevice with caller-supplied profile scratch (scratch_bytes); allocates nothing.
+    int LocalizeDeviceNoAlloc(const void *d_pixels, int pitch, int64_t roi_stride, int pdt, int count,
+                              const LocalizationJob *d_jobs, LocalizationResult *d_results, cudaStream_t stream,
+                              void *scratch, size_t scratch_bytes);
     int64_t LaunchCount() const { return launches_.load(); }
     void Warn(const std::string &msg);
     int device() const { return device_; }

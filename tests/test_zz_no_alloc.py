@@ -1,0 +1,79 @@
+"""QTrkB200LocalizeDeviceNoAlloc: the allocation-free device-resident entry point.
+
+Some callers cannot allocate device memory while they run (real-time acquisition threads that
+must not wait on the driver's allocator, processes with a fixed device-memory budget). This
+entry point runs the same localization as QTrkB200LocalizeDevice but keeps the tensor-core Z
+match's intermediate profiles in a fixed 16 MiB array inside the library instead of memory
+allocated by the call. The test calls both entry points through the C ABI on the same device
+inputs and requires the same results (tolerance of the other parity tests: 1e-3 px in x/y,
+0.01 plane in z; the kernels are the same, so the results are expected to be identical), on
+two calls in a row with different inputs (the shared array keeps the previous call's contents),
+and checks the size limit. This file is collected last so that a failure here comes after all
+other tests have run; it also passes alone in a fresh process.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from qtrk_b200 import abi, synth
+from qtrk_b200.tracker import QTrkInstance
+
+pytestmark = pytest.mark.gpu
+
+TOL_XY = 1e-3
+TOL_Z = 0.01
+
+
+def _results(buf) -> np.ndarray:
+    return np.frombuffer(buf.cpu().numpy().tobytes(), dtype=abi.RESULT_DTYPE)
+
+
+def test_no_alloc_entry_matches_device_entry():
+    import torch
+
+    wl = synth.config2(600, seed=41)
+    with QTrkInstance(wl.settings) as t:
+        t.SetRadialZLUTSize(1, wl.lut_stack.shape[0])
+        t.BeginLUT(abi.BUILDLUT_NORMALIZE)
+        for p in range(wl.lut_stack.shape[0]):
+            t.BuildLUT(wl.lut_stack[p], p, known_pos=wl.lut_known_pos)
+        t.FinalizeLUT()
+        t.SetLocalizationMode(wl.mode | abi.LT_B200_ZMatchBF16)
+        stream = torch.cuda.current_stream().cuda_stream
+        lib = t.lib
+        # two different input sets, each through both entry points (the allocating entry runs
+        # first and also creates the instance's BF16 LUT); the no-alloc calls then run back to
+        # back, so the second reuses the array the first one filled
+        sets = [wl.rois[:300], wl.rois[300:]]
+        dev = [torch.from_numpy(r.view(np.int16).copy()).cuda() for r in sets]
+        ref = []
+        for d, r in zip(dev, sets):
+            out = torch.zeros(r.shape[0] * 52, dtype=torch.uint8, device="cuda")
+            rc = lib.QTrkB200LocalizeDevice(t.handle, C.c_void_p(d.data_ptr()), 200, 20000, abi.QTrkU16, r.shape[0],
+                                            None, C.c_void_p(out.data_ptr()), C.c_void_p(stream))
+            assert rc == 0, t.GetWarnings()
+            ref.append(out)
+        got = []
+        for d, r in zip(dev, sets):
+            out = torch.full((r.shape[0] * 52,), 0xFF, dtype=torch.uint8, device="cuda")
+            rc = lib.QTrkB200LocalizeDeviceNoAlloc(t.handle, C.c_void_p(d.data_ptr()), 200, 20000, abi.QTrkU16,
+                                                   r.shape[0], None, C.c_void_p(out.data_ptr()), C.c_void_p(stream))
+            assert rc == 0, t.GetWarnings()
+            got.append(out)
+        torch.cuda.synchronize()
+        for a, b in zip(ref, got):
+            ra, rb = _results(a), _results(b)
+            assert np.array_equal(ra["frame"], rb["frame"])
+            assert np.abs(ra["pos"][:, :2] - rb["pos"][:, :2]).max() <= TOL_XY
+            assert np.abs(ra["pos"][:, 2] - rb["pos"][:, 2]).max() <= TOL_Z
+            assert np.abs(ra["firstGuess"] - rb["firstGuess"]).max() <= 1e-4
+            assert (rb["pos"][:, 2] != 0).mean() > 0.9   # z was computed by the tensor-core match
+
+        # beyond the fixed array: rejected with an error code, nothing launched
+        n_big = 40000
+        out = torch.zeros(n_big * 52, dtype=torch.uint8, device="cuda")  # large enough in any case
+        rc = lib.QTrkB200LocalizeDeviceNoAlloc(t.handle, C.c_void_p(dev[0].data_ptr()), 200, 0, abi.QTrkU16, n_big,
+                                               None, C.c_void_p(out.data_ptr()), C.c_void_p(stream))
+        assert rc == -3
+        assert "fixed array holds" in t.GetWarnings()
