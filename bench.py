@@ -49,10 +49,10 @@ PIXEL_NM = 100.0  # stated pixel size for nm error reporting
 
 
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from qtrk_b200 import replicas
+
+    e = replicas.env()
+    return e.world_size, e.rank, e.local_rank
 
 
 def measured_peaks() -> tuple[dict, str]:
@@ -222,16 +222,12 @@ def main(argv=None) -> int:
 
     import torch
 
-    ws, rank, local = dist_env()
-    if ws > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
+    from qtrk_b200 import replicas
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
-    else:
-        torch.cuda.set_device(0)
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local if ws > 1 else 0)
     dev = torch.device("cuda", torch.cuda.current_device())
+    replicas.init("nccl", timeout_s=300, device=dev)
 
     from qtrk_b200 import abi
     from qtrk_b200.tracker import QTrkInstance
@@ -250,16 +246,10 @@ def main(argv=None) -> int:
         trk.SetRadialZLUT(np.ascontiguousarray(np.broadcast_to(lut, (N_ROIS,) + lut.shape[1:])))
     trk.SetLocalizationMode(wl.mode)
 
-    def barrier():
-        if ws > 1:
-            torch.distributed.barrier()
+    barrier = replicas.barrier
 
     def max_over_ranks(x: float) -> float:
-        if ws == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.reduce_max(x, device=dev)
 
     # ---- device-resident path (value) ----
     d_rois = torch.from_numpy(wl.rois.view(np.int16)).to(dev)
@@ -289,7 +279,7 @@ def main(argv=None) -> int:
     barrier()
     dev_ms = ev0.elapsed_time(ev1)
     dev_ms_max = max_over_ranks(dev_ms)
-    value = ws * N_ROIS * args.steps / (dev_ms_max / 1e3)
+    value = replicas.aggregate_rate(N_ROIS * args.steps, ws, dev_ms_max / 1e3)
     launches_value = trk.KernelLaunchCount() - launches0
     # per-launch duration of the localization kernel (one launch per step on this stream)
     kernel_ms = dev_ms / args.steps
@@ -393,8 +383,7 @@ def main(argv=None) -> int:
     }
     trk.Destroy()
     if ws > 1:
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
+        replicas.finalize()
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0

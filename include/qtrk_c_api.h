@@ -218,6 +218,17 @@ QTRK_API int QTRK_CALLCONV QTrkB200GetLastError(char *dst, int maxStrLen);
 QTRK_API int64_t QTRK_CALLCONV QTrkB200GetKernelLaunchCount(struct QueuedTracker *qtrk);
 
 /*
+ * Z-LUT bias correction table, table[bead][bias_plane] (bias_planes wide, count beads high); NULL
+ * removes it. Replaces QueuedTracker::SetZLUTBiasCorrection (cputrack/QueuedTracker.h:334,
+ * QueuedTracker.cpp:178-182; LabVIEW: qtrk_set_zlut_bias_table, lv_queuetrk_api.cpp:467-480).
+ * While set, every z is corrected by QueuedTracker::ZLUTBiasCorrection's four fixed-point steps
+ * (QueuedTracker.cpp:115-140) on the device. QTrkSetRadialZLUT removes the table, as the
+ * reference does (QueuedCPUTracker.cpp:368-369).
+ */
+QTRK_API void QTRK_CALLCONV QTrkB200SetZLUTBiasTable(struct QueuedTracker *qtrk, const float *table, int bias_planes,
+                                                     int count);
+
+/*
  * Localize `count` ROIs that are already resident in device memory, on the caller's CUDA
  * stream (cudaStream_t passed as void*; NULL = legacy default stream). ROI i starts at
  * d_pixels + i * roi_stride_bytes; rows are `pitch` bytes apart. d_jobs (device,

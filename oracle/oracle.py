@@ -217,6 +217,7 @@ class PortOracle:
                                                P, _f64p, P]),
             "oracle_joint_refine": (None, [_f64p, C.c_int, C.c_int, C.c_double, _f64p, _f32p, C.c_int, C.c_int,
                                            C.c_int, C.c_double, C.c_double, P, C.c_int]),
+            "oracle_zlut_bias_correct": (C.c_double, [C.c_double, C.c_int, _f32p, C.c_int, C.c_int, C.c_int]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -271,6 +272,10 @@ class PortOracle:
         self.lib.oracle_gauss5(img, img.shape[1], img.shape[0], np.ascontiguousarray(init, np.float64), iterations,
                                out, _ptr(fisher))
         return (out, fisher.reshape(5, 5)) if with_fisher else out
+
+    def zlut_bias_correct(self, z, planes, table, bead):
+        table = np.ascontiguousarray(table, np.float32)
+        return self.lib.oracle_zlut_bias_correct(float(z), planes, table, table.shape[1], table.shape[0], int(bead))
 
     def radial_bin_window(self, n):
         out = np.zeros(n)

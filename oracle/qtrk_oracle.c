@@ -463,6 +463,28 @@ ORACLE_API void oracle_build_lut_bead(const oracle_config *c, const double *img,
     free(prof);
 }
 
+/* QueuedTracker::ZLUTBiasCorrection, QueuedTracker.cpp:115-140, with Interpolate1D of
+ * utils.h:60-67 on the bead's row of table[count][tw]. */
+ORACLE_API double oracle_zlut_bias_correct(double z, int planes, const float *table, int tw, int count, int bead)
+{
+    if (!table || bead < 0 || bead >= count) return z;
+    const float *row = table + (size_t)bead * tw;
+    double pos = z;
+    for (int k = 0; k < 4; k++) {
+        double tblpos = pos / planes * tw;
+        int fx = (int)tblpos;
+        double bias;
+        if (fx < 0)
+            bias = row[0];
+        else if (fx >= tw - 1)
+            bias = row[tw - 1];
+        else
+            bias = (row[fx + 1] - row[fx]) * (tblpos - fx) + row[fx];
+        pos = z - bias;
+    }
+    return pos;
+}
+
 /* ======================= extensions (no reference counterpart) ======================= */
 
 /* Integrated-Gaussian pixel model of utils.cpp:393-402 with exact erf; used by the

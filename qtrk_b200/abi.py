@@ -169,6 +169,7 @@ PROTOTYPES = {
 B200_PROTOTYPES = {
     "QTrkB200GetLastError": (C.c_int, [C.c_char_p, C.c_int]),
     "QTrkB200GetKernelLaunchCount": (C.c_int64, [_TRK]),
+    "QTrkB200SetZLUTBiasTable": (None, [_TRK, _P, C.c_int, C.c_int]),
     "QTrkB200LocalizeDevice": (C.c_int, [_TRK, _P, C.c_int, C.c_int64, C.c_int, C.c_int, _P, _P, _P]),
     "QTrkB200LocalizeDeviceNoAlloc": (C.c_int, [_TRK, _P, C.c_int, C.c_int64, C.c_int, C.c_int, _P, _P, _P]),
 }

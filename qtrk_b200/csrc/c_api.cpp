@@ -484,6 +484,11 @@ QTRK_API int64_t QTRK_CALLCONV QTrkB200GetKernelLaunchCount(QueuedTracker *q)
     return q ? T(q)->LaunchCount() : 0;
 }
 
+QTRK_API void QTRK_CALLCONV QTrkB200SetZLUTBiasTable(QueuedTracker *q, const float *table, int bias_planes, int count)
+{
+    guarded(q, "QTrkB200SetZLUTBiasTable", [&](Tracker *t) { t->SetZLUTBiasTable(table, bias_planes, count); });
+}
+
 QTRK_API int QTRK_CALLCONV QTrkB200LocalizeDevice(QueuedTracker *q, const void *d_pixels, int pitch,
                                                   int64_t roi_stride_bytes, QTRK_PixelDataType_t pdt, int count,
                                                   const LocalizationJob *d_jobs, LocalizationResult *d_results,

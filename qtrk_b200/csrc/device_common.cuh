@@ -135,7 +135,7 @@ __device__ __forceinline__ bool check_boundaries(float cx, float cy, float radiu
 // The weights are indexed from 0 even when the window is clipped at the array start, as in
 // the reference.
 template <typename Get>
-__device__ double max_interp7(Get at, int len, int iMax, const float (&wts)[7])
+__device__ inline double max_interp7(Get at, int len, int iMax, const float (&wts)[7])
 {
     const int startPos = max(iMax - 3, 0);
     const int endPos = min(iMax + 4, len);
@@ -165,7 +165,7 @@ __device__ double max_interp7(Get at, int len, int iMax, const float (&wts)[7])
 // call; every lane returns the result). maxPos = iMax - b/(2a) with a = A/d, b = B/d, so the
 // determinant d cancels and one division remains; |a| < 1e-9 is tested as |A| < 1e-9 |d|.
 template <typename Get>
-__device__ double max_interp7_warp(Get at, int len, int iMax, const float (&wts)[7])
+__device__ inline double max_interp7_warp(Get at, int len, int iMax, const float (&wts)[7])
 {
     const int lane = threadIdx.x & 31;
     const int startPos = max(iMax - 3, 0);
@@ -247,7 +247,7 @@ __device__ __forceinline__ float finish_pixel(float v, int i, const TrackParams 
 }
 
 template <class G>
-__device__ void load_roi(const G &g, float *img, const uint8_t *src, int pitch, const TrackParams &P, int bead)
+__device__ inline void load_roi(const G &g, float *img, const uint8_t *src, int pitch, const TrackParams &P, int bead)
 {
     const int W = P.width, H = P.height, n = W * H;
     const int bpp = P.pdt == 0 ? 1 : (P.pdt == 1 ? 2 : 4);
@@ -381,7 +381,7 @@ __device__ __forceinline__ int lanes_per_bin(int nbins)
 // radius minr + rstep*i (the image mean when fewer than 4 are in bounds), times the
 // radial weight. Directions come from the quadrant table at stride `stride`.
 // -------------------------------------------------------------------------------------
-__device__ void qi_quadrant_profiles(const float *img, int W, int H, float cx, float cy, float mean, int nr, int nang,
+__device__ inline void qi_quadrant_profiles(const float *img, int W, int H, float cx, float cy, float mean, int nr, int nang,
                                      int stride, float minr, float rstep, const float2 *dirs, const float *rweights,
                                      float *qprof)
 {
@@ -444,7 +444,7 @@ __device__ __forceinline__ float2 fft_tw(const float2 *tw, int k, bool inverse)
     return w;
 }
 
-__device__ void warp_fft(float2 *buf, int L, int log2L, const float2 *tw, bool inverse)
+__device__ inline void warp_fft(float2 *buf, int L, int log2L, const float2 *tw, bool inverse)
 {
     const int lane = threadIdx.x & 31;
     int s = 1;
@@ -503,7 +503,7 @@ __device__ __forceinline__ float2 qi_concat(const float *qprof, int nr, int n)
 // FFT(reverse(p))* = e^{-2 pi i k/L} FFT(p) for real p, the product the reference forms
 // from two forward FFTs equals e^{-2 pi i k/L} P[k]^2, so one forward and one inverse
 // FFT per iteration give both axes. Result: ac[n] = (out_x[n], out_y[n]). Warp 0 only.
-__device__ void qi_autoconv_fft(const float *qprof, int nr, float2 *A, float2 *ac, const float2 *tw)
+__device__ inline void qi_autoconv_fft(const float *qprof, int nr, float2 *A, float2 *ac, const float2 *tw)
 {
     const int lane = threadIdx.x & 31;
     const int L = 2 * nr, log2L = ilog2_pow2(L);
@@ -527,7 +527,7 @@ __device__ void qi_autoconv_fft(const float *qprof, int nr, float2 *A, float2 *a
 }
 
 // Same quantity by direct summation (any L; used when 2nr is not a power of two). All threads.
-__device__ void qi_autoconv_direct(const float *qprof, int nr, float2 *A, float2 *ac)
+__device__ inline void qi_autoconv_direct(const float *qprof, int nr, float2 *A, float2 *ac)
 {
     const int L = 2 * nr;
     for (int n = threadIdx.x; n < L; n += blockDim.x) A[n] = qi_concat(qprof, nr, n);
@@ -551,7 +551,7 @@ __device__ void qi_autoconv_direct(const float *qprof, int nr, float2 *A, float2
 // bilinear samples on the full circle (FP64 sum), or `mean` when no more than 4 samples
 // are in bounds; then NormalizeRadialProfile (utils.cpp:230-261) when asked.
 // -------------------------------------------------------------------------------------
-__device__ void radial_profile(const float *img, int W, int H, float cx, float cy, float mean, int nb, int nang,
+__device__ inline void radial_profile(const float *img, int W, int H, float cx, float cy, float mean, int nb, int nang,
                                float minr, float rstep, const float2 *dirs, float *prof, bool normalize,
                                double *red)
 {
@@ -624,7 +624,7 @@ __device__ void radial_profile(const float *img, int W, int H, float cx, float c
 // CPUTracker::LUTProfileCompare, cpu_tracker.cpp:791-868 (plain form): one warp per plane
 // group, lanes over radial bins. scores[k] = -sum_r (w_r (p_r - L_kr))^2 with the difference
 // taken in FP32 and squared/accumulated in FP64, as the reference does.
-__device__ void zlut_scores_plain(const float *prof, const float *lut, int planes, int nb, const float *weights,
+__device__ inline void zlut_scores_plain(const float *prof, const float *lut, int planes, int nb, const float *weights,
                                   double *scores)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -641,6 +641,30 @@ __device__ void zlut_scores_plain(const float *prof, const float *lut, int plane
         if (lane == 0) scores[k] = -acc;
     }
     __syncthreads();
+}
+
+// QueuedTracker::ZLUTBiasCorrection, cputrack/QueuedTracker.cpp:115-140: four fixed-point steps
+// pos = z - bias(pos), bias read from the bead's row of the table by Interpolate1D
+// (cputrack/utils.h:60-67: truncating index, clamped to the first/last entry).
+__device__ __forceinline__ float zlut_bias_correct(float z, int planes, const float *table, int tw, int tcount,
+                                                   int bead)
+{
+    if (!table || bead < 0 || bead >= tcount || tw <= 0) return z;
+    const float *row = table + (size_t)bead * tw;
+    float pos = z;
+    for (int k = 0; k < 4; k++) {
+        const float tblpos = pos / (float)planes * tw;
+        const int fx = (int)tblpos;
+        float bias;
+        if (fx < 0)
+            bias = row[0];
+        else if (fx >= tw - 1)
+            bias = row[tw - 1];
+        else
+            bias = (row[fx + 1] - row[fx]) * (tblpos - fx) + row[fx];
+        pos = z - bias;
+    }
+    return pos;
 }
 
 // -------------------------------------------------------------------------------------
@@ -684,7 +708,7 @@ __device__ __forceinline__ GaussAxisTerms gauss_axis_terms(int c, float p, float
 // CPUTracker::Compute2DGaussianMLE, cpu_tracker.cpp:514-589. col: 3*W floats, row: 3*H floats
 // of shared scratch. px/py enter as the start position (the COM) and leave as the estimate.
 template <class G>
-__device__ void gauss4_mle(const G &g, const float *img, int W, int H, float mean, float &px, float &py, int iters,
+__device__ inline void gauss4_mle(const G &g, const float *img, int W, int H, float mean, float &px, float &py, int iters,
                            float sigma, float *col, float *row)
 {
     float I0 = mean * 0.5f * (float)W * (float)H;
@@ -782,7 +806,7 @@ __device__ __forceinline__ bool solve5(double (&A)[5][5], double (&b)[5], double
 // gradients in FP32 per pixel, FP64 reduction and an FP64 5x5 solve per step. p[] = {x, y,
 // I0, bg, sigma}; col/row: 5*W and 5*H floats of shared scratch.
 template <class G>
-__device__ void gauss5_mle(const G &g, const float *img, int W, int H, float (&p)[5], int iters, float *col,
+__device__ inline void gauss5_mle(const G &g, const float *img, int W, int H, float (&p)[5], int iters, float *col,
                            float *row)
 {
     for (int it = 0; it < iters; it++) {

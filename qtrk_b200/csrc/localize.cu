@@ -151,7 +151,7 @@ __device__ float z_localize(const SmemView &s, const TrackParams &P, float mean,
         auto at = [&](int i) { return scores[i]; };
         const int im = warp_argmax(at, P.lut_planes);
         const float z = (float)max_interp7_warp(at, P.lut_planes, im, kZLUTWeights);
-        if (threadIdx.x == 0) s.misc[2] = z;
+        if (threadIdx.x == 0) s.misc[2] = zlut_bias_correct(z, P.lut_planes, P.zbias, P.zbias_w, P.zbias_count, bead);
     }
     __syncthreads();
     return s.misc[2];

@@ -61,6 +61,11 @@ struct TrackParams {
     void *zprof_bf16;
     int zprof_nbp;
 
+    // Z-LUT bias table (QueuedTracker::ZLUTBiasCorrection, cputrack/QueuedTracker.cpp:115-140):
+    // [zbias_count][zbias_w] or nullptr
+    const float *zbias;
+    int zbias_w, zbias_count;
+
     // 2D Gaussian MLE (cputrack/cpu_tracker.cpp:514-589)
     int g_iterations;
     float g_sigma;

@@ -306,6 +306,7 @@ Tracker::~Tracker()
     cudaFree(d_cmp_);
     cudaFree(d_calib_off_);
     cudaFree(d_calib_gain_);
+    cudaFree(d_zbias_);
     cudaFree(d_lut_bf16_);
     cudaFree(d_lut_norm_);
     cudaFree(d_dev_zprof_);
@@ -325,6 +326,9 @@ TrackParams Tracker::Params(int pdt) const
     P.lut_planes = lut_planes_;
     P.z_weights = have_zw_ ? d_zw_ : nullptr;
     P.cmp_scores = cmp_enabled_ ? d_cmp_ : nullptr;
+    P.zbias = d_zbias_;
+    P.zbias_w = zbias_w_;
+    P.zbias_count = zbias_count_;
     P.calib_offset = d_calib_off_;
     P.calib_gain = d_calib_gain_;
     P.calib_count = (d_calib_off_ || d_calib_gain_) ? calib_count_ : 0;
@@ -520,6 +524,9 @@ ZMatchParams Tracker::TensorCoreParams() const
     Q.lut = d_lut_;
     Q.weights = have_zw_ ? d_zw_ : nullptr;
     Q.error_flag = d_err_;
+    Q.zbias = d_zbias_;
+    Q.zbias_w = zbias_w_;
+    Q.zbias_count = zbias_count_;
     return Q;
 }
 
@@ -831,6 +838,9 @@ void Tracker::SetRadialZLUT(const float *data, int count, int planes)
     cudaFree(d_cmp_);
     d_lut_ = nullptr;
     d_cmp_ = nullptr;
+    cudaFree(d_zbias_);  // a new LUT drops the bias table, as QueuedCPUTracker.cpp:368-369
+    d_zbias_ = nullptr;
+    zbias_w_ = zbias_count_ = 0;
     const int res = cfg.zlut_radialsteps;
     const size_t total = (size_t)std::max(count, 0) * std::max(planes, 0) * res;
     if (total > 0) {
@@ -889,6 +899,25 @@ void Tracker::SetRadialWeights(const float *w)
         have_zw_ = false;
     }
     tc_lut_stale_ = true;
+}
+
+// QueuedTracker::SetZLUTBiasCorrection (cputrack/QueuedTracker.cpp:178-182): table[bead][bias_plane],
+// bias_planes wide and count (beads) high; nullptr removes it.
+void Tracker::SetZLUTBiasTable(const float *table, int bias_planes, int count)
+{
+    DeviceGuard dg(device_);
+    WaitIdleForReconfigure();
+    std::lock_guard<std::mutex> lk(mu_);
+    cudaFree(d_zbias_);
+    d_zbias_ = nullptr;
+    zbias_w_ = zbias_count_ = 0;
+    if (table && bias_planes > 0 && count > 0) {
+        const size_t n = (size_t)bias_planes * count;
+        CheckCuda(cudaMalloc(&d_zbias_, n * 4), "cudaMalloc(bias table)");
+        CheckCuda(cudaMemcpy(d_zbias_, table, n * 4, cudaMemcpyHostToDevice), "upload bias table");
+        zbias_w_ = bias_planes;
+        zbias_count_ = count;
+    }
 }
 
 void Tracker::EnableRadialZLUTCompareProfile(bool enabled)

@@ -72,6 +72,7 @@ class Tracker : public QueuedTracker {
     std::string GetWarnings();
 
     // Extensions
+    void SetZLUTBiasTable(const float *table, int bias_planes, int count);
     int LocalizeDevice(const void *d_pixels, int pitch, int64_t roi_stride, int pdt, int count,
                        const LocalizationJob *d_jobs, LocalizationResult *d_results, cudaStream_t stream);
     // LocalizeDevice with caller-supplied profile scratch (scratch_bytes); allocates nothing.
@@ -155,6 +156,10 @@ class Tracker : public QueuedTracker {
     __nv_bfloat16 *d_dev_zprof_bf16_ = nullptr;
     int4 *d_dev_tiles_ = nullptr;
     int dev_scratch_rois_ = 0;
+
+    // Z-LUT bias table
+    float *d_zbias_ = nullptr;
+    int zbias_w_ = 0, zbias_count_ = 0;
 
     // pixel calibration
     float *d_calib_off_ = nullptr, *d_calib_gain_ = nullptr;

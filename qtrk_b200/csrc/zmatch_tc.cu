@@ -27,6 +27,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include "device_common.cuh"
 #include "kernels.h"
 #include "zmatch_tc.h"
 
@@ -40,7 +41,7 @@ constexpr float kBoundScale = 0.001953125f;  // 2^-9 (see above)
 constexpr int kTmemCols = 256;
 constexpr uint32_t kWaitLimit = 1u << 20;  // try_wait polls before the kernel gives up
 
-__device__ const float kZLUTWeights[7] = {0.15f, 0.5f, 0.85f, 1.0f, 0.85f, 0.5f, 0.15f};
+__device__ const float kZLUTWeightsTC[7] = {0.15f, 0.5f, 0.85f, 1.0f, 0.85f, 0.5f, 0.15f};
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
@@ -296,7 +297,7 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
                 for (int i = 0; i < np; i++) {
                     const int k = s0 + i;
                     const double y = (k == bk) ? best_e : exact_score(prof, lut + (size_t)k * nb, Q.weights, nb);
-                    const double x = k - bk, wt = kZLUTWeights[i], sq = x * x;
+                    const double x = k - bk, wt = kZLUTWeightsTC[i], sq = x * x;
                     Sx += x * wt;
                     Sy += y * wt;
                     Sx2 += sq * wt;
@@ -311,7 +312,7 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
                 const double B = Sx4 * (Sxy * Sw - Sy * Sx) - Sx3 * (Sx2y * Sw - Sy * Sx2) + Sx2 * (Sx2y * Sx - Sxy * Sx2);
                 if (!(fabs(A) < 1e-9 * fabs(d))) zz = bk - B / (2 * A);
             }
-            z = (float)zz;
+            z = zlut_bias_correct((float)zz, Q.planes, Q.zbias, Q.zbias_w, Q.zbias_count, bead);
         }
         reinterpret_cast<float *>(Q.results)[(size_t)my_roi * 13 + 8] = z;
     }

@@ -26,6 +26,8 @@ struct ZMatchParams {
                                      // `uniform_bead`
     int count, uniform_bead;
     LocalizationResult *results;     // z (word 8 of each 13-word record) is written
+    const float *zbias;              // Z-LUT bias table [zbias_count][zbias_w] or nullptr
+    int zbias_w, zbias_count;
     unsigned *error_flag;            // set to 1 if an MMA completion wait gave up
 };
 

@@ -1,0 +1,81 @@
+"""GPU tests of the Z-LUT bias correction and the Gaussian MLE forms against the FP64 oracle."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from golden_io import load
+from qtrk_b200 import abi, synth
+from qtrk_b200.tracker import QTrkInstance
+
+pytestmark = pytest.mark.gpu
+
+
+def test_zlut_bias_table(port):
+    """QueuedTracker::ZLUTBiasCorrection (QueuedTracker.cpp:115-140) applied on the device."""
+    g = load("config1_60x60_f32.npz")
+    rois = g["rois"].astype(np.float32)
+    planes = g["lut"].shape[1]
+    rng = np.random.default_rng(5)
+    table = np.ascontiguousarray(rng.uniform(-0.8, 0.8, (1, 37)).astype(np.float32))
+    for extra in (0, abi.LT_B200_ZMatchBF16):
+        with QTrkInstance(g["settings"]) as t:
+            t.SetRadialZLUT(g["lut"])
+            t.SetLocalizationMode(int(g["mode"]) | extra)
+            plain = t.Localize(rois)
+            t.lib.QTrkB200SetZLUTBiasTable(t.handle, table.ctypes.data_as(C.c_void_p), 37, 1)
+            corr = t.Localize(rois)
+            t.lib.QTrkB200SetZLUTBiasTable(t.handle, None, 0, 0)
+            back = t.Localize(rois)
+        expect = np.array([port.zlut_bias_correct(z, planes, table, 0) for z in plain["pos"][:, 2]])
+        assert np.abs(corr["pos"][:, 2] - expect).max() < 1e-4
+        assert np.array_equal(back["pos"][:, 2], plain["pos"][:, 2])
+        assert np.array_equal(corr["pos"][:, :2], plain["pos"][:, :2])
+
+
+def test_gaussian_4p_cta_kernel_matches_reference(ref):
+    """ROIs above 32x32 take the CTA kernel's MLE: same results as the reference's
+    CPUTracker::Compute2DGaussianMLE (cpu_tracker.cpp:514-589) on every ROI where that
+    diagonal-Newton iteration has converged (last step < 1e-5 px; where it has not, the
+    reference's float iteration is ill-conditioned and even an FP64 restatement departs from it)."""
+    rng = np.random.Generator(np.random.PCG64(53))
+    n, w, it = 128, 36, 12
+    cx = 18 + rng.uniform(-2, 2, n)
+    cy = 18 + rng.uniform(-2, 2, n)
+    ph = np.exp(rng.uniform(np.log(20000), np.log(60000), n))
+    imgs = rng.poisson(synth.gaussian_spots(n, w, cx, cy, 3.0, ph, 10.0)).astype(np.float32)
+    s = abi.settings(width=w, height=w, gauss2D_sigma=3.0, gauss2D_iterations=it, qi_minradius=1, zlut_minradius=1)
+    with QTrkInstance(s) as t:
+        t.SetLocalizationMode(abi.LT_Gaussian2D)
+        cta = t.Localize(imgs)
+    r = np.array([ref.gauss2d(im, ref.com(im)[:2], it, 3.0) for im in imgs])
+    r1 = np.array([ref.gauss2d(im, ref.com(im)[:2], it - 1, 3.0) for im in imgs])
+    conv = np.abs(r[:, :2] - r1[:, :2]).max(1) < 1e-5
+    assert conv.mean() > 0.75
+    assert np.abs(cta["pos"][conv, :2] - r[conv, :2]).max() < 1e-3
+    assert np.abs(cta["firstGuess"] - np.array([ref.com(im)[:2] for im in imgs])).max() < 1e-4
+
+
+def test_gaussian_5p_matches_fp64_oracle_and_crlb(port):
+    """5-parameter (x, y, I0, bg, sigma) full-Newton MLE vs the FP64 oracle and the Cramer-Rao bound."""
+    wl = synth.config3(600, seed=52)
+    s = wl.settings
+    s.gauss2D_iterations = 10
+    with QTrkInstance(s) as t:
+        t.SetLocalizationMode(abi.LT_Gaussian2D | abi.LT_B200_Gaussian5P)
+        r = t.Localize(wl.rois)
+    dx, crlb = [], []
+    for i in range(600):
+        img = wl.rois[i].astype(np.float64)
+        com = port.com(img)
+        init = np.array([r["firstGuess"][i, 0], r["firstGuess"][i, 1], com[2] * 0.5 * 256, com[2] * 0.5, 1.5])
+        o, fisher = port.gauss5(img, init, 10, with_fisher=True)
+        dx.append(max(abs(r["pos"][i, 0] - o[0]), abs(r["pos"][i, 1] - o[1])))
+        assert abs(r["pos"][i, 2] - o[4]) < 1e-3          # sigma is returned in pos.z
+        crlb.append(np.sqrt(np.diag(np.linalg.inv(fisher)))[:2])
+    assert max(dx) < 1e-3, max(dx)
+    # errors about the truth, each divided by that ROI's Cramer-Rao bound, have unit scatter
+    # for an efficient estimator (600 ROIs: the sample std is within a few percent of 1)
+    err = np.stack([r["pos"][:, 0] - wl.true_xyz[:, 0], r["pos"][:, 1] - wl.true_xyz[:, 1]], 1)
+    ratio = (err / np.array(crlb)).std(0)
+    assert (ratio > 0.8).all() and (ratio < 1.25).all(), ratio
