@@ -266,4 +266,54 @@ QTRK_API int QTRK_CALLCONV QTrkB200LocalizeDeviceNoAlloc(struct QueuedTracker *q
                                                          int count, const LocalizationJob *d_jobs,
                                                          LocalizationResult *d_results, void *stream);
 
+/*
+ * Request server: real-time localization of frames from several instances on one GPU. No
+ * counterpart in the reference (its callers run one QueuedTracker per camera and poll each).
+ * A server owns device "lanes" (one stream, a 48 MiB pixel buffer and room for 8,192 ROIs each);
+ * the number of lanes is device_memory_budget divided by a lane's size (at least 1, at most 16).
+ * Instances are attached once; frames are then submitted from any thread. A dispatcher thread
+ * admits waiting frames to free lanes in arrival order, merges waiting frames of the same
+ * instance and pixel type into one launch while they fit the lane (continuous batching), copies
+ * each frame's ROI band to the lane and replays a CUDA graph holding the localization kernel and
+ * the result copy (one graph per lane, instance and power-of-two ROI-count bucket). A frame's
+ * results are the ones QTrkScheduleFrame gives for it: ROIs outside the frame are skipped and
+ * result i carries zlutIndex = i + job->zlutIndex. The tensor-core Z match is not used here.
+ */
+typedef struct QTrkB200ServeStats {
+    int64_t frames;            /* frames completed */
+    int64_t rois;              /* ROIs localized */
+    int64_t launches;          /* graph launches (one per lane batch) */
+    int64_t graphs;            /* graphs captured */
+    int64_t waits_for_memory;  /* frames that arrived while every lane was busy or frames waited */
+    int32_t lanes;             /* lanes the memory budget allowed */
+    int32_t reserved;
+    double elapsed_s;          /* first submission to last completion */
+    double p50_ms, p99_ms, max_ms;  /* per-frame latency, submission to results on the host */
+} QTrkB200ServeStats;
+
+QTRK_API void *QTRK_CALLCONV QTrkB200ServerCreate(int device, int64_t device_memory_budget);
+QTRK_API void QTRK_CALLCONV QTrkB200ServerDestroy(void *server);
+/* Attach an instance (on the server's GPU); returns its index, or -1. The instance must outlive
+ * the server; its LUT and mode may change between frames (each launch reads them then). */
+QTRK_API int QTRK_CALLCONV QTrkB200ServerAttach(void *server, struct QueuedTracker *qtrk);
+/* Submit one frame of an attached instance. The frame (host memory, pitch in bytes) must stay
+ * valid until the request completes. Returns the request id (> 0), or -1 on error (more than
+ * 8,192 ROIs, a ROI band larger than a lane, a bad argument). */
+QTRK_API int64_t QTRK_CALLCONV QTrkB200ServerSubmitFrame(void *server, int instance, const void *frame, int pitch,
+                                                         int width, int height, const ROIPosition *positions,
+                                                         int numROI, QTRK_PixelDataType_t pdt,
+                                                         const LocalizationJob *jobInfo);
+/* Results of a request: the number written (the request is then forgotten), -1 while it is
+ * pending, -2 for an unknown id, -3 when its launch failed (QTrkB200GetLastError says why). */
+QTRK_API int QTRK_CALLCONV QTrkB200ServerPoll(void *server, int64_t request, LocalizationResult *results,
+                                              int maxResults);
+QTRK_API void QTRK_CALLCONV QTrkB200ServerGetStats(void *server, QTrkB200ServeStats *stats);
+/* Restart the statistics (frames, ROIs, launches, waits, latencies, elapsed time); captured
+ * graphs and lanes are kept. Frames in flight are counted by the new statistics. */
+QTRK_API void QTRK_CALLCONV QTrkB200ServerResetStats(void *server);
+/* hold != 0: submitted frames wait and no new launch starts (launches in flight finish);
+ * hold == 0: admission resumes and the frames that waited are batched together. For callers that
+ * collect the frames of one trigger (several cameras) before they are localized together. */
+QTRK_API void QTRK_CALLCONV QTrkB200ServerHold(void *server, int hold);
+
 #endif /* QTRK_B200_C_API_H */

@@ -109,6 +109,17 @@ class ROIPosition(C.Structure):
     _fields_ = [("x", C.c_int), ("y", C.c_int)]
 
 
+class QTrkB200ServeStats(C.Structure):
+    """Request-server statistics (library extension; 80 bytes)."""
+
+    _fields_ = [
+        ("frames", C.c_int64), ("rois", C.c_int64), ("launches", C.c_int64), ("graphs", C.c_int64),
+        ("waits_for_memory", C.c_int64), ("lanes", C.c_int32), ("reserved", C.c_int32),
+        ("elapsed_s", C.c_double), ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double),
+    ]
+
+
+assert C.sizeof(QTrkB200ServeStats) == 80
 assert C.sizeof(LocalizationJob) == 24
 assert C.sizeof(LocalizationResult) == 52
 assert C.sizeof(QTrkSettings) == 84
@@ -172,6 +183,14 @@ B200_PROTOTYPES = {
     "QTrkB200SetZLUTBiasTable": (None, [_TRK, _P, C.c_int, C.c_int]),
     "QTrkB200LocalizeDevice": (C.c_int, [_TRK, _P, C.c_int, C.c_int64, C.c_int, C.c_int, _P, _P, _P]),
     "QTrkB200LocalizeDeviceNoAlloc": (C.c_int, [_TRK, _P, C.c_int, C.c_int64, C.c_int, C.c_int, _P, _P, _P]),
+    "QTrkB200ServerCreate": (_P, [C.c_int, C.c_int64]),
+    "QTrkB200ServerDestroy": (None, [_P]),
+    "QTrkB200ServerAttach": (C.c_int, [_P, _TRK]),
+    "QTrkB200ServerSubmitFrame": (C.c_int64, [_P, C.c_int, _P, C.c_int, C.c_int, C.c_int, _P, C.c_int, C.c_int, _P]),
+    "QTrkB200ServerPoll": (C.c_int, [_P, C.c_int64, _P, C.c_int]),
+    "QTrkB200ServerGetStats": (None, [_P, _P]),
+    "QTrkB200ServerHold": (None, [_P, C.c_int]),
+    "QTrkB200ServerResetStats": (None, [_P]),
 }
 
 

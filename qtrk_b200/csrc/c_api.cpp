@@ -15,6 +15,7 @@
 
 #include "kernels.h"
 #include "qtrk_c_api.h"
+#include "serve.h"
 #include "tracker.h"
 
 using qtrk::Tracker;
@@ -501,3 +502,79 @@ QTRK_API int QTRK_CALLCONV QTrkB200LocalizeDevice(QueuedTracker *q, const void *
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------
+// Request server
+// ---------------------------------------------------------------------------------------
+QTRK_API void *QTRK_CALLCONV QTrkB200ServerCreate(int device, int64_t device_memory_budget)
+{
+    try {
+        return new qtrk::Server(device, device_memory_budget);
+    } catch (const std::exception &e) {
+        set_last_error(std::string("QTrkB200ServerCreate: ") + e.what());
+        return nullptr;
+    }
+}
+
+QTRK_API void QTRK_CALLCONV QTrkB200ServerDestroy(void *server)
+{
+    delete static_cast<qtrk::Server *>(server);
+}
+
+QTRK_API int QTRK_CALLCONV QTrkB200ServerAttach(void *server, QueuedTracker *q)
+{
+    if (!server || !q) {
+        set_last_error("QTrkB200ServerAttach: null argument");
+        return -1;
+    }
+    try {
+        return static_cast<qtrk::Server *>(server)->Attach(T(q));
+    } catch (const std::exception &e) {
+        set_last_error(std::string("QTrkB200ServerAttach: ") + e.what());
+        return -1;
+    }
+}
+
+QTRK_API int64_t QTRK_CALLCONV QTrkB200ServerSubmitFrame(void *server, int instance, const void *frame, int pitch,
+                                                         int width, int height, const ROIPosition *positions,
+                                                         int numROI, QTRK_PixelDataType_t pdt,
+                                                         const LocalizationJob *jobInfo)
+{
+    if (!server) {
+        set_last_error("QTrkB200ServerSubmitFrame: null server");
+        return -1;
+    }
+    try {
+        return static_cast<qtrk::Server *>(server)->Submit(instance, frame, pitch, width, height, positions, numROI,
+                                                           (int)pdt, jobInfo);
+    } catch (const std::exception &e) {
+        set_last_error(std::string("QTrkB200ServerSubmitFrame: ") + e.what());
+        return -1;
+    }
+}
+
+QTRK_API int QTRK_CALLCONV QTrkB200ServerPoll(void *server, int64_t request, LocalizationResult *results,
+                                              int maxResults)
+{
+    if (!server) return -2;
+    qtrk::Server *sv = static_cast<qtrk::Server *>(server);
+    const int r = sv->Poll(request, results, maxResults);
+    if (r == -3) set_last_error("QTrkB200ServerPoll: " + sv->LastError());
+    return r;
+}
+
+QTRK_API void QTRK_CALLCONV QTrkB200ServerGetStats(void *server, QTrkB200ServeStats *stats)
+{
+    if (!server || !stats) return;
+    *stats = static_cast<qtrk::Server *>(server)->Stats();
+}
+
+QTRK_API void QTRK_CALLCONV QTrkB200ServerHold(void *server, int hold)
+{
+    if (server) static_cast<qtrk::Server *>(server)->Hold(hold != 0);
+}
+
+QTRK_API void QTRK_CALLCONV QTrkB200ServerResetStats(void *server)
+{
+    if (server) static_cast<qtrk::Server *>(server)->ResetStats();
+}

@@ -21,6 +21,11 @@ cudaError_t launch_localize(const TrackParams &P, const uint8_t *pixels, int pit
                             const int64_t *roi_offsets, const LocalizationJob *jobs, int count,
                             LocalizationResult *results, cudaStream_t stream);
 
+// The kernel node that launch_localize would launch for `count` ROIs (function, grid, block,
+// shared memory); the caller sets kernelParams to the 8 arguments of launch_localize's kernel
+// (P, pixels, pitch, roi_stride, roi_offsets, jobs, count, results). For explicitly built graphs.
+void localize_node(const TrackParams &P, int count, cudaKernelNodeParams &kp);
+
 // One BuildLUT plane: nbeads ROIs stacked at pitch*H; adds each profile to lut[bead][plane].
 cudaError_t launch_build_lut(const TrackParams &P, const uint8_t *pixels, int pitch, int nbeads, int plane,
                              const float2 *known_pos, bool normalize, float *lut, cudaStream_t stream);

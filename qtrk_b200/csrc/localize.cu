@@ -436,6 +436,23 @@ cudaError_t launch_localize(const TrackParams &P, const uint8_t *pixels, int pit
     return cudaGetLastError();
 }
 
+void localize_node(const TrackParams &P, int count, cudaKernelNodeParams &kp)
+{
+    kp = cudaKernelNodeParams{};
+    if (use_gauss_warp(P)) {
+        kp.func = reinterpret_cast<void *>(gauss_warp_kernel);
+        kp.gridDim = dim3((count + 7) / 8);
+        kp.blockDim = dim3(256);
+        kp.sharedMemBytes = gauss_warp_smem(P);
+    } else {
+        kp.func = (P.mode & kLT_Gaussian2D) && !(P.mode & kLT_QI) ? reinterpret_cast<void *>(localize_kernel<true>)
+                                                                   : reinterpret_cast<void *>(localize_kernel<false>);
+        kp.gridDim = dim3(count);
+        kp.blockDim = dim3(kBlockThreads);
+        kp.sharedMemBytes = P.smem_bytes;
+    }
+}
+
 cudaError_t launch_build_lut(const TrackParams &P, const uint8_t *pixels, int pitch, int nbeads, int plane,
                              const float2 *known_pos, bool normalize, float *lut, cudaStream_t stream)
 {

@@ -338,6 +338,14 @@ TrackParams Tracker::Params(int pdt) const
     return P;
 }
 
+TrackParams Tracker::AcquireLaunch(int pdt, cudaStream_t stream)
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    CheckCuda(cudaStreamWaitEvent(stream, lut_ready_, 0), "cudaStreamWaitEvent");
+    launches_++;
+    return Params(pdt);
+}
+
 void Tracker::AllocateSlots()
 {
     const QTrkSettings &s = cfg.base;

@@ -83,6 +83,9 @@ class Tracker : public QueuedTracker {
     void Warn(const std::string &msg);
     int device() const { return device_; }
     TrackParams Params(int pdt) const;  // current parameters for a launch
+    // Parameters for one launch that another component (the request server) puts on `stream`:
+    // the stream is ordered after pending LUT work and the launch is counted.
+    TrackParams AcquireLaunch(int pdt, cudaStream_t stream);
 
   private:
     struct Slot {

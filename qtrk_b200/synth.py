@@ -27,13 +27,16 @@ def profile(r: np.ndarray, zp: np.ndarray | float) -> np.ndarray:
     return np.exp(-r * r / (2 * s * s)) * np.cos(2 * np.pi * r / per)
 
 
-def render(w: int, h: int, cx: np.ndarray, cy: np.ndarray, zp: np.ndarray, bg: float, amp: float) -> np.ndarray:
-    """Noise-free expected pixel values, shape (n, h, w), float64, clamped at 0."""
-    ys = np.arange(h, dtype=np.float64)[None, :, None]
-    xs = np.arange(w, dtype=np.float64)[None, None, :]
-    r = np.sqrt((xs - cx[:, None, None]) ** 2 + (ys - cy[:, None, None]) ** 2)
-    lam = bg + amp * profile(r, np.asarray(zp, np.float64)[:, None, None])
-    return np.maximum(lam, 0.0)
+def render(w: int, h: int, cx: np.ndarray, cy: np.ndarray, zp: np.ndarray, bg: float, amp: float,
+           dtype=np.float64) -> np.ndarray:
+    """Noise-free expected pixel values, shape (n, h, w), clamped at 0 (float64 unless dtype says)."""
+    ys = np.arange(h, dtype=dtype)[None, :, None]
+    xs = np.arange(w, dtype=dtype)[None, None, :]
+    cx = np.asarray(cx, dtype)[:, None, None]
+    cy = np.asarray(cy, dtype)[:, None, None]
+    r = np.sqrt((xs - cx) ** 2 + (ys - cy) ** 2)
+    lam = dtype(bg) + dtype(amp) * profile(r, np.asarray(zp, dtype)[:, None, None])
+    return np.maximum(lam, dtype(0))
 
 
 @dataclass
@@ -163,3 +166,58 @@ def config4_stack(nbeads: int = 256, planes: int = 200, seed: int = 4, noise: bo
                      qi_radial_coverage=1.4, qi_angular_coverage=0.7, zlut_minradius=3.0, zlut_roi_coverage=0.9,
                      zlut_radial_coverage=48.5 / 33.0, zlut_angular_coverage=0.7, cuda_device=-2, numThreads=-1)
     return s, stack, np.stack([cx, cy], 1).astype(np.float32)
+
+
+@dataclass
+class ServedCamera:
+    """One tracker instance of the serving workload: frames tiled with ROIs, its own LUT stack."""
+    name: str
+    settings: abi.QTrkSettings
+    mode: int
+    frames: list                # 2-D frames (u8/u16), ROIs tiled on a grid
+    positions: np.ndarray       # (beads, 2) int32 ROI corners, the same in every frame
+    lut_stack: np.ndarray       # (planes, 1, w, w) f32 noise-free images for BuildLUT
+    lut_known_pos: np.ndarray
+
+
+def settings_square(w: int, **kw) -> abi.QTrkSettings:
+    """w x w ROIs with the radius span of settings_config2 scaled to the ROI (3 px to 0.47 w)."""
+    s = settings_config2(width=w, height=w)
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
+
+
+SERVING_CAMERAS = ((40, np.uint8, 2000, 100), (64, np.uint16, 1000, 150), (100, np.uint16, 300, 200),
+                   (128, np.uint8, 50, 200))
+
+
+def serving_fleet(n_frames: int = 2, seed: int = 5, cameras=SERVING_CAMERAS) -> list:
+    """Serving workload: four instances with ROI sizes 40/64/100/128 px, 2000/1000/300/50 beads per
+    frame, u8/u16/u16/u8 pixels, LUTs of 100/150/200/200 planes. Bead image: background + amplitude
+    p(r; 0.25 z) + Poisson (u8: 10 + 100 p, u16: 200 + 2000 p clipped to 4095); centres within
+    +-2 px of the ROI centre, z uniform over the LUT's planes."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    fleet = []
+    for w, dt, beads, planes in cameras:
+        bg, amp, top = (10.0, 100.0, 255) if dt == np.uint8 else (200.0, 2000.0, 4095)
+        cols = int(np.ceil(np.sqrt(beads)))
+        rows = (beads + cols - 1) // cols
+        ys, xs = np.divmod(np.arange(beads), cols)
+        positions = np.ascontiguousarray(np.stack([xs * w, ys * w], 1).astype(np.int32))
+        frames = []
+        for _ in range(n_frames):
+            cx = w / 2 + rng.uniform(-2, 2, beads)
+            cy = w / 2 + rng.uniform(-2, 2, beads)
+            z = rng.uniform(0.05 * planes, 0.95 * planes, beads)
+            lam = render(w, w, cx, cy, 0.25 * z, bg, amp, dtype=np.float32)
+            rois = np.minimum(rng.poisson(lam), top).astype(dt)
+            frame = np.zeros((rows * w, cols * w), dt)
+            for b in range(beads):
+                frame[ys[b] * w:(ys[b] + 1) * w, xs[b] * w:(xs[b] + 1) * w] = rois[b]
+            frames.append(frame)
+        kz = 0.25 * np.arange(planes, dtype=np.float64)
+        stack = render(w, w, np.full(planes, w / 2), np.full(planes, w / 2), kz, bg, amp).astype(np.float32)
+        fleet.append(ServedCamera(f"{w}x{w}-{np.dtype(dt).name}-{beads}beads", settings_square(w), MODE_QI_Z,
+                                  frames, positions, stack[:, None], np.array([[w / 2, w / 2]], np.float32)))
+    return fleet

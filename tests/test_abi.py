@@ -135,3 +135,9 @@ def test_create_without_gpu_fails_cleanly(qlib):
     # calls on a null instance are rejected, not crashed
     qlib.QTrkFlush(None)
     assert qlib.QTrkGetResultCount(None) == 0
+    # the request server needs a GPU too
+    assert not qlib.QTrkB200ServerCreate(0, 1 << 30)
+    assert "QTrkB200ServerCreate" in tracker.last_error()
+    assert qlib.QTrkB200ServerPoll(None, 1, None, 0) == -2
+    assert qlib.QTrkB200ServerSubmitFrame(None, 0, None, 0, 0, 0, None, 0, 0, None) == -1
+    assert qlib.QTrkB200ServerAttach(None, None) == -1
