@@ -204,6 +204,10 @@ QTRK_API void QTRK_CALLCONV ComputeRadialProfile(float *dst, int radialSteps, in
                                                  bool normalize);                                            /* utils.h:182 */
 QTRK_API void QTRK_CALLCONV NormalizeRadialProfile(float *prof, int rsteps);                                  /* utils.h:183 */
 QTRK_API void QTRK_CALLCONV NormalizeImage(ImageData *image);                                                 /* utils.h:185 */
+/* utils.h:187-188 (C++ references there; a pointer is the same ABI). Noise from the C library's
+ * rand(): seed it with srand() for a repeatable image. */
+QTRK_API void QTRK_CALLCONV ApplyPoissonNoise(ImageData *img, float poissonMax, float maxValue);
+QTRK_API void QTRK_CALLCONV ApplyGaussianNoise(ImageData *img, float sigma);
 QTRK_API void QTRK_CALLCONV GenerateImageFromLUT(ImageData *image, ImageData *zlut, float minradius, float maxradius,
                                                  vector3f pos, bool useSplineInterp, int ovs);                /* utils.h:186 */
 QTRK_API void QTRK_CALLCONV GenerateGaussianSpotImage(ImageData *img, vector2f pos, float sigma, float I0, float Ibg); /* utils.h:216 */

@@ -171,6 +171,8 @@ PROTOTYPES = {
                                     C.c_float, C.c_bool]),
     "NormalizeRadialProfile": (None, [_P, C.c_int]),
     "NormalizeImage": (None, [C.POINTER(ImageData)]),
+    "ApplyPoissonNoise": (None, [C.POINTER(ImageData), C.c_float, C.c_float]),
+    "ApplyGaussianNoise": (None, [C.POINTER(ImageData), C.c_float]),
     "GenerateImageFromLUT": (None, [C.POINTER(ImageData), C.POINTER(ImageData), C.c_float, C.c_float, vector3f,
                                     C.c_bool, C.c_int]),
     "GenerateGaussianSpotImage": (None, [C.POINTER(ImageData), vector2f, C.c_float, C.c_float, C.c_float]),

@@ -386,6 +386,57 @@ QTRK_API void QTRK_CALLCONV NormalizeImage(ImageData *img)
     for (int k = 0; k < n; k++) img->data[k] = (img->data[k] - mn) / (mx - mn);
 }
 
+// Noise utilities (cputrack/utils.cpp:404-433 with the samplers of cputrack/random_distr.h):
+// both draw from the C library's rand(), so a caller that seeds it with srand() gets the same
+// image from the reference and from this library. The samplers are the textbook ones:
+// Box-Muller for a standard normal (U0 offset by 1e-9 so that log(U0) is finite), and for the
+// Poisson variate Knuth's product-of-uniforms method (capped at 200 factors) up to lambda 10 and
+// floor(0.5 + lambda + sqrt(lambda) N(0,1)) clamped at 0 above it. Single precision throughout.
+static float uniform_f() { return rand() / (float)RAND_MAX; }
+
+static float normal_f()
+{
+    const float u0 = uniform_f() + 1e-9f;
+    const float u1 = uniform_f();
+    // the transcendental steps run in double and the product is rounded once, as the
+    // reference's unqualified log/sqrt/cos calls resolve to the double functions
+    return (float)(std::sqrt(-2 * std::log((double)u0)) * std::cos((double)(2 * 3.141593f * u1)));
+}
+
+static int poisson_f(float lambda)
+{
+    if (lambda > 10) {
+        const float v = (float)(0.5f + lambda + normal_f() * std::sqrt((double)lambda));
+        return (int)std::max(0.0f, v);
+    }
+    const float limit = (float)std::exp((double)-lambda);
+    float prod = 1;
+    int k = 0;
+    do {
+        k++;
+        prod *= uniform_f();
+    } while (prod > limit && k < 200);
+    return k - 1;
+}
+
+QTRK_API void QTRK_CALLCONV ApplyPoissonNoise(ImageData *img, float poissonMax, float maxValue)
+{
+    if (!img || !img->data) return;
+    const float ratio = maxValue / poissonMax;
+    const int n = img->w * img->h;
+    for (int k = 0; k < n; k++) img->data[k] = (float)(int)(poisson_f(poissonMax * img->data[k]) * ratio);
+}
+
+QTRK_API void QTRK_CALLCONV ApplyGaussianNoise(ImageData *img, float sigma)
+{
+    if (!img || !img->data) return;
+    const int n = img->w * img->h;
+    for (int k = 0; k < n; k++) {
+        const float v = img->data[k] + sigma * normal_f();
+        img->data[k] = v < 0.0f ? 0.0f : v;
+    }
+}
+
 // Abramowitz & Stegun 7.1.26, the erf the reference's utilities bind (cputrack/utils.h:395-417).
 static float erf_as_host(float x)
 {

@@ -113,6 +113,29 @@ def test_image_generators_match_reference(qlib, ref):
             np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-5)
 
 
+def test_noise_utilities_match_reference(qlib, ref):
+    """ApplyPoissonNoise / ApplyGaussianNoise draw from libc rand(): same srand seed, same image."""
+    libc = C.CDLL(None)
+    base = np.abs(np.sin(np.arange(64 * 48, dtype=np.float32) * 0.37)).reshape(48, 64).astype(np.float32)
+    base[0, :8] = [0, 0.001, 0.01, 0.05, 0.2, 0.6, 0.9, 1.0]
+    for fn, args in (("ApplyPoissonNoise", (40.0, 255.0)), ("ApplyPoissonNoise", (3000.0, 3000.0)),
+                     ("ApplyGaussianNoise", (0.25,))):
+        a, b = base.copy(), base.copy()
+        libc.srand(1234)
+        getattr(qlib, fn)(C.byref(_img(a)), *args)
+        libc.srand(1234)
+        getattr(ref.lib, fn)(C.byref(_img(b)), *args)
+        assert np.array_equal(a, b), fn
+        assert not np.array_equal(a, base)
+    # the Poisson sampler's moments (both branches): mean and variance of lambda
+    for lam in (2.5, 400.0):
+        img = np.full((200, 250), lam / 1000.0, np.float32)
+        libc.srand(7)
+        qlib.ApplyPoissonNoise(C.byref(_img(img)), 1000.0, 1000.0)
+        assert abs(img.mean() - lam) < 0.03 * lam + 0.05
+        assert abs(img.var() - lam) < 0.08 * lam + 0.1
+
+
 def _gpu_present() -> bool:
     try:
         import torch
