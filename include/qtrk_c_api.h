@@ -131,6 +131,27 @@ typedef struct QTrkComputedConfig {
 
 /* 8 bytes; cputrack/qtrk_c_api.h:116-119 */
 typedef struct ROIPosition { int x, y; } ROIPosition;
+
+/* 41 bytes; cputrack/qtrk_c_api.h:211-219. Output position = (pos - ROI centre + offset) * scaling. */
+typedef struct ResultManagerConfig {
+    int numBeads, numFrameInfoColumns;
+    vector3f scaling;
+    vector3f offset;
+    int writeInterval;          /* frames between file writes */
+    uint32_t maxFramesInMemory; /* 0: unlimited */
+    uint8_t binaryOutput;
+} ResultManagerConfig;
+
+/* 28 bytes; cputrack/qtrk_c_api.h:220-229 */
+typedef struct RMFrameCounters {
+    int startFrame;        /* first frame still held in memory */
+    int processedFrames;   /* frames whose results are complete (or given up as lost) */
+    int lastSaveFrame;
+    int capturedFrames;    /* frames with frame info stored */
+    int localizationsDone;
+    int lostFrames;
+    int fileError;
+} RMFrameCounters;
 #pragma pack(pop)
 
 #define QTrkCUDA_UseList -3
@@ -269,6 +290,33 @@ QTRK_API int QTRK_CALLCONV QTrkB200LocalizeDeviceNoAlloc(struct QueuedTracker *q
                                                          int64_t roi_stride_bytes, QTRK_PixelDataType_t pdt,
                                                          int count, const LocalizationJob *d_jobs,
                                                          LocalizationResult *d_results, void *stream);
+
+/* ---- ResultManager (cputrack/qtrk_c_api.cpp:181-241, cputrack/ResultManager.cpp) ----
+ * Bins the results of one tracker per frame and bead (bead = zlutIndex), writes completed frames
+ * to a text or binary file every writeInterval frames, keeps at most maxFramesInMemory frames.
+ * A background thread fetches the attached tracker's results. */
+struct ResultManager;
+#ifndef __cplusplus
+typedef struct ResultManager ResultManager;
+#endif
+QTRK_API struct ResultManager *QTRK_CALLCONV RMCreate(const char *file, const char *frameinfo,
+                                                      ResultManagerConfig *cfg, const char *semicolonSeparatedNames);
+QTRK_API void QTRK_CALLCONV RMSetTracker(struct ResultManager *rm, struct QueuedTracker *qtrk);
+QTRK_API void QTRK_CALLCONV RMDestroy(struct ResultManager *rm);
+QTRK_API void QTRK_CALLCONV RMStoreFrameInfo(struct ResultManager *rm, int frame, double timestamp, float *cols);
+QTRK_API int QTRK_CALLCONV RMGetBeadResults(struct ResultManager *rm, int start, int numFrames, int bead,
+                                            LocalizationResult *results);
+QTRK_API void QTRK_CALLCONV RMGetFrameCounters(struct ResultManager *rm, RMFrameCounters *dst);
+QTRK_API void QTRK_CALLCONV RMFlush(struct ResultManager *rm);
+QTRK_API int QTRK_CALLCONV RMGetResults(struct ResultManager *rm, int startFrame, int numFrames,
+                                        LocalizationResult *results);
+QTRK_API void QTRK_CALLCONV RMRemoveBead(struct ResultManager *rm, int bead);
+QTRK_API void QTRK_CALLCONV RMGetConfig(struct ResultManager *rm, ResultManagerConfig *cfg);
+/* Extension: store results that did not come from the attached tracker's queue (for example the
+ * request server's per-frame results); roi_width/roi_height give the ROI centre that is
+ * subtracted. No counterpart in the reference. */
+QTRK_API void QTRK_CALLCONV QTrkB200RMStoreResults(struct ResultManager *rm, const LocalizationResult *results,
+                                                   int count, int roi_width, int roi_height);
 
 /*
  * Request server: real-time localization of frames from several instances on one GPU. No

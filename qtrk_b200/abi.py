@@ -109,6 +109,23 @@ class ROIPosition(C.Structure):
     _fields_ = [("x", C.c_int), ("y", C.c_int)]
 
 
+class ResultManagerConfig(C.Structure):
+    """41 bytes, cputrack/qtrk_c_api.h:211-219."""
+
+    _pack_ = 1
+    _fields_ = [("numBeads", C.c_int), ("numFrameInfoColumns", C.c_int), ("scaling", vector3f),
+                ("offset", vector3f), ("writeInterval", C.c_int), ("maxFramesInMemory", C.c_uint32),
+                ("binaryOutput", C.c_uint8)]
+
+
+class RMFrameCounters(C.Structure):
+    """28 bytes, cputrack/qtrk_c_api.h:220-229."""
+
+    _pack_ = 1
+    _fields_ = [(n, C.c_int) for n in ("startFrame", "processedFrames", "lastSaveFrame", "capturedFrames",
+                                       "localizationsDone", "lostFrames", "fileError")]
+
+
 class QTrkB200ServeStats(C.Structure):
     """Request-server statistics (library extension; 80 bytes)."""
 
@@ -120,6 +137,8 @@ class QTrkB200ServeStats(C.Structure):
 
 
 assert C.sizeof(QTrkB200ServeStats) == 80
+assert C.sizeof(ResultManagerConfig) == 41
+assert C.sizeof(RMFrameCounters) == 28
 assert C.sizeof(LocalizationJob) == 24
 assert C.sizeof(LocalizationResult) == 52
 assert C.sizeof(QTrkSettings) == 84
@@ -173,6 +192,16 @@ PROTOTYPES = {
     "NormalizeImage": (None, [C.POINTER(ImageData)]),
     "ApplyPoissonNoise": (None, [C.POINTER(ImageData), C.c_float, C.c_float]),
     "ApplyGaussianNoise": (None, [C.POINTER(ImageData), C.c_float]),
+    "RMCreate": (_P, [C.c_char_p, C.c_char_p, C.POINTER(ResultManagerConfig), C.c_char_p]),
+    "RMSetTracker": (None, [_P, _TRK]),
+    "RMDestroy": (None, [_P]),
+    "RMStoreFrameInfo": (None, [_P, C.c_int, C.c_double, _P]),
+    "RMGetBeadResults": (C.c_int, [_P, C.c_int, C.c_int, C.c_int, _P]),
+    "RMGetFrameCounters": (None, [_P, C.POINTER(RMFrameCounters)]),
+    "RMFlush": (None, [_P]),
+    "RMGetResults": (C.c_int, [_P, C.c_int, C.c_int, _P]),
+    "RMRemoveBead": (None, [_P, C.c_int]),
+    "RMGetConfig": (None, [_P, C.POINTER(ResultManagerConfig)]),
     "GenerateImageFromLUT": (None, [C.POINTER(ImageData), C.POINTER(ImageData), C.c_float, C.c_float, vector3f,
                                     C.c_bool, C.c_int]),
     "GenerateGaussianSpotImage": (None, [C.POINTER(ImageData), vector2f, C.c_float, C.c_float, C.c_float]),
@@ -185,6 +214,7 @@ B200_PROTOTYPES = {
     "QTrkB200SetZLUTBiasTable": (None, [_TRK, _P, C.c_int, C.c_int]),
     "QTrkB200LocalizeDevice": (C.c_int, [_TRK, _P, C.c_int, C.c_int64, C.c_int, C.c_int, _P, _P, _P]),
     "QTrkB200LocalizeDeviceNoAlloc": (C.c_int, [_TRK, _P, C.c_int, C.c_int64, C.c_int, C.c_int, _P, _P, _P]),
+    "QTrkB200RMStoreResults": (None, [_P, _P, C.c_int, C.c_int, C.c_int]),
     "QTrkB200ServerCreate": (_P, [C.c_int, C.c_int64]),
     "QTrkB200ServerDestroy": (None, [_P]),
     "QTrkB200ServerAttach": (C.c_int, [_P, _TRK]),

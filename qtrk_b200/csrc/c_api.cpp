@@ -15,6 +15,7 @@
 
 #include "kernels.h"
 #include "qtrk_c_api.h"
+#include "result_manager.h"
 #include "serve.h"
 #include "tracker.h"
 
@@ -628,4 +629,83 @@ QTRK_API void QTRK_CALLCONV QTrkB200ServerHold(void *server, int hold)
 QTRK_API void QTRK_CALLCONV QTrkB200ServerResetStats(void *server)
 {
     if (server) static_cast<qtrk::Server *>(server)->ResetStats();
+}
+
+// ---------------------------------------------------------------------------------------
+// ResultManager (cputrack/qtrk_c_api.cpp:181-241)
+// ---------------------------------------------------------------------------------------
+QTRK_API ResultManager *QTRK_CALLCONV RMCreate(const char *file, const char *frameinfo, ResultManagerConfig *cfg,
+                                               const char *semicolonSeparatedNames)
+{
+    if (!cfg) {
+        set_last_error("RMCreate: null config");
+        return nullptr;
+    }
+    // Column names split at ';' as qtrk_c_api.cpp:185-195 does: the separator is kept as the
+    // first character of the following name.
+    std::vector<std::string> names;
+    std::string name;
+    for (const char *c = semicolonSeparatedNames ? semicolonSeparatedNames : ""; *c; c++) {
+        if (*c == ';') {
+            names.push_back(name);
+            name.clear();
+        }
+        name += *c;
+    }
+    if (!name.empty()) names.push_back(name);
+    try {
+        return new ResultManager(file, frameinfo, *cfg, names);
+    } catch (const std::exception &e) {
+        set_last_error(std::string("RMCreate: ") + e.what());
+        return nullptr;
+    }
+}
+
+QTRK_API void QTRK_CALLCONV RMSetTracker(ResultManager *rm, QueuedTracker *q)
+{
+    if (rm) rm->SetTracker(q ? T(q) : nullptr);
+}
+
+QTRK_API void QTRK_CALLCONV RMDestroy(ResultManager *rm) { delete rm; }
+
+QTRK_API void QTRK_CALLCONV RMStoreFrameInfo(ResultManager *rm, int frame, double timestamp, float *cols)
+{
+    if (rm) rm->StoreFrameInfo(frame, timestamp, cols);
+}
+
+QTRK_API int QTRK_CALLCONV RMGetBeadResults(ResultManager *rm, int start, int numFrames, int bead,
+                                            LocalizationResult *results)
+{
+    return rm && results ? rm->GetBeadPositions(start, start + numFrames, bead, results) : 0;
+}
+
+QTRK_API void QTRK_CALLCONV RMGetFrameCounters(ResultManager *rm, RMFrameCounters *dst)
+{
+    if (rm && dst) *dst = rm->Counters();
+}
+
+QTRK_API void QTRK_CALLCONV RMFlush(ResultManager *rm)
+{
+    if (rm) rm->Flush();
+}
+
+QTRK_API int QTRK_CALLCONV RMGetResults(ResultManager *rm, int startFrame, int numFrames, LocalizationResult *results)
+{
+    return rm && results ? rm->GetResults(results, startFrame, numFrames) : 0;
+}
+
+QTRK_API void QTRK_CALLCONV RMRemoveBead(ResultManager *rm, int bead)
+{
+    if (rm) rm->RemoveBead(bead);
+}
+
+QTRK_API void QTRK_CALLCONV RMGetConfig(ResultManager *rm, ResultManagerConfig *cfg)
+{
+    if (rm && cfg) *cfg = rm->Config();
+}
+
+QTRK_API void QTRK_CALLCONV QTrkB200RMStoreResults(ResultManager *rm, const LocalizationResult *results, int count,
+                                                   int roi_width, int roi_height)
+{
+    if (rm && results && count > 0) rm->StoreResults(results, count, roi_width, roi_height);
 }
