@@ -291,6 +291,17 @@ QTRK_API int QTRK_CALLCONV QTrkB200LocalizeDeviceNoAlloc(struct QueuedTracker *q
                                                          int count, const LocalizationJob *d_jobs,
                                                          LocalizationResult *d_results, void *stream);
 
+/* ---- bead finder (cputrack/qtrk_c_api.h:203-205; qtrk_c_api.cpp:28-58; BeadFinder.cpp) ----
+ * Template match of the sample ROI at (smpCornerPosX, smpCornerPosY) over the image; returns
+ * the ROI corners of the beads found (*beadcount of them), to be freed with
+ * QTrkFreeROIPositions; `sample` (if roi x roi) receives the sample. The convolution runs on the
+ * current CUDA device. Returns NULL (and *beadcount = 0) on invalid arguments; unlike the
+ * reference, a sample ROI that is not inside the image is an error. */
+QTRK_API void QTRK_CALLCONV QTrkFreeROIPositions(ROIPosition *data);
+QTRK_API ROIPosition *QTRK_CALLCONV QTrkFindBeads(ImageData *imgData, int smpCornerPosX, int smpCornerPosY, int roi,
+                                                  float imgRelDist, float acceptance, int *beadcount,
+                                                  ImageData *sample);
+
 /* ---- ResultManager (cputrack/qtrk_c_api.cpp:181-241, cputrack/ResultManager.cpp) ----
  * Bins the results of one tracker per frame and bead (bead = zlutIndex), writes completed frames
  * to a text or binary file every writeInterval frames, keeps at most maxFramesInMemory frames.

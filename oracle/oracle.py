@@ -218,6 +218,8 @@ class PortOracle:
             "oracle_joint_refine": (None, [_f64p, C.c_int, C.c_int, C.c_double, _f64p, _f32p, C.c_int, C.c_int,
                                            C.c_int, C.c_double, C.c_double, P, C.c_int]),
             "oracle_zlut_bias_correct": (C.c_double, [C.c_double, C.c_int, _f32p, C.c_int, C.c_int, C.c_int]),
+            "oracle_find_beads": (C.c_int, [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                            C.c_float, P, C.c_int, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -344,6 +346,19 @@ class PortOracle:
         self.lib.oracle_joint_refine(img, img.shape[1], img.shape[0], mean, io, lut, lut.shape[0], lut.shape[1],
                                      angsteps, minr, maxr, _ptr(w), steps)
         return io
+
+    def find_beads(self, img, sample_corner, roi, rel_dist, similarity, return_conv=False):
+        """QTrkFindBeads restated (FP64 convolution); returns (n, 2) int ROI corners [, conv map]."""
+        img = np.ascontiguousarray(img, np.float32)
+        h, w = img.shape
+        out = np.zeros((4096, 2), np.int32)
+        w2, h2 = 1 << max(0, (w - 1).bit_length()), 1 << max(0, (h - 1).bit_length())
+        conv = np.zeros((h2, w2)) if return_conv else None
+        n = self.lib.oracle_find_beads(img, w, h, int(sample_corner[0]), int(sample_corner[1]), roi, rel_dist,
+                                       similarity, out.ctypes.data, len(out),
+                                       conv.ctypes.data if conv is not None else None)
+        pos = out[:min(n, len(out))].copy()
+        return (pos, conv) if return_conv else pos
 
 
 def cpu_count() -> int:

@@ -716,3 +716,138 @@ ORACLE_API void oracle_joint_refine(const double *img, int w, int h, double mean
         if (io[2] > planes - 1) io[2] = planes - 1;
     }
 }
+
+/*
+ * Bead finder, BeadFinder.cpp:170-222 (Find) with SearchArea (:79-105) and RecenterAndFilter
+ * (:108-166), as QTrkFindBeads (qtrk_c_api.cpp:33-58) calls it. The FFT convolution of the
+ * reference (image minus its mean, zero-padded to powers of two, times the FFT of the
+ * mean-free sample placed at offset -roi, inverse FFT) is the circular convolution
+ *   conv(py,px) = sum_{a,b<roi} t(a,b) c((py+roi-a) mod H2, (px+roi-b) mod W2),
+ * evaluated here directly in double (the inverse FFT's missing 1/(W2 H2) does not change any
+ * decision: every test on the map is relative to its maximum). Means, the recentering sums
+ * and the distance tests follow the reference's float arithmetic and int truncations.
+ * Returns the number of positions (at most max_out written to out_xy as x,y pairs);
+ * conv_out (W2*H2 doubles, may be NULL) receives the map before the search zeroes it.
+ */
+static int bf_next_pow2(int x)
+{
+    int y = 1;
+    while (y < x) y *= 2;
+    return y;
+}
+
+ORACLE_API int oracle_find_beads(const float *img, int w, int h, int sx, int sy, int roi, float rel_dist,
+                                 float similarity, int *out_xy, int max_out, double *conv_out)
+{
+    int W2 = bf_next_pow2(w), H2 = bf_next_pow2(h);
+    float mean = 0.0f, smean = 0.0f;
+    for (int i = 0; i < w * h; i++) mean += img[i];
+    mean /= (float)(w * h);
+    float *t = (float *)malloc(sizeof(float) * roi * roi);
+    for (int y = 0; y < roi; y++)
+        for (int x = 0; x < roi; x++) t[y * roi + x] = img[(sy + y) * w + sx + x];
+    for (int i = 0; i < roi * roi; i++) smean += t[i];
+    smean /= (float)(roi * roi);
+    for (int i = 0; i < roi * roi; i++) t[i] = t[i] - smean;
+    double *conv = (double *)malloc(sizeof(double) * W2 * H2);
+    for (int py = 0; py < H2; py++)
+        for (int px = 0; px < W2; px++) {
+            double acc = 0;
+            for (int a = 0; a < roi; a++) {
+                int yy = (py + roi - a) & (H2 - 1);
+                if (yy >= h) continue;
+                for (int b = 0; b < roi; b++) {
+                    int xx = (px + roi - b) & (W2 - 1);
+                    if (xx >= w) continue;
+                    acc += (double)t[a * roi + b] * (double)(img[yy * w + xx] - mean);
+                }
+            }
+            conv[py * W2 + px] = acc;
+        }
+    if (conv_out) memcpy(conv_out, conv, sizeof(double) * W2 * H2);
+    double maxv = 0;
+    for (int i = 0; i < W2 * H2; i++)
+        if (conv[i] > maxv) maxv = conv[i];
+    const float mdist = 0.5f * rel_dist * roi;
+    const int dist = (int)mdist;
+    int npts = 0, cap = 64;
+    int *pts = (int *)malloc(sizeof(int) * 2 * cap);
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) {
+            if (!(conv[y * W2 + x] > maxv * similarity)) continue;
+            /* SearchArea: the maximum inside the disc of radius dist (clipped to the padded map);
+               every visited value is zeroed */
+            int bx = x, by = y;
+            double best = conv[y * W2 + x];
+            int y0 = y - dist < 0 ? 0 : y - dist, x0 = x - dist < 0 ? 0 : x - dist;
+            int x1 = x + dist > W2 - 1 ? W2 - 1 : x + dist, y1 = y + dist > H2 - 1 ? H2 - 1 : y + dist;
+            for (int yy = y0; yy <= y1; yy++)
+                for (int xx = x0; xx <= x1; xx++) {
+                    int dx = xx - x, dy = yy - y;
+                    if (dx * dx + dy * dy > dist * dist) continue;
+                    if (conv[yy * W2 + xx] > best) {
+                        best = conv[yy * W2 + xx];
+                        bx = xx;
+                        by = yy;
+                    }
+                    conv[yy * W2 + xx] = 0;
+                }
+            if (npts == cap) {
+                cap *= 2;
+                pts = (int *)realloc(pts, sizeof(int) * 2 * cap);
+            }
+            pts[2 * npts] = bx;
+            pts[2 * npts + 1] = by;
+            npts++;
+        }
+    /* RecenterAndFilter: COM of the squared deviation from the ROI mean (float sums), shift by
+       it minus roi/2 (int truncation), bounds checks, and both of two positions closer than
+       mdist are dropped (the earlier one from the list, the later one never added). */
+    int *acc_xy = (int *)malloc(sizeof(int) * 2 * (npts + 1));
+    int nacc = 0;
+    for (int i = 0; i < npts; i++) {
+        int px = pts[2 * i], py = pts[2 * i + 1];
+        if (px < 0 || py < 0 || px > w - 1 - roi || py > h - 1 - roi) continue;
+        float sum = 0.0f;
+        for (int y = 0; y < roi; y++)
+            for (int x = 0; x < roi; x++) sum += img[(y + py) * w + x + px];
+        float m = sum / (roi * roi), sumx = 0, sumy = 0;
+        sum = 0;
+        for (int y = 0; y < roi; y++)
+            for (int x = 0; x < roi; x++) {
+                float v = img[(y + py) * w + x + px] - m;
+                v = v * v;
+                sum += v;
+                sumx += v * x;
+                sumy += v * y;
+            }
+        if (sum == 0.0f) continue;
+        px = (int)((float)px + (sumx / sum - roi / 2));
+        py = (int)((float)py + (sumy / sum - roi / 2));
+        if (px < 0 || py < 0 || px > w - 1 - roi || py > h - 1 - roi) continue;
+        int accepted = 1;
+        for (int c = 0; c < nacc; c++) {
+            int dx = acc_xy[2 * c] - px, dy = acc_xy[2 * c + 1] - py;
+            if ((float)(dx * dx + dy * dy) < mdist * mdist) {
+                memmove(&acc_xy[2 * c], &acc_xy[2 * c + 2], sizeof(int) * 2 * (nacc - c - 1));
+                nacc--;
+                accepted = 0;
+                break;
+            }
+        }
+        if (accepted) {
+            acc_xy[2 * nacc] = px;
+            acc_xy[2 * nacc + 1] = py;
+            nacc++;
+        }
+    }
+    for (int i = 0; i < nacc && i < max_out; i++) {
+        out_xy[2 * i] = acc_xy[2 * i];
+        out_xy[2 * i + 1] = acc_xy[2 * i + 1];
+    }
+    free(acc_xy);
+    free(pts);
+    free(conv);
+    free(t);
+    return nacc;
+}

@@ -192,6 +192,9 @@ PROTOTYPES = {
     "NormalizeImage": (None, [C.POINTER(ImageData)]),
     "ApplyPoissonNoise": (None, [C.POINTER(ImageData), C.c_float, C.c_float]),
     "ApplyGaussianNoise": (None, [C.POINTER(ImageData), C.c_float]),
+    "QTrkFindBeads": (_P, [C.POINTER(ImageData), C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                           C.POINTER(C.c_int), C.POINTER(ImageData)]),
+    "QTrkFreeROIPositions": (None, [_P]),
     "RMCreate": (_P, [C.c_char_p, C.c_char_p, C.POINTER(ResultManagerConfig), C.c_char_p]),
     "RMSetTracker": (None, [_P, _TRK]),
     "RMDestroy": (None, [_P]),

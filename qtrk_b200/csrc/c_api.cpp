@@ -79,6 +79,11 @@ void copy_string(const std::string &s, char *dst, int maxlen)
 
 }  // namespace
 
+namespace qtrk {
+// For entry points defined in other translation units (the bead finder).
+void set_last_error_msg(const std::string &m) { set_last_error(m); }
+}  // namespace qtrk
+
 extern "C" {
 
 QTRK_API void QTRK_CALLCONV TestDLLCallConv(int) {}

@@ -221,3 +221,26 @@ def serving_fleet(n_frames: int = 2, seed: int = 5, cameras=SERVING_CAMERAS) -> 
         fleet.append(ServedCamera(f"{w}x{w}-{np.dtype(dt).name}-{beads}beads", settings_square(w), MODE_QI_Z,
                                   frames, positions, stack[:, None], np.array([[w / 2, w / 2]], np.float32)))
     return fleet
+
+
+def bead_frame(w: int = 320, h: int = 256, n_beads: int = 12, roi: int = 32, seed: int = 6, noise: float = 2.0):
+    """A frame for the bead finder: n_beads bead images (10 + 100 p(r; z), z ~ U[5, 15]) at random
+    non-overlapping positions at least one ROI from each other and inside the frame, plus
+    Gaussian noise (sigma `noise`). Returns (frame f32, centres (n, 2) float64)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    centres = []
+    tries = 0
+    while len(centres) < n_beads and tries < 10000:
+        tries += 1
+        c = rng.uniform([roi, roi], [w - roi, h - roi])
+        if all(np.hypot(*(c - o)) > 1.5 * roi for o in centres):
+            centres.append(c)
+    centres = np.array(centres)
+    ys = np.arange(h, dtype=np.float64)[:, None]
+    xs = np.arange(w, dtype=np.float64)[None, :]
+    frame = np.full((h, w), 10.0)
+    for (cx, cy), z in zip(centres, rng.uniform(5, 15, len(centres))):
+        r = np.sqrt((xs - cx) ** 2 + (ys - cy) ** 2)
+        frame += 100.0 * profile(r, z) * (r < roi)
+    frame = np.maximum(frame + rng.normal(0, noise, frame.shape), 0)
+    return frame.astype(np.float32), centres

@@ -164,3 +164,8 @@ def test_create_without_gpu_fails_cleanly(qlib):
     assert qlib.QTrkB200ServerPoll(None, 1, None, 0) == -2
     assert qlib.QTrkB200ServerSubmitFrame(None, 0, None, 0, 0, 0, None, 0, 0, None) == -1
     assert qlib.QTrkB200ServerAttach(None, None) == -1
+    # so does the bead finder's convolution: NULL, no beads, an error message
+    frame = np.ones((64, 64), np.float32)
+    n = C.c_int(5)
+    assert not qlib.QTrkFindBeads(C.byref(_img(frame)), 0, 0, 16, 1.0, 0.5, C.byref(n), None)
+    assert n.value == 0 and "QTrkFindBeads" in tracker.last_error()

@@ -79,3 +79,55 @@ def test_gaussian_5p_matches_fp64_oracle_and_crlb(port):
     err = np.stack([r["pos"][:, 0] - wl.true_xyz[:, 0], r["pos"][:, 1] - wl.true_xyz[:, 1]], 1)
     ratio = (err / np.array(crlb)).std(0)
     assert (ratio > 0.8).all() and (ratio < 1.25).all(), ratio
+
+
+@pytest.mark.parametrize("roi,seed,noise", [(32, 6, 2.0), (24, 7, 4.0), (40, 8, 1.0)])
+def test_find_beads_matches_reference(ref, port, roi, seed, noise):
+    """QTrkFindBeads (GPU convolution + host search) gives the reference's bead list."""
+    import ctypes as C
+
+    from qtrk_b200.tracker import load_library
+
+    lib = load_library()
+    frame, centres = synth.bead_frame(300, 220, 10, roi, seed=seed, noise=noise)
+    corner = (int(centres[0][0] - roi / 2), int(centres[0][1] - roi / 2))
+    img = abi.ImageData(frame.ctypes.data_as(C.POINTER(C.c_float)), frame.shape[1], frame.shape[0])
+    for rel, acc in ((1.0, 0.3), (1.0, 0.6), (0.8, 0.45)):
+        outs = []
+        for L in (lib, ref.lib):
+            n = C.c_int()
+            smp = np.zeros((roi, roi), np.float32)
+            smp_img = abi.ImageData(smp.ctypes.data_as(C.POINTER(C.c_float)), roi, roi)
+            p = L.QTrkFindBeads(C.byref(img), corner[0], corner[1], roi, rel, acc, C.byref(n), C.byref(smp_img))
+            assert p
+            outs.append(np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_int)), shape=(2 * n.value,)).reshape(-1, 2).copy())
+            L.QTrkFreeROIPositions(p)
+            assert np.array_equal(smp, frame[corner[1]:corner[1] + roi, corner[0]:corner[0] + roi])
+        assert np.array_equal(outs[0], outs[1]), (rel, acc)
+        assert np.array_equal(outs[0], port.find_beads(frame, corner, roi, rel, acc))
+
+
+def test_find_beads_large_frame():
+    """A 2048 x 2048 frame with a 100 px sample: every planted bead found, within a ROI's reach."""
+    import ctypes as C
+    import time
+
+    from qtrk_b200.tracker import load_library
+
+    lib = load_library()
+    roi = 100
+    frame, centres = synth.bead_frame(2048, 2048, 120, roi, seed=9, noise=2.0)
+    corner = (int(centres[0][0] - roi / 2), int(centres[0][1] - roi / 2))
+    img = abi.ImageData(frame.ctypes.data_as(C.POINTER(C.c_float)), 2048, 2048)
+    n = C.c_int()
+    t0 = time.perf_counter()
+    p = lib.QTrkFindBeads(C.byref(img), corner[0], corner[1], roi, 1.0, 0.5, C.byref(n), None)
+    dt = time.perf_counter() - t0
+    assert p
+    pos = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_int)), shape=(2 * n.value,)).reshape(-1, 2).copy()
+    lib.QTrkFreeROIPositions(p)
+    found = pos + roi / 2
+    inside = (centres[:, 0] > roi) & (centres[:, 1] > roi) & (centres[:, 0] < 2048 - roi) & (centres[:, 1] < 2048 - roi)
+    d = np.hypot(centres[inside, None, 0] - found[None, :, 0], centres[inside, None, 1] - found[None, :, 1]).min(1)
+    assert (d < 3).all(), d.max()
+    print(f"FindBeads 2048x2048, roi {roi}: {n.value} beads in {dt * 1e3:.1f} ms")

@@ -4,6 +4,8 @@ The reference itself runs here from oracle/_ref/libqtrk_ref.so (compiled from it
 cputrack/ sources); where that library is absent, the committed fixtures in tests/golden/
 (outputs of the same reference build) pin the port instead.
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -192,3 +194,25 @@ def test_port_reproduces_golden_buildlut(port):
     cc = port.computed_config(g["settings"])
     lut = port.build_lut(cc, g["stack"], abi.BUILDLUT_NORMALIZE)
     assert np.abs(lut - g["lut"]).max() < 2e-3
+
+
+def _ref_find_beads(ref, frame, corner, roi, rel, acc):
+    img = abi.ImageData(frame.ctypes.data_as(C.POINTER(C.c_float)), frame.shape[1], frame.shape[0])
+    n = C.c_int()
+    p = ref.lib.QTrkFindBeads(C.byref(img), int(corner[0]), int(corner[1]), roi, rel, acc, C.byref(n), None)
+    out = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_int)), shape=(2 * n.value,)).reshape(-1, 2).copy() \
+        if n.value else np.zeros((0, 2), np.int32)
+    ref.lib.QTrkFreeROIPositions(p)
+    return out
+
+
+@pytest.mark.parametrize("roi,seed,noise", [(32, 6, 2.0), (24, 7, 4.0), (40, 8, 1.0)])
+def test_bead_finder_oracle_matches_reference(ref, port, roi, seed, noise):
+    """oracle_find_beads (direct FP64 convolution) gives the reference's bead list (KISS FFT)."""
+    frame, centres = synth.bead_frame(300, 220, 10, roi, seed=seed, noise=noise)
+    corner = (int(centres[0][0] - roi / 2), int(centres[0][1] - roi / 2))
+    for rel, acc in ((1.0, 0.3), (1.0, 0.6), (0.8, 0.45)):
+        a = _ref_find_beads(ref, frame, corner, roi, rel, acc)
+        b = port.find_beads(frame, corner, roi, rel, acc)
+        assert np.array_equal(a, b), (rel, acc)
+        assert len(a) >= 6
