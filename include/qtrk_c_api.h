@@ -252,6 +252,13 @@ QTRK_API int64_t QTRK_CALLCONV QTrkB200GetKernelLaunchCount(struct QueuedTracker
  */
 QTRK_API void QTRK_CALLCONV QTrkB200SetZLUTBiasTable(struct QueuedTracker *qtrk, const float *table, int bias_planes,
                                                      int count);
+/* QueuedTracker::ComputeZBiasCorrection (cputrack/QueuedTracker.cpp:143-189; the reference reaches
+ * it through qtrk_compute_zlut_bias_table, lv_queuetrk_api.cpp:457-466): render every bead's LUT at
+ * bias_planes evenly spaced z (smpPerPixel^2 samples per pixel, B-spline or linear over planes),
+ * localize each image (COM, 2 QI iterations, Z match), and set table[bead][plane] = z - true z as the
+ * instance's bias table. `result` (may be NULL) receives the count x bias_planes table. */
+QTRK_API void QTRK_CALLCONV QTrkB200ComputeZLUTBiasTable(struct QueuedTracker *qtrk, int bias_planes, float *result,
+                                                         int smpPerPixel, int useSplineInterp);
 
 /*
  * Localize `count` ROIs that are already resident in device memory, on the caller's CUDA
@@ -290,6 +297,14 @@ QTRK_API int QTRK_CALLCONV QTrkB200LocalizeDeviceNoAlloc(struct QueuedTracker *q
                                                          int64_t roi_stride_bytes, QTRK_PixelDataType_t pdt,
                                                          int count, const LocalizationJob *d_jobs,
                                                          LocalizationResult *d_results, void *stream);
+
+/* ---- .radialzlut files (the layout cputrack/utils.cpp:680-710 reads): int32 count, planes,
+ * radialsteps, then count*planes*radialsteps float32 in [bead][plane][bin] order. Read with
+ * dst = NULL to query the sizes. Return 0, or < 0 on error (QTrkB200GetLastError says why). */
+QTRK_API int QTRK_CALLCONV QTrkB200ReadRadialZLUTFile(const char *path, float *dst, int *count, int *planes,
+                                                      int *radialsteps);
+QTRK_API int QTRK_CALLCONV QTrkB200WriteRadialZLUTFile(const char *path, const float *data, int count, int planes,
+                                                       int radialsteps);
 
 /* ---- bead finder (cputrack/qtrk_c_api.h:203-205; qtrk_c_api.cpp:28-58; BeadFinder.cpp) ----
  * Template match of the sample ROI at (smpCornerPosX, smpCornerPosY) over the image; returns

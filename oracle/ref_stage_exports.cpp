@@ -117,3 +117,26 @@ REF_EXPORT void ref_stage_radial_bin_window(int rsteps, float *dst)
 REF_EXPORT float ref_stage_erf(float x) { return erf(x); }
 
 /* QueuedTracker::ScheduleFrame's zlutIndex/skip rule is reached through QTrkScheduleFrame. */
+
+/*
+ * QueuedTracker::ComputeZBiasCorrection (QueuedTracker.cpp:143-189) on a tracker created through
+ * the reference's C ABI; out = the count x bias_planes table (the reference also installs it as
+ * the tracker's bias table).
+ */
+REF_EXPORT void ref_compute_zbias(QueuedTracker *qtrk, int bias_planes, float *out, int smp_per_pixel, int spline)
+{
+    CImageData result;
+    qtrk->ComputeZBiasCorrection(bias_planes, &result, smp_per_pixel, spline != 0);
+    for (int i = 0; i < result.w * result.h; i++) out[i] = result.data[i];
+}
+
+/* ReadLUTFile (utils.cpp:680-710) of "path#bead": out (max_n floats) receives the normalised
+ * planes x radialsteps LUT; *w = radialsteps, *h = planes. */
+REF_EXPORT void ref_read_lut_file(const char *spec, float *out, int max_n, int *w, int *h)
+{
+    ImageData lut = ReadLUTFile(spec);
+    *w = lut.w;
+    *h = lut.h;
+    for (int i = 0; i < lut.w * lut.h && i < max_n; i++) out[i] = lut.data[i];
+    lut.free();
+}

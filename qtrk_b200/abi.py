@@ -215,9 +215,13 @@ B200_PROTOTYPES = {
     "QTrkB200GetLastError": (C.c_int, [C.c_char_p, C.c_int]),
     "QTrkB200GetKernelLaunchCount": (C.c_int64, [_TRK]),
     "QTrkB200SetZLUTBiasTable": (None, [_TRK, _P, C.c_int, C.c_int]),
+    "QTrkB200ComputeZLUTBiasTable": (None, [_TRK, C.c_int, _P, C.c_int, C.c_int]),
     "QTrkB200LocalizeDevice": (C.c_int, [_TRK, _P, C.c_int, C.c_int64, C.c_int, C.c_int, _P, _P, _P]),
     "QTrkB200LocalizeDeviceNoAlloc": (C.c_int, [_TRK, _P, C.c_int, C.c_int64, C.c_int, C.c_int, _P, _P, _P]),
     "QTrkB200RMStoreResults": (None, [_P, _P, C.c_int, C.c_int, C.c_int]),
+    "QTrkB200ReadRadialZLUTFile": (C.c_int, [C.c_char_p, _P, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                             C.POINTER(C.c_int)]),
+    "QTrkB200WriteRadialZLUTFile": (C.c_int, [C.c_char_p, _P, C.c_int, C.c_int, C.c_int]),
     "QTrkB200ServerCreate": (_P, [C.c_int, C.c_int64]),
     "QTrkB200ServerDestroy": (None, [_P]),
     "QTrkB200ServerAttach": (C.c_int, [_P, _TRK]),

@@ -4,6 +4,7 @@
 // QueuedTracker virtuals, but no C++ exception crosses the ABI: failures are reported
 // through QTrkGetWarnings (per instance) or QTrkB200GetLastError (no instance).
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -547,6 +548,13 @@ QTRK_API void QTRK_CALLCONV QTrkB200SetZLUTBiasTable(QueuedTracker *q, const flo
     guarded(q, "QTrkB200SetZLUTBiasTable", [&](Tracker *t) { t->SetZLUTBiasTable(table, bias_planes, count); });
 }
 
+QTRK_API void QTRK_CALLCONV QTrkB200ComputeZLUTBiasTable(QueuedTracker *q, int bias_planes, float *result,
+                                                         int smpPerPixel, int useSplineInterp)
+{
+    guarded(q, "QTrkB200ComputeZLUTBiasTable",
+            [&](Tracker *t) { t->ComputeZBiasTable(bias_planes, smpPerPixel, useSplineInterp != 0, result); });
+}
+
 QTRK_API int QTRK_CALLCONV QTrkB200LocalizeDevice(QueuedTracker *q, const void *d_pixels, int pitch,
                                                   int64_t roi_stride_bytes, QTRK_PixelDataType_t pdt, int count,
                                                   const LocalizationJob *d_jobs, LocalizationResult *d_results,
@@ -713,4 +721,55 @@ QTRK_API void QTRK_CALLCONV QTrkB200RMStoreResults(ResultManager *rm, const Loca
                                                    int roi_width, int roi_height)
 {
     if (rm && results && count > 0) rm->StoreResults(results, count, roi_width, roi_height);
+}
+
+// ---------------------------------------------------------------------------------------
+// .radialzlut files: int32 count, planes, radialsteps, then count*planes*radialsteps float32
+// ([bead][plane][bin]), the layout cputrack/utils.cpp:680-710 (ReadLUTFile) reads.
+// ---------------------------------------------------------------------------------------
+QTRK_API int QTRK_CALLCONV QTrkB200ReadRadialZLUTFile(const char *path, float *dst, int *count, int *planes,
+                                                      int *radialsteps)
+{
+    FILE *f = path ? std::fopen(path, "rb") : nullptr;
+    if (!f) {
+        set_last_error(std::string("QTrkB200ReadRadialZLUTFile: cannot open ") + (path ? path : "(null)"));
+        return -1;
+    }
+    int32_t hdr[3];
+    int rc = 0;
+    if (std::fread(hdr, 4, 3, f) != 3 || hdr[0] < 0 || hdr[1] < 0 || hdr[2] < 0) {
+        set_last_error("QTrkB200ReadRadialZLUTFile: bad header");
+        rc = -2;
+    } else {
+        if (count) *count = hdr[0];
+        if (planes) *planes = hdr[1];
+        if (radialsteps) *radialsteps = hdr[2];
+        const size_t n = (size_t)hdr[0] * hdr[1] * hdr[2];
+        if (dst && std::fread(dst, 4, n, f) != n) {
+            set_last_error("QTrkB200ReadRadialZLUTFile: file shorter than its header says");
+            rc = -3;
+        }
+    }
+    std::fclose(f);
+    return rc;
+}
+
+QTRK_API int QTRK_CALLCONV QTrkB200WriteRadialZLUTFile(const char *path, const float *data, int count, int planes,
+                                                       int radialsteps)
+{
+    if (!path || (!data && count * planes * radialsteps > 0) || count < 0 || planes < 0 || radialsteps < 0) {
+        set_last_error("QTrkB200WriteRadialZLUTFile: invalid argument");
+        return -1;
+    }
+    FILE *f = std::fopen(path, "wb");
+    if (!f) {
+        set_last_error(std::string("QTrkB200WriteRadialZLUTFile: cannot create ") + path);
+        return -1;
+    }
+    const int32_t hdr[3] = {count, planes, radialsteps};
+    const size_t n = (size_t)count * planes * radialsteps;
+    const bool ok = std::fwrite(hdr, 4, 3, f) == 3 && (n == 0 || std::fwrite(data, 4, n, f) == n);
+    std::fclose(f);
+    if (!ok) set_last_error("QTrkB200WriteRadialZLUTFile: write failed");
+    return ok ? 0 : -2;
 }

@@ -26,6 +26,13 @@ cudaError_t launch_localize(const TrackParams &P, const uint8_t *pixels, int pit
 // (P, pixels, pitch, roi_stride, roi_offsets, jobs, count, results). For explicitly built graphs.
 void localize_node(const TrackParams &P, int count, cudaKernelNodeParams &kp);
 
+// Bias-table images [first_image, first_image + n_images) of QueuedTracker::ComputeZBiasCorrection
+// (bead = image / bias_planes, z = (image % bias_planes) / bias_planes * planes) rendered from
+// the device LUT [beads][planes][nb] into images[n_images][h][w], with their jobs.
+cudaError_t launch_lut_images(const float *lut, int nb, int planes, int first_image, int n_images, int bias_planes,
+                              int w, int h, float minr, float maxr, int ovs, bool spline, float *images,
+                              LocalizationJob *jobs, cudaStream_t stream);
+
 // One BuildLUT plane: nbeads ROIs stacked at pitch*H; adds each profile to lut[bead][plane].
 cudaError_t launch_build_lut(const TrackParams &P, const uint8_t *pixels, int pitch, int nbeads, int plane,
                              const float2 *known_pos, bool normalize, float *lut, cudaStream_t stream);

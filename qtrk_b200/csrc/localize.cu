@@ -436,6 +436,80 @@ cudaError_t launch_localize(const TrackParams &P, const uint8_t *pixels, int pit
     return cudaGetLastError();
 }
 
+// Bias-table images (QueuedTracker::ComputeZBiasCorrection, cputrack/QueuedTracker.cpp:143-189):
+// image i = bead (i / bias_planes) at the ROI centre (w/2, h/2, int division) and
+// z = (i % bias_planes) / bias_planes * planes, rendered as GenerateImageFromLUT
+// (cputrack/utils.cpp:325-390) does: the bead's LUT interpolated over planes (uniform cubic
+// B-spline over 4 planes, or linear), then ovs x ovs samples per pixel, each a linear
+// interpolation of that profile at (|offset| - minradius) * bins / (maxradius - minradius),
+// clamped to [0, bins - 2]. One block per image; block b renders image first + b into slot b
+// of `images` and `jobs` (job: frame = image index, zlutIndex = bead).
+__global__ void __launch_bounds__(256) lut_image_kernel(const float *__restrict__ lut, int nb, int planes, int first,
+                                                        int bias_planes, int w, int h, float minr, float maxr,
+                                                        int ovs, int spline, float *__restrict__ images,
+                                                        LocalizationJob *__restrict__ jobs)
+{
+    extern __shared__ float zi[];  // [nb]
+    const int img = first + blockIdx.x;
+    const int bead = img / bias_planes, plane = img - bead * bias_planes;
+    const float z = plane / (float)bias_planes * planes;
+    const float *L = lut + (size_t)bead * planes * nb;
+    for (int r = threadIdx.x; r < nb; r += blockDim.x) {
+        float v;
+        if (spline) {
+            const int iz = max(1, min(planes - 3, (int)z));
+            const float t = z - iz, t2 = t * t, t3 = t2 * t;
+            const float wt[4] = {(1 - 3 * t + 3 * t2 - t3) / 6, (4 - 6 * t2 + 3 * t3) / 6,
+                                 (1 + 3 * t + 3 * t2 - 3 * t3) / 6, t3 / 6};
+            v = 0.0f;
+            for (int i = 0; i < 4; i++) v += wt[i] * L[(i - 1 + iz) * nb + r];
+        } else {
+            const int iz = (int)z;
+            if (iz >= planes - 1) {
+                v = L[(planes - 1) * nb + r];
+            } else {
+                const float a = L[iz * nb + r], b = L[(iz + 1) * nb + r];
+                v = a + (b - a) * (z - iz);
+            }
+        }
+        zi[r] = v;
+    }
+    if (threadIdx.x == 0) {
+        LocalizationJob j{};
+        j.frame = (uint32_t)img;
+        j.zlutIndex = bead;
+        jobs[blockIdx.x] = j;
+    }
+    __syncthreads();
+    const float cx = (float)(w / 2), cy = (float)(h / 2);
+    const float radialcov = nb / (maxr - minr), step = 1.0f / ovs;
+    for (int p = threadIdx.x; p < w * h; p += blockDim.x) {
+        const int y = p / w, x = p - y * w;
+        float s = 0.0f;
+        for (int ox = 0; ox < ovs; ox++)
+            for (int oy = 0; oy < ovs; oy++) {
+                const float X = x + (ox + 0.5f) * step - cx - 0.5f;
+                const float Y = y + (oy + 0.5f) * step - cy - 0.5f;
+                float r = (sqrtf(X * X + Y * Y) - minr) * radialcov;
+                if (r > nb - 2) r = (float)(nb - 2);
+                if (r < 0) r = 0;
+                const int i = (int)r;
+                s += zi[i] + (zi[i + 1] - zi[i]) * (r - i);
+            }
+        images[(size_t)blockIdx.x * w * h + p] = s / (ovs * ovs);
+    }
+}
+
+cudaError_t launch_lut_images(const float *lut, int nb, int planes, int first_image, int n_images, int bias_planes,
+                              int w, int h, float minr, float maxr, int ovs, bool spline, float *images,
+                              LocalizationJob *jobs, cudaStream_t stream)
+{
+    if (n_images <= 0) return cudaSuccess;
+    lut_image_kernel<<<n_images, 256, sizeof(float) * nb, stream>>>(lut, nb, planes, first_image, bias_planes, w, h,
+                                                                    minr, maxr, ovs, spline ? 1 : 0, images, jobs);
+    return cudaGetLastError();
+}
+
 void localize_node(const TrackParams &P, int count, cudaKernelNodeParams &kp)
 {
     kp = cudaKernelNodeParams{};

@@ -928,6 +928,91 @@ void Tracker::SetZLUTBiasTable(const float *table, int bias_planes, int count)
     }
 }
 
+// QueuedTracker::ComputeZBiasCorrection (cputrack/QueuedTracker.cpp:143-189): for every bead
+// and each of bias_planes evenly spaced z (plane / bias_planes * planes), render the bead's LUT
+// at the ROI centre (GenerateImageFromLUT with smp_per_pixel^2 samples per pixel), localize it
+// with COM, 2 QI iterations with the QI radial window, and the Z match with the Z radial window
+// on the normalised profile (a fresh CPUTracker in the reference: no calibration images, no
+// background correction, no bias table), and store z - true z. Both stages run on the GPU; the
+// table becomes this instance's bias table.
+void Tracker::ComputeZBiasTable(int bias_planes, int smp_per_pixel, bool spline, float *out)
+{
+    if (bias_planes <= 0 || smp_per_pixel <= 0) throw std::invalid_argument("ComputeZBiasTable: invalid argument");
+    DeviceGuard dg(device_);
+    WaitIdleForReconfigure();
+    TrackParams P;
+    int count, planes;
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (!d_lut_ || lut_count_ <= 0 || lut_planes_ < 2) throw std::runtime_error("ComputeZBiasTable: no Z-LUT set");
+        count = lut_count_;
+        planes = lut_planes_;
+        P = Params(2);
+    }
+    const int W = cfg.base.width, H = cfg.base.height, nb = P.z_nbins;
+    P.mode = kLT_QI | kLT_LocalizeZ | kLT_NormalizeProfile;
+    P.qi_iterations = 2;
+    P.com_bgcorrection = 0.0f;
+    P.cmp_scores = nullptr;
+    P.zbias = nullptr;
+    P.zbias_w = P.zbias_count = 0;
+    P.calib_offset = P.calib_gain = nullptr;
+    P.calib_count = 0;
+    P.zprof_f32 = nullptr;
+    P.zprof_bf16 = nullptr;
+    plan_smem(P);
+    const std::vector<float> zw = radial_bin_window(nb);
+    const int total = count * bias_planes;
+    const int chunk = std::max(1, std::min(total, (int)((256u << 20) / ((size_t)W * H * 4))));
+    float *d_zw = nullptr, *d_img = nullptr;
+    LocalizationJob *d_jobs = nullptr;
+    LocalizationResult *d_res = nullptr;
+    cudaStream_t st = nullptr;
+    std::vector<LocalizationResult> res(total);
+    auto release = [&] {
+        cudaFree(d_zw);
+        cudaFree(d_img);
+        cudaFree(d_jobs);
+        cudaFree(d_res);
+        if (st) cudaStreamDestroy(st);
+    };
+    try {
+        CheckCuda(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+        CheckCuda(cudaMalloc(&d_zw, sizeof(float) * nb), "cudaMalloc");
+        CheckCuda(cudaMalloc(&d_img, sizeof(float) * (size_t)chunk * W * H), "cudaMalloc(bias images)");
+        CheckCuda(cudaMalloc(&d_jobs, sizeof(LocalizationJob) * chunk), "cudaMalloc");
+        CheckCuda(cudaMalloc(&d_res, sizeof(LocalizationResult) * chunk), "cudaMalloc");
+        CheckCuda(cudaMemcpyAsync(d_zw, zw.data(), sizeof(float) * nb, cudaMemcpyHostToDevice, st), "upload weights");
+        P.z_weights = d_zw;
+        CheckCuda(cudaStreamWaitEvent(st, lut_ready_, 0), "cudaStreamWaitEvent");
+        for (int first = 0; first < total; first += chunk) {
+            const int n = std::min(chunk, total - first);
+            CheckCuda(launch_lut_images(P.lut, nb, planes, first, n, bias_planes, W, H, P.z_minr, P.z_maxr,
+                                        smp_per_pixel, spline, d_img, d_jobs, st),
+                      "bias image launch");
+            CheckCuda(launch_localize(P, reinterpret_cast<const uint8_t *>(d_img), W * 4, (int64_t)W * H * 4, nullptr,
+                                      d_jobs, n, d_res, st),
+                      "localize launch");
+            launches_ += 2;
+            CheckCuda(cudaMemcpyAsync(res.data() + first, d_res, sizeof(LocalizationResult) * n,
+                                      cudaMemcpyDeviceToHost, st),
+                      "download results");
+        }
+        CheckCuda(cudaStreamSynchronize(st), "bias table");
+    } catch (...) {
+        release();
+        throw;
+    }
+    release();
+    std::vector<float> table(total);
+    for (int i = 0; i < total; i++) {
+        const int plane = i % bias_planes;
+        table[i] = res[i].pos.z - plane / (float)bias_planes * planes;
+    }
+    SetZLUTBiasTable(table.data(), bias_planes, count);
+    if (out) std::copy(table.begin(), table.end(), out);
+}
+
 void Tracker::EnableRadialZLUTCompareProfile(bool enabled)
 {
     DeviceGuard dg(device_);

@@ -73,6 +73,7 @@ class Tracker : public QueuedTracker {
 
     // Extensions
     void SetZLUTBiasTable(const float *table, int bias_planes, int count);
+    void ComputeZBiasTable(int bias_planes, int smp_per_pixel, bool spline, float *out);
     int LocalizeDevice(const void *d_pixels, int pitch, int64_t roi_stride, int pdt, int count,
                        const LocalizationJob *d_jobs, LocalizationResult *d_results, cudaStream_t stream);
     // LocalizeDevice with caller-supplied profile scratch (scratch_bytes); allocates nothing.

@@ -131,3 +131,39 @@ def test_find_beads_large_frame():
     d = np.hypot(centres[inside, None, 0] - found[None, :, 0], centres[inside, None, 1] - found[None, :, 1]).min(1)
     assert (d < 3).all(), d.max()
     print(f"FindBeads 2048x2048, roi {roi}: {n.value} beads in {dt * 1e3:.1f} ms")
+
+
+@pytest.mark.parametrize("spline,smp", [(1, 4), (0, 2)])
+def test_compute_zlut_bias_table_matches_reference(ref, spline, smp):
+    """QTrkB200ComputeZLUTBiasTable (images rendered and localized on the GPU) against the
+    reference's QueuedTracker::ComputeZBiasCorrection; the table is installed as the bias table."""
+    g = load("config1_60x60_f32.npz")
+    s, lut = g["settings"], np.ascontiguousarray(g["lut"], np.float32)
+    two = np.ascontiguousarray(np.concatenate([lut, lut[:, ::-1]]))  # 2 beads, the second reversed in z
+    bias_planes = 100
+    L = ref.lib
+    L.ref_compute_zbias.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int]
+    L.ref_compute_zbias.restype = None
+    trk = L.QTrkCreateInstance(C.byref(s))
+    try:
+        L.QTrkSetRadialZLUT(trk, two.ctypes.data_as(C.c_void_p), 2, two.shape[1])
+        L.QTrkSetLocalizationMode(trk, int(g["mode"]))
+        want = np.zeros(2 * bias_planes, np.float32)
+        L.ref_compute_zbias(trk, bias_planes, want.ctypes.data, smp, spline)
+    finally:
+        L.QTrkFreeInstance(trk)
+    rois = g["rois"].astype(np.float32)[:64]
+    with QTrkInstance(s) as t:
+        t.SetRadialZLUT(two)
+        t.SetLocalizationMode(int(g["mode"]))
+        got = np.zeros(2 * bias_planes, np.float32)
+        t.lib.QTrkB200ComputeZLUTBiasTable(t.handle, bias_planes, got.ctypes.data_as(C.c_void_p), smp, spline)
+        assert "QTrkB200ComputeZLUTBiasTable" not in t.GetWarnings()
+        with_table = t.Localize(rois)
+        t.lib.QTrkB200SetZLUTBiasTable(t.handle, got.ctypes.data_as(C.c_void_p), bias_planes, 2)
+        again = t.Localize(rois)
+        t.lib.QTrkB200SetZLUTBiasTable(t.handle, None, 0, 0)
+        plain = t.Localize(rois)
+    assert np.abs(got - want).max() < 0.01, np.abs(got - want).max()
+    assert np.array_equal(with_table["pos"], again["pos"])
+    assert not np.array_equal(with_table["pos"][:, 2], plain["pos"][:, 2])
