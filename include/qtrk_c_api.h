@@ -344,6 +344,20 @@ QTRK_API void QTRK_CALLCONV RMGetConfig(struct ResultManager *rm, ResultManagerC
 QTRK_API void QTRK_CALLCONV QTrkB200RMStoreResults(struct ResultManager *rm, const LocalizationResult *results,
                                                    int count, int roi_width, int roi_height);
 
+/* Instance-level forms of the reference's handle-less calls (qtrk_c_api.h:152-158 act on every or
+ * the latest instance), as the LabVIEW layer needs them. */
+QTRK_API void QTRK_CALLCONV QTrkB200SetPixelCalibrationFactors(struct QueuedTracker *qtrk, float offsetFactor,
+                                                               float gainFactor);
+QTRK_API void QTRK_CALLCONV QTrkB200EnableRadialZLUTCompareProfile(struct QueuedTracker *qtrk, int enable);
+QTRK_API void QTRK_CALLCONV QTrkB200GetRadialZLUTCompareProfile(struct QueuedTracker *qtrk, float *dst);
+/* SetCUDADevices (cudatrack/QueuedCUDATracker.cu): the device list for cuda_device = QTrkCUDA_UseList.
+ * An instance drives one GPU, the first device of the list (the current device if the list is empty). */
+QTRK_API void QTRK_CALLCONV QTrkB200SetCUDADevices(const int *devices, int count);
+/* RMCreate with the frame-info column names as an array (rm_create of lv_resultmanager_api.cpp:26-35). */
+QTRK_API struct ResultManager *QTRK_CALLCONV QTrkB200RMCreateNamed(const char *file, const char *frameinfo,
+                                                                   ResultManagerConfig *cfg,
+                                                                   const char *const *names, int count);
+
 /*
  * Request server: real-time localization of frames from several instances on one GPU. No
  * counterpart in the reference (its callers run one QueuedTracker per camera and poll each).

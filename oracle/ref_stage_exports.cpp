@@ -140,3 +140,19 @@ REF_EXPORT void ref_read_lut_file(const char *spec, float *out, int max_n, int *
     for (int i = 0; i < lut.w * lut.h && i < max_n; i++) out[i] = lut.data[i];
     lut.free();
 }
+
+/* SampleFisherMatrix::ComputeAverageFisher (FisherMatrix.h:106-135) as qtrk_compute_fisher
+ * (lv_queuetrk_api.cpp:520-545) calls it: images from the LUT (lw bins x lh planes), sample range
+ * (1,1,1), delta 0.001. out9 = the averaged 3x3 matrix (row major). */
+#include "FisherMatrix.h"
+REF_EXPORT void ref_average_fisher(const float *lut, int lw, int lh, float minr, float maxr, int w, int h, float px,
+                                   float py, float pz, int nsamples, float maxval, float *out9)
+{
+    ImageData lutImg((float *)lut, lw, lh);
+    SampleFisherMatrix fm(maxval);
+    Matrix3X3 mat = fm.ComputeAverageFisher(vector3f(px, py, pz), nsamples, vector3f(1, 1, 1),
+                                            vector3f(1, 1, 1) * 0.001f, w, h, [&](ImageData &out, vector3f pos) {
+                                                GenerateImageFromLUT(&out, &lutImg, minr, maxr, pos);
+                                            });
+    for (int i = 0; i < 9; i++) out9[i] = mat[i];
+}

@@ -23,6 +23,8 @@ CSRC = PKG / "csrc"
 INCLUDE = ROOT / "include"
 OBJ = PKG / "_build"
 LIB = PKG / "libqtrk_b200.so"
+LV_SRC = PKG / "csrc_lv" / "lv_api.cpp"
+LV_LIB = PKG / "libqtrk_b200_lv.so"  # LabVIEW binding over the C ABI of LIB
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = [
@@ -88,7 +90,27 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         tmp.replace(LIB)
         if verbose:
             print(f"built {LIB}")
+    build_lv(force or bool(stale), verbose)
     return LIB
+
+
+def build_lv(force: bool = False, verbose: bool = False) -> Path:
+    """libqtrk_b200_lv.so: the LabVIEW binding, linked against libqtrk_b200.so (found next to it
+    through an $ORIGIN run path). NumericArrayResize and MoveBlock stay undefined: the LabVIEW
+    process that loads the binding provides them."""
+    obj = OBJ / (LV_SRC.name + ".o")
+    deps = [LV_SRC, INCLUDE / "qtrk_lv_api.h", INCLUDE / "qtrk_c_api.h", Path(__file__)]
+    if force or not obj.exists() or obj.stat().st_mtime < max(d.stat().st_mtime for d in deps):
+        _compile(LV_SRC, verbose)
+    if force or not LV_LIB.exists() or LV_LIB.stat().st_mtime < max(obj.stat().st_mtime, LIB.stat().st_mtime):
+        tmp = LV_LIB.with_suffix(".so.tmp")
+        cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), str(obj), "-L", str(PKG), "-lqtrk_b200",
+               "-Xlinker", "-rpath=$ORIGIN", "-Xcompiler", "-fPIC", "-lpthread"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed (LabVIEW binding):\n{r.stdout}\n{r.stderr}")
+        tmp.replace(LV_LIB)
+    return LV_LIB
 
 
 def main(argv=None) -> int:

@@ -773,3 +773,48 @@ QTRK_API int QTRK_CALLCONV QTrkB200WriteRadialZLUTFile(const char *path, const f
     if (!ok) set_last_error("QTrkB200WriteRadialZLUTFile: write failed");
     return ok ? 0 : -2;
 }
+
+// ---------------------------------------------------------------------------------------
+// Instance-level forms of the reference's handle-less calls, and a ResultManager constructor
+// taking its column names as an array (both for the LabVIEW layer).
+// ---------------------------------------------------------------------------------------
+QTRK_API void QTRK_CALLCONV QTrkB200SetPixelCalibrationFactors(QueuedTracker *q, float offsetFactor, float gainFactor)
+{
+    guarded(q, "QTrkB200SetPixelCalibrationFactors",
+            [&](Tracker *t) { t->SetPixelCalibrationFactors(offsetFactor, gainFactor); });
+}
+
+QTRK_API void QTRK_CALLCONV QTrkB200EnableRadialZLUTCompareProfile(QueuedTracker *q, int enable)
+{
+    guarded(q, "QTrkB200EnableRadialZLUTCompareProfile", [&](Tracker *t) { t->EnableRadialZLUTCompareProfile(enable != 0); });
+}
+
+QTRK_API void QTRK_CALLCONV QTrkB200GetRadialZLUTCompareProfile(QueuedTracker *q, float *dst)
+{
+    guarded(q, "QTrkB200GetRadialZLUTCompareProfile", [&](Tracker *t) { t->GetRadialZLUTCompareProfile(dst); });
+}
+
+QTRK_API void QTRK_CALLCONV QTrkB200SetCUDADevices(const int *devices, int count)
+{
+    std::vector<int> d;
+    for (int i = 0; devices && i < count; i++) d.push_back(devices[i]);
+    qtrk::set_device_list(d);
+}
+
+QTRK_API ResultManager *QTRK_CALLCONV QTrkB200RMCreateNamed(const char *file, const char *frameinfo,
+                                                           ResultManagerConfig *cfg, const char *const *names,
+                                                           int count)
+{
+    if (!cfg) {
+        set_last_error("QTrkB200RMCreateNamed: null config");
+        return nullptr;
+    }
+    std::vector<std::string> cols;
+    for (int i = 0; names && i < count; i++) cols.emplace_back(names[i] ? names[i] : "");
+    try {
+        return new ResultManager(file, frameinfo, *cfg, cols);
+    } catch (const std::exception &e) {
+        set_last_error(std::string("QTrkB200RMCreateNamed: ") + e.what());
+        return nullptr;
+    }
+}

@@ -114,6 +114,17 @@ void for_each_tracker(void (*fn)(Tracker *, void *), void *arg)
     std::lock_guard<std::mutex> lk(g_reg_mu);
     for (Tracker *t : g_trackers) fn(t, arg);
 }
+static std::vector<int> g_device_list;
+void set_device_list(const std::vector<int> &devices)
+{
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    g_device_list = devices;
+}
+static std::vector<int> device_list()
+{
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    return g_device_list;
+}
 float default_offset_factor() { return g_default_of; }
 float default_gain_factor() { return g_default_gf; }
 void set_default_factors(float of, float gf)
@@ -149,6 +160,8 @@ Tracker::Tracker(const QTrkSettings &settings)
         throw std::runtime_error(std::string("no usable CUDA device: ") + (e ? cudaGetErrorString(e) : "count is 0"));
     if (s.cuda_device >= 0) {
         device_ = s.cuda_device;
+    } else if (s.cuda_device == QTrkCUDA_UseList && !device_list().empty()) {
+        device_ = device_list().front();
     } else {
         // QTrkCUDA_UseAll / UseBest / UseList: one instance drives one GPU (the current one);
         // several GPUs are served by one instance per GPU.

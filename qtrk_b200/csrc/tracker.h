@@ -185,6 +185,7 @@ void register_tracker(Tracker *t);
 void unregister_tracker(Tracker *t);
 Tracker *latest_tracker();
 void for_each_tracker(void (*fn)(Tracker *, void *), void *arg);
+void set_device_list(const std::vector<int> &devices);  // QTrkCUDA_UseList devices
 float default_offset_factor();
 float default_gain_factor();
 void set_default_factors(float of, float gf);
