@@ -274,6 +274,24 @@ QTRK_API int QTRK_CALLCONV QTrkB200LocalizeDevice(struct QueuedTracker *qtrk, co
                                                   void *stream);
 
 /*
+ * The adjoint of the Z match. No counterpart in the reference. For `count` device-resident ROIs
+ * (ROI i at d_pixels + i * roi_stride_bytes, rows `pitch` bytes apart) and device positions
+ * d_xyz[3i..3i+2] (x, y in pixels, z in LUT planes) against bead d_beads[i]'s LUT (bead 0 when
+ * d_beads is NULL):
+ *   cost_i = sum_r (w_r (phat_r(x, y) - Lz_r))^2,
+ * phat the radial profile of the Z match at (x, y) (normalised when LT_NormalizeProfile is in the
+ * mode), Lz the LUT linear between planes floor(z) and floor(z)+1 (clamped), w the radial weights
+ * (1 when unset). Writes d_cost[i], d_grad_xyz[3i..3i+2] = d cost_i / d(x, y, z) and, when
+ * d_grad_lut is not NULL, ADDS d cost_i / d LUT into d_grad_lut [beads][planes][radialsteps]
+ * (zero it first). Device pointers, asynchronous on `stream`; returns 0, or < 0 on invalid
+ * arguments (-3: no Z-LUT).
+ */
+QTRK_API int QTRK_CALLCONV QTrkB200ZLUTCostGradient(struct QueuedTracker *qtrk, const void *d_pixels, int pitch,
+                                                    int64_t roi_stride_bytes, QTRK_PixelDataType_t pdt, int count,
+                                                    const float *d_xyz, const int *d_beads, float *d_cost,
+                                                    float *d_grad_xyz, float *d_grad_lut, void *stream);
+
+/*
  * QTrkB200LocalizeDevice without any device-memory allocation. No counterpart in the
  * reference. For callers that cannot allocate while they run: real-time acquisition threads
  * (camera callbacks, LabVIEW timed loops) that must keep each call's latency bounded, since

@@ -213,10 +213,10 @@ class PortOracle:
             "oracle_build_lut_bead": (None, [P, _f64p, C.c_int, C.c_double, C.c_double, C.c_int, _f64p]),
             "oracle_gauss5": (None, [_f64p, C.c_int, C.c_int, _f64p, C.c_int, _f64p, P]),
             "oracle_zcost_grad": (C.c_double, [_f64p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
-                                               C.c_double, _f32p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
-                                               P, _f64p, P]),
+                                                 C.c_double, _f32p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                                 P, C.c_int, _f64p, P]),
             "oracle_joint_refine": (None, [_f64p, C.c_int, C.c_int, C.c_double, _f64p, _f32p, C.c_int, C.c_int,
-                                           C.c_int, C.c_double, C.c_double, P, C.c_int]),
+                                           C.c_int, C.c_double, C.c_double, P, C.c_int, C.c_int]),
             "oracle_zlut_bias_correct": (C.c_double, [C.c_double, C.c_int, _f32p, C.c_int, C.c_int, C.c_int]),
             "oracle_find_beads": (C.c_int, [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
                                             C.c_float, P, C.c_int, P]),
@@ -327,24 +327,27 @@ class PortOracle:
                     lut[b, p] = r
         return lut
 
-    def zcost_grad(self, img, mean, xyz, lut, angsteps, minr, maxr, weights=None, want_lut_grad=False):
+    def zcost_grad(self, img, mean, xyz, lut, angsteps, minr, maxr, weights=None, normalize=True,
+                   want_lut_grad=False):
+        """(cost, grad xyz (3,), grad LUT (planes, bins) or None) of the radial-profile/LUT cost."""
         img = np.ascontiguousarray(img, np.float64)
         lut = np.ascontiguousarray(lut, np.float32)
         planes, nb = lut.shape
-        grad = np.zeros(3)
-        glut = np.zeros(planes * nb) if want_lut_grad else None
         w = None if weights is None else np.ascontiguousarray(weights, np.float64)
+        grad = np.zeros(3)
+        glut = np.zeros((planes, nb)) if want_lut_grad else None
         c = self.lib.oracle_zcost_grad(img, img.shape[1], img.shape[0], mean, xyz[0], xyz[1], xyz[2], lut, planes,
-                                       nb, angsteps, minr, maxr, _ptr(w), grad, _ptr(glut))
-        return (c, grad, glut.reshape(planes, nb)) if want_lut_grad else (c, grad)
+                                       nb, angsteps, minr, maxr, _ptr(w), int(normalize), grad,
+                                       glut.ctypes.data if glut is not None else None)
+        return c, grad, glut
 
-    def joint_refine(self, img, mean, xyz, lut, angsteps, minr, maxr, weights=None, steps=5):
+    def joint_refine(self, img, mean, xyz, lut, angsteps, minr, maxr, weights=None, normalize=True, steps=5):
         img = np.ascontiguousarray(img, np.float64)
         lut = np.ascontiguousarray(lut, np.float32)
         io = np.ascontiguousarray(np.array(xyz, np.float64))
         w = None if weights is None else np.ascontiguousarray(weights, np.float64)
         self.lib.oracle_joint_refine(img, img.shape[1], img.shape[0], mean, io, lut, lut.shape[0], lut.shape[1],
-                                     angsteps, minr, maxr, _ptr(w), steps)
+                                     angsteps, minr, maxr, _ptr(w), int(normalize), steps)
         return io
 
     def find_beads(self, img, sample_corner, roi, rel_dist, similarity, return_conv=False):

@@ -583,28 +583,27 @@ ORACLE_API void oracle_gauss5(const double *img, int w, int h, const double *ini
 
 /*
  * Radial-profile-to-LUT cost and its analytic gradient (the adjoint of the GPU library).
- * cost(x, y, z, L) = sum_r (w_r (p_r(x, y) - Lz_r))^2 where p is the (unnormalised) radial
- * profile of utils.cpp:275-320 at (x, y) and Lz is the LUT linearly interpolated between
- * planes floor(z) and floor(z)+1 (clamped to the table). grad = {dx, dy, dz};
- * glut (planes*nbins, may be NULL) receives d cost / d L.
+ * p(x, y) is the radial profile of utils.cpp:275-320 at (x, y): per bin the mean of the
+ * in-bounds bilinear samples over `angsteps` directions, or `mean` when at most 4 samples are
+ * in bounds; with `normalize` it is NormalizeRadialProfile'd (utils.cpp:230-261: minus its
+ * mean, divided by its RMS), as the Z match uses it. Lz is the LUT linearly interpolated
+ * between planes iz = clamp(floor(z), 0, planes-2) and iz+1. With radial weights w,
+ *   cost(x, y, z, L) = sum_r (w_r (p_r(x, y) - Lz_r))^2.
+ * d p_r / dx is the mean of the samples' bilinear x-derivatives ((v10-v00)(1-fy) + (v11-v01)fy),
+ * and likewise for y; through the normalisation,
+ *   d phat_r = (dp_r - mean(dp) - phat_r * sum_j(phat_j dp_j) / n) / rms.
  */
-ORACLE_API double oracle_zcost_grad(const double *img, int w, int h, double mean, double x, double y, double z,
-                                    const float *lut, int planes, int nbins, int angsteps, double minR, double maxR,
-                                    const double *weights, double *grad, double *glut)
+static void zprofile_grad(const double *img, int w, int h, double mean, double x, double y, int nbins,
+                          int angsteps, double minR, double maxR, int normalize, double *p, double *dpx,
+                          double *dpy)
 {
     double rstep = (maxR - minR) / nbins;
-    int iz = (int)floor(z);
-    if (iz < 0) iz = 0;
-    if (iz > planes - 2) iz = planes - 2;
-    double fz = z - iz;
-    double cost = 0, gx = 0, gy = 0, gz = 0;
-    if (glut) memset(glut, 0, sizeof(double) * planes * nbins);
     for (int i = 0; i < nbins; i++) {
         double r = minR + rstep * i, sum = 0, sx = 0, sy = 0;
         int n = 0;
         for (int a = 0; a < angsteps; a++) {
-            double ang = 2 * REF_PI_F * a / angsteps, ca = cos(ang), sa = sin(ang);
-            double px = x + ca * r, py = y + sa * r;
+            double ang = 2 * REF_PI_F * a / angsteps;
+            double px = x + cos(ang) * r, py = y + sin(ang) * r;
             int rx = (int)px, ry = (int)py;
             if (rx < 0 || ry < 0 || rx + 1 >= w || ry + 1 >= h) continue;
             double v00 = img[w * ry + rx], v10 = img[w * ry + rx + 1];
@@ -616,27 +615,69 @@ ORACLE_API double oracle_zcost_grad(const double *img, int w, int h, double mean
             sy += v1 - v0;
             n++;
         }
-        double p, dpx = 0, dpy = 0;
         if (n > MIN_RADPROFILE_SMP_COUNT) {
-            p = sum / n;
-            dpx = sx / n;
-            dpy = sy / n;
-        } else
-            p = mean;
+            p[i] = sum / n;
+            dpx[i] = sx / n;
+            dpy[i] = sy / n;
+        } else {
+            p[i] = mean;
+            dpx[i] = dpy[i] = 0;
+        }
+    }
+    if (!normalize) return;
+    double m = 0, mx = 0, my = 0;
+    for (int i = 0; i < nbins; i++) {
+        m += p[i];
+        mx += dpx[i];
+        my += dpy[i];
+    }
+    m /= nbins;
+    mx /= nbins;
+    my /= nbins;
+    double ss = 0;
+    for (int i = 0; i < nbins; i++) ss += (p[i] - m) * (p[i] - m);
+    double rms = sqrt(ss / nbins), kx = 0, ky = 0;
+    for (int i = 0; i < nbins; i++) {
+        p[i] = (p[i] - m) / rms;
+        kx += p[i] * dpx[i];
+        ky += p[i] * dpy[i];
+    }
+    kx /= nbins;
+    ky /= nbins;
+    for (int i = 0; i < nbins; i++) {
+        dpx[i] = (dpx[i] - mx - p[i] * kx) / rms;
+        dpy[i] = (dpy[i] - my - p[i] * ky) / rms;
+    }
+}
+
+/* grad = {dcost/dx, dcost/dy, dcost/dz}; glut (planes*nbins, may be NULL) = dcost/dL. */
+ORACLE_API double oracle_zcost_grad(const double *img, int w, int h, double mean, double x, double y, double z,
+                                    const float *lut, int planes, int nbins, int angsteps, double minR, double maxR,
+                                    const double *weights, int normalize, double *grad, double *glut)
+{
+    double *p = (double *)malloc(sizeof(double) * 3 * nbins), *dpx = p + nbins, *dpy = p + 2 * nbins;
+    zprofile_grad(img, w, h, mean, x, y, nbins, angsteps, minR, maxR, normalize, p, dpx, dpy);
+    int iz = (int)floor(z);
+    if (iz < 0) iz = 0;
+    if (iz > planes - 2) iz = planes - 2;
+    double fz = z - iz;
+    double cost = 0, gx = 0, gy = 0, gz = 0;
+    if (glut) memset(glut, 0, sizeof(double) * planes * nbins);
+    for (int i = 0; i < nbins; i++) {
         double l0 = lut[iz * nbins + i], l1 = lut[(iz + 1) * nbins + i];
-        double lz = l0 + (l1 - l0) * fz;
         double wr = weights ? weights[i] : 1.0;
-        double e = wr * (p - lz);
-        cost += e * e;
-        double de = 2 * e * wr;
-        gx += de * dpx;
-        gy += de * dpy;
+        double e = p[i] - (l0 + (l1 - l0) * fz);
+        cost += wr * wr * e * e;
+        double de = 2 * wr * wr * e;
+        gx += de * dpx[i];
+        gy += de * dpy[i];
         gz += -de * (l1 - l0);
         if (glut) {
             glut[iz * nbins + i] += -de * (1 - fz);
             glut[(iz + 1) * nbins + i] += -de * fz;
         }
     }
+    free(p);
     grad[0] = gx;
     grad[1] = gy;
     grad[2] = gz;
@@ -644,58 +685,72 @@ ORACLE_API double oracle_zcost_grad(const double *img, int w, int h, double mean
 }
 
 /*
- * Joint Gauss-Newton refinement of (x, y, z) on the cost above: J^T J from the per-bin
- * residual Jacobian, a 3x3 solve per step with a Levenberg damping of 1e-9*trace, `steps`
- * steps, z clamped to [0, planes-1]. io = {x, y, z} in, refined out.
+ * Joint Gauss-Newton refinement of (x, y, z) on the cost above plus a quadratic prior that ties
+ * (x, y) to their starting point (the QI estimate):
+ *   E = cost(x, y, z) + k ((x - x0)^2 + (y - y0)^2),  k = 100 sum_r w_r^2 (L_iz+1,r - L_iz,r)^2,
+ * 100 times the curvature of the cost along z at the starting plane. The prior is needed because
+ * a radial profile is, to first order, insensitive to where its centre is (the x-derivative of a
+ * radially symmetric image averages to zero over a circle), so the cost alone leaves x and y
+ * undetermined and its noise-driven minimum lies ~0.1 px from the truth where QI is ~0.02 px
+ * off; at this stiffness x and y keep QI's precision and z follows the LUT interpolation. Per step: residuals w_r (phat_r - Lz_r), Jacobian w_r (dphat_r/dx, dphat_r/dy,
+ * -(L_iz+1,r - L_iz,r)), normal equations (J^T J + diag(k, k, 0)) d = -(J^T res + k (x-x0, y-y0, 0))
+ * with a Levenberg term 1e-9 * trace (+1e-30) on the diagonal, solved by Cramer's rule. The step
+ * is taken if it lowers E, else halved up to 4 times; if none does, the refinement stops. z is
+ * clamped to [0, planes-1]. io = {x, y, z} in, refined out.
  */
+static double zcost_at(const double *img, int w, int h, double mean, double x, double y, double z, const float *lut,
+                       int planes, int nbins, int angsteps, double minR, double maxR, const double *weights,
+                       int normalize, double *p, double *dpx, double *dpy)
+{
+    zprofile_grad(img, w, h, mean, x, y, nbins, angsteps, minR, maxR, normalize, p, dpx, dpy);
+    int iz = (int)floor(z);
+    if (iz < 0) iz = 0;
+    if (iz > planes - 2) iz = planes - 2;
+    double fz = z - iz, cost = 0;
+    for (int i = 0; i < nbins; i++) {
+        double l0 = lut[iz * nbins + i], l1 = lut[(iz + 1) * nbins + i];
+        double wr = weights ? weights[i] : 1.0;
+        double e = p[i] - (l0 + (l1 - l0) * fz);
+        cost += wr * wr * e * e;
+    }
+    return cost;
+}
+
 ORACLE_API void oracle_joint_refine(const double *img, int w, int h, double mean, double *io, const float *lut,
                                     int planes, int nbins, int angsteps, double minR, double maxR,
-                                    const double *weights, int steps)
+                                    const double *weights, int normalize, int steps)
 {
-    double rstep = (maxR - minR) / nbins;
+    double *p = (double *)malloc(sizeof(double) * 3 * nbins), *dpx = p + nbins, *dpy = p + 2 * nbins;
+    const double x0 = io[0], y0 = io[1];
+    double k = 0; /* prior stiffness, set from the plane of the current z */
+    double cur = 0;
     for (int s = 0; s < steps; s++) {
         double x = io[0], y = io[1], z = io[2];
+        zprofile_grad(img, w, h, mean, x, y, nbins, angsteps, minR, maxR, normalize, p, dpx, dpy);
         int iz = (int)floor(z);
         if (iz < 0) iz = 0;
         if (iz > planes - 2) iz = planes - 2;
         double fz = z - iz;
-        double A[3][3] = {{0}}, g[3] = {0};
+        double A[3][3] = {{0}}, g[3] = {0}, cost = 0;
         for (int i = 0; i < nbins; i++) {
-            double r = minR + rstep * i, sum = 0, sx = 0, sy = 0;
-            int n = 0;
-            for (int a = 0; a < angsteps; a++) {
-                double ang = 2 * REF_PI_F * a / angsteps;
-                double px = x + cos(ang) * r, py = y + sin(ang) * r;
-                int rx = (int)px, ry = (int)py;
-                if (rx < 0 || ry < 0 || rx + 1 >= w || ry + 1 >= h) continue;
-                double v00 = img[w * ry + rx], v10 = img[w * ry + rx + 1];
-                double v01 = img[w * (ry + 1) + rx], v11 = img[w * (ry + 1) + rx + 1];
-                double fx = px - rx, fy = py - ry;
-                double v0 = v00 + (v10 - v00) * fx, v1 = v01 + (v11 - v01) * fx;
-                sum += v0 + (v1 - v0) * fy;
-                sx += (v10 - v00) * (1 - fy) + (v11 - v01) * fy;
-                sy += v1 - v0;
-                n++;
-            }
-            double p, J[3] = {0, 0, 0};
             double l0 = lut[iz * nbins + i], l1 = lut[(iz + 1) * nbins + i];
-            if (n > MIN_RADPROFILE_SMP_COUNT) {
-                p = sum / n;
-                J[0] = sx / n;
-                J[1] = sy / n;
-            } else
-                p = mean;
-            J[2] = -(l1 - l0);
             double wr = weights ? weights[i] : 1.0;
-            double e = wr * (p - (l0 + (l1 - l0) * fz));
+            double J[3] = {dpx[i], dpy[i], -(l1 - l0)};
+            double e = p[i] - (l0 + (l1 - l0) * fz);
+            cost += wr * wr * e * e;
             for (int a = 0; a < 3; a++) {
-                g[a] += wr * J[a] * e;
+                g[a] += wr * wr * J[a] * e;
                 for (int b = 0; b < 3; b++) A[a][b] += wr * wr * J[a] * J[b];
             }
         }
+        if (s == 0) k = 100.0 * A[2][2];
+        cur = cost + k * ((x - x0) * (x - x0) + (y - y0) * (y - y0));
+        A[0][0] += k;
+        A[1][1] += k;
+        g[0] += k * (x - x0);
+        g[1] += k * (y - y0);
         double tr = A[0][0] + A[1][1] + A[2][2];
         for (int a = 0; a < 3; a++) A[a][a] += 1e-9 * tr + 1e-30;
-        /* solve A d = -g by Cramer's rule */
         double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) -
                      A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
                      A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
@@ -709,12 +764,25 @@ ORACLE_API void oracle_joint_refine(const double *img, int w, int h, double mean
                     M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0])) /
                    det;
         }
-        io[0] = x + d[0];
-        io[1] = y + d[1];
-        io[2] = z + d[2];
-        if (io[2] < 0) io[2] = 0;
-        if (io[2] > planes - 1) io[2] = planes - 1;
+        int taken = 0;
+        for (int hv = 0; hv < 5 && !taken; hv++) {
+            double t = ldexp(1.0, -hv), nz = z + t * d[2], nx = x + t * d[0], ny = y + t * d[1];
+            if (nz < 0) nz = 0;
+            if (nz > planes - 1) nz = planes - 1;
+            double c = zcost_at(img, w, h, mean, nx, ny, nz, lut, planes, nbins, angsteps, minR, maxR, weights,
+                                normalize, p, dpx, dpy) +
+                       k * ((nx - x0) * (nx - x0) + (ny - y0) * (ny - y0));
+            if (c < cur) {
+                io[0] = x + t * d[0];
+                io[1] = y + t * d[1];
+                io[2] = nz;
+                cur = c;
+                taken = 1;
+            }
+        }
+        if (!taken) break;
     }
+    free(p);
 }
 
 /*

@@ -555,6 +555,17 @@ QTRK_API void QTRK_CALLCONV QTrkB200ComputeZLUTBiasTable(QueuedTracker *q, int b
             [&](Tracker *t) { t->ComputeZBiasTable(bias_planes, smpPerPixel, useSplineInterp != 0, result); });
 }
 
+QTRK_API int QTRK_CALLCONV QTrkB200ZLUTCostGradient(QueuedTracker *q, const void *d_pixels, int pitch,
+                                                    int64_t roi_stride_bytes, QTRK_PixelDataType_t pdt, int count,
+                                                    const float *d_xyz, const int *d_beads, float *d_cost,
+                                                    float *d_grad_xyz, float *d_grad_lut, void *stream)
+{
+    return guarded_ret<int>(q, "QTrkB200ZLUTCostGradient", -100, [&](Tracker *t) {
+        return t->ZLUTCostGradient(d_pixels, pitch, roi_stride_bytes, pdt, count, d_xyz, d_beads, d_cost, d_grad_xyz,
+                                   d_grad_lut, static_cast<cudaStream_t>(stream));
+    });
+}
+
 QTRK_API int QTRK_CALLCONV QTrkB200LocalizeDevice(QueuedTracker *q, const void *d_pixels, int pitch,
                                                   int64_t roi_stride_bytes, QTRK_PixelDataType_t pdt, int count,
                                                   const LocalizationJob *d_jobs, LocalizationResult *d_results,

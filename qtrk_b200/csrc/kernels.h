@@ -33,6 +33,19 @@ cudaError_t launch_lut_images(const float *lut, int nb, int planes, int first_im
                               int w, int h, float minr, float maxr, int ovs, bool spline, float *images,
                               LocalizationJob *jobs, cudaStream_t stream);
 
+// Radial-profile/LUT cost of `count` ROIs (ROI i at pixels + i*roi_stride) at xyz[3i..3i+2] against
+// bead beads[i]'s LUT (bead 0 when beads is null): cost[i], grad[3i..] = d cost / d(x, y, z), and
+// glut [beads][planes][bins] += d cost / d LUT (glut may be null). One kernel launch.
+cudaError_t launch_zcost_grad(const TrackParams &P, const uint8_t *pixels, int pitch, int64_t roi_stride, int count,
+                              const float *xyz, const int *beads, float *cost, float *grad, float *glut,
+                              cudaStream_t stream);
+
+// Joint Gauss-Newton (x, y, z) refinement of localized ROIs, in place on results (same ROI
+// addressing as launch_localize). One kernel launch.
+cudaError_t launch_joint_refine(const TrackParams &P, const uint8_t *pixels, int pitch, int64_t roi_stride,
+                                const int64_t *roi_offsets, const LocalizationJob *jobs, int count,
+                                LocalizationResult *results, cudaStream_t stream);
+
 // One BuildLUT plane: nbeads ROIs stacked at pitch*H; adds each profile to lut[bead][plane].
 cudaError_t launch_build_lut(const TrackParams &P, const uint8_t *pixels, int pitch, int nbeads, int plane,
                              const float2 *known_pos, bool normalize, float *lut, cudaStream_t stream);

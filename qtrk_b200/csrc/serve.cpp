@@ -314,7 +314,7 @@ void Server::LaunchBatch(Lane &lane, Tracker *t, const std::vector<Request *> &b
     ck(cudaMemcpyAsync(lane.d_jobs, lane.h_jobs, sizeof(LocalizationJob) * k, cudaMemcpyHostToDevice, lane.stream),
        "H2D jobs");
     TrackParams P = t->AcquireLaunch(pdt, lane.stream);
-    P.mode &= ~kLT_ZMatchBF16;  // one ROI per bead per frame: the plain Z match
+    P.mode &= ~(kLT_ZMatchBF16 | kLT_JointRefine);  // the graph holds the localization kernel alone
     int bucket = 32;
     while (bucket < k) bucket <<= 1;
     Graph &g = GraphFor(lane, batch[0]->inst, bucket, P);

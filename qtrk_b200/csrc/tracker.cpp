@@ -351,6 +351,44 @@ TrackParams Tracker::Params(int pdt) const
     return P;
 }
 
+// The adjoint of the Z match (see adjoint.cu): cost and gradients of `count` device-resident ROIs
+// at device positions xyz against the instance's LUT, on the caller's stream.
+int Tracker::ZLUTCostGradient(const void *d_pixels, int pitch, int64_t roi_stride, int pdt, int count,
+                              const float *d_xyz, const int *d_beads, float *d_cost, float *d_grad, float *d_glut,
+                              cudaStream_t stream)
+{
+    if (!d_pixels || !d_xyz || !d_cost || !d_grad || count < 0 || pdt < 0 || pdt > 2) {
+        Warn("QTrkB200ZLUTCostGradient: invalid argument");
+        return -1;
+    }
+    if (pitch < cfg.base.width * pdt_bytes(pdt)) {
+        Warn("QTrkB200ZLUTCostGradient: pitch smaller than a row");
+        return -2;
+    }
+    DeviceGuard dg(device_);
+    TrackParams P;
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        P = Params(pdt);
+    }
+    if (!P.lut || P.lut_count <= 0 || P.lut_planes < 2) {
+        Warn("QTrkB200ZLUTCostGradient: no Z-LUT set");
+        return -3;
+    }
+    CheckCuda(cudaStreamWaitEvent(stream, lut_ready_, 0), "cudaStreamWaitEvent");
+    CheckCuda(launch_zcost_grad(P, static_cast<const uint8_t *>(d_pixels), pitch, roi_stride, count, d_xyz, d_beads,
+                                d_cost, d_grad, d_glut, stream),
+              "cost gradient launch");
+    launches_++;
+    return 0;
+}
+
+// LT_B200_JointRefine: a joint Gauss-Newton pass follows the Z fit when the mode has one.
+bool Tracker::RefineAfterZ(const TrackParams &P)
+{
+    return (P.mode & kLT_JointRefine) && (P.mode & kLT_LocalizeZ) && P.lut && P.lut_count > 0 && P.lut_planes >= 2;
+}
+
 TrackParams Tracker::AcquireLaunch(int pdt, cudaStream_t stream)
 {
     std::lock_guard<std::mutex> lk(mu_);
@@ -496,6 +534,12 @@ void Tracker::SubmitLocked(int idx)
         Q.count = s.count;
         Q.results = s.d_res;
         CheckCuda(launch_zmatch_tc(Q, ntiles, s.stream), "Z-match kernel launch");
+        launches_++;
+    }
+    if (RefineAfterZ(P)) {
+        CheckCuda(launch_joint_refine(P, s.d_pix, s.pitch, (int64_t)roib, s.frame ? s.d_off : nullptr, s.d_jobs,
+                                      s.count, s.d_res, s.stream),
+                  "joint refine launch");
         launches_++;
     }
     CheckCuda(cudaMemcpyAsync(s.h_res, s.d_res, sizeof(LocalizationResult) * s.count, cudaMemcpyDeviceToHost, s.stream),
@@ -1252,6 +1296,12 @@ int Tracker::LocalizeDevice(const void *d_pixels, int pitch, int64_t roi_stride,
         CheckCuda(launch_zmatch_tc(Q, (count + 127) / 128, stream), "Z-match kernel launch");
         launches_++;
     }
+    if (RefineAfterZ(P)) {
+        CheckCuda(launch_joint_refine(P, static_cast<const uint8_t *>(d_pixels), pitch, roi_stride, nullptr, d_jobs,
+                                      count, d_results, stream),
+                  "joint refine launch");
+        launches_++;
+    }
     return 0;
 }
 
@@ -1323,6 +1373,12 @@ int Tracker::LocalizeDeviceNoAlloc(const void *d_pixels, int pitch, int64_t roi_
     launches_++;
     if (tc) {
         CheckCuda(launch_zmatch_tc(Q, (count + 127) / 128, stream), "Z-match kernel launch");
+        launches_++;
+    }
+    if (RefineAfterZ(P)) {
+        CheckCuda(launch_joint_refine(P, static_cast<const uint8_t *>(d_pixels), pitch, roi_stride, nullptr, d_jobs,
+                                      count, d_results, stream),
+                  "joint refine launch");
         launches_++;
     }
     return 0;

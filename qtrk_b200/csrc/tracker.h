@@ -80,6 +80,8 @@ class Tracker : public QueuedTracker {
     int LocalizeDeviceNoAlloc(const void *d_pixels, int pitch, int64_t roi_stride, int pdt, int count,
                               const LocalizationJob *d_jobs, LocalizationResult *d_results, cudaStream_t stream,
                               void *scratch, size_t scratch_bytes);
+    int ZLUTCostGradient(const void *d_pixels, int pitch, int64_t roi_stride, int pdt, int count, const float *d_xyz,
+                         const int *d_beads, float *d_cost, float *d_grad, float *d_glut, cudaStream_t stream);
     int64_t LaunchCount() const { return launches_.load(); }
     void Warn(const std::string &msg);
     int device() const { return device_; }
@@ -117,6 +119,7 @@ class Tracker : public QueuedTracker {
     void CheckCuda(cudaError_t e, const char *what);
     static bool IsPinned(const void *p);
     bool UseTensorCoreMatch() const;     // mode asks for it and the LUT shape allows it
+    static bool RefineAfterZ(const TrackParams &P);
     void PrepareTensorCoreLUT();         // BF16 weighted LUT + norms when stale (LUT stream)
     ZMatchParams TensorCoreParams() const;
     int BuildTiles(const LocalizationJob *jobs, int count, int *perm, int4 *tiles) const;
