@@ -292,6 +292,26 @@ QTRK_API int QTRK_CALLCONV QTrkB200ZLUTCostGradient(struct QueuedTracker *qtrk, 
                                                     float *d_grad_xyz, float *d_grad_lut, void *stream);
 
 /*
+ * Z-LUT refinement from a calibration stack. No counterpart in the reference. The device stack
+ * holds `planes` x `beads` ROIs, ROI (plane k, bead b) at d_stack + (k * beads + b) * roi_stride_bytes
+ * (the order BuildLUT is fed in); the instance's LUT must have `beads` x `planes` rows (typically the
+ * BuildLUT result). d_xy (device, [planes][beads][2], may be NULL) gives each ROI's bead position; NULL
+ * locates them with COM + QI. Minimises, over the LUT and one z offset per plane (the stage position
+ * error, common to all beads),
+ *   sum_{k,b} cost(x, y, k + d_k, L_b) + smoothness * sum |L_b,k+1 - 2 L_b,k + L_b,k-1|^2
+ * (cost as in QTrkB200ZLUTCostGradient) with `iterations` diagonally preconditioned steps. The data
+ * term alone is already minimal at the BuildLUT result (each row absorbs its plane's image), so the
+ * smoothness weight must be > 0 for anything to change; offsets keep zero mean and zero linear trend.
+ * The refined LUT replaces the instance's LUT (its bias table is kept). plane_z (host, `planes`, may
+ * be NULL) receives k + d_k; cost_history (host, iterations + 1, may be NULL) the objective before each
+ * iteration and at the end.
+ */
+QTRK_API void QTRK_CALLCONV QTrkB200RefineZLUT(struct QueuedTracker *qtrk, const void *d_stack, int pitch,
+                                               int64_t roi_stride_bytes, QTRK_PixelDataType_t pdt, int beads, int planes,
+                                               const float *d_xy, int iterations, float smoothness, float *plane_z,
+                                               float *cost_history);
+
+/*
  * QTrkB200LocalizeDevice without any device-memory allocation. No counterpart in the
  * reference. For callers that cannot allocate while they run: real-time acquisition threads
  * (camera callbacks, LabVIEW timed loops) that must keep each call's latency bounded, since

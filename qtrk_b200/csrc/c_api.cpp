@@ -566,6 +566,16 @@ QTRK_API int QTRK_CALLCONV QTrkB200ZLUTCostGradient(QueuedTracker *q, const void
     });
 }
 
+QTRK_API void QTRK_CALLCONV QTrkB200RefineZLUT(QueuedTracker *q, const void *d_stack, int pitch, int64_t roi_stride_bytes,
+                                               QTRK_PixelDataType_t pdt, int beads, int planes, const float *d_xy,
+                                               int iterations, float smoothness, float *plane_z, float *cost_history)
+{
+    guarded(q, "QTrkB200RefineZLUT", [&](Tracker *t) {
+        t->RefineZLUT(d_stack, pitch, roi_stride_bytes, pdt, beads, planes, d_xy, iterations, smoothness, plane_z,
+                      cost_history);
+    });
+}
+
 QTRK_API int QTRK_CALLCONV QTrkB200LocalizeDevice(QueuedTracker *q, const void *d_pixels, int pitch,
                                                   int64_t roi_stride_bytes, QTRK_PixelDataType_t pdt, int count,
                                                   const LocalizationJob *d_jobs, LocalizationResult *d_results,

@@ -383,6 +383,217 @@ int Tracker::ZLUTCostGradient(const void *d_pixels, int pitch, int64_t roi_strid
     return 0;
 }
 
+// Z-LUT refinement from a calibration stack (no counterpart in the reference). ROI (plane k, bead b)
+// of the stack is at d_stack + (k * beads + b) * roi_stride; its bead position (x, y) comes from
+// d_xy [planes][beads][2] or, when that is null, from COM + QI on the GPU (the BuildLUT rule). The
+// objective over the LUT L and one z offset per plane (the stage position error, shared by all
+// beads) is
+//   E = sum_{k,b} cost(x_kb, y_kb, k + d_k, L_b) + smoothness * sum_{b,k} |L_b,k+1 - 2 L_b,k + L_b,k-1|^2,
+// cost the radial-profile/LUT cost of the adjoint kernel. Without the smoothness term a LUT
+// built from the same stack already minimises the data term exactly (each plane's row absorbs
+// its image), so nothing can move; with it, noise and stage errors that make the rows rough are
+// traded against the fit. Each iteration: one adjoint launch over the whole stack (cost, d/dz,
+// d/dL on the GPU), then on the host a Gauss-Newton step per plane offset (gradient over the
+// beads / curvature sum_r w^2 (L_k+1 - L_k)^2, clamped to +-0.5 plane; offsets keep zero mean and
+// zero linear trend, the gauge a LUT cannot see), a diagonally preconditioned step on L (0.7 x
+// gradient / exact diagonal curvature of data + smoothness terms), renormalisation of every LUT
+// row when profiles are normalised, and the LUT upload. cost_history[i] = E before iteration i
+// (iterations + 1 values); plane_z[k] = k + d_k.
+void Tracker::RefineZLUT(const void *d_stack, int pitch, int64_t roi_stride, int pdt, int beads, int planes,
+                         const float *d_xy, int iterations, float smoothness, float *plane_z, float *cost_history)
+{
+    if (!d_stack || beads <= 0 || planes < 3 || iterations < 0 || pdt < 0 || pdt > 2 || smoothness < 0)
+        throw std::invalid_argument("RefineZLUT: invalid argument");
+    DeviceGuard dg(device_);
+    WaitIdleForReconfigure();
+    const int nb = cfg.zlut_radialsteps;
+    TrackParams P;
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (!d_lut_ || lut_count_ != beads || lut_planes_ != planes)
+            throw std::invalid_argument("RefineZLUT: the instance's Z-LUT must have `beads` x `planes` rows");
+        P = Params(pdt);
+    }
+    if (pitch < cfg.base.width * pdt_bytes(pdt)) throw std::invalid_argument("RefineZLUT: pitch smaller than a row");
+    const int n = beads * planes;
+    const size_t lsz = (size_t)beads * planes * nb;
+    std::vector<float> L(lsz);
+    GetRadialZLUT(L.data());
+    std::vector<double> w2(nb, 1.0);
+    if (P.z_weights) {
+        std::vector<float> w(nb);
+        CheckCuda(cudaMemcpy(w.data(), P.z_weights, sizeof(float) * nb, cudaMemcpyDeviceToHost), "weights");
+        for (int r = 0; r < nb; r++) w2[r] = (double)w[r] * w[r];
+    }
+    const bool normalize = (P.mode & kLT_NormalizeProfile) != 0;
+    float *d_xyz = nullptr, *d_cost = nullptr, *d_grad = nullptr, *d_glut = nullptr;
+    int *d_beads = nullptr;
+    LocalizationResult *d_res = nullptr;
+    cudaStream_t st = nullptr;
+    auto release = [&] {
+        cudaFree(d_xyz);
+        cudaFree(d_cost);
+        cudaFree(d_grad);
+        cudaFree(d_glut);
+        cudaFree(d_beads);
+        cudaFree(d_res);
+        if (st) cudaStreamDestroy(st);
+    };
+    std::vector<double> d(planes, 0.0);
+    try {
+        CheckCuda(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
+        CheckCuda(cudaMalloc(&d_xyz, sizeof(float) * 3 * n), "cudaMalloc");
+        CheckCuda(cudaMalloc(&d_cost, sizeof(float) * n), "cudaMalloc");
+        CheckCuda(cudaMalloc(&d_grad, sizeof(float) * 3 * n), "cudaMalloc");
+        CheckCuda(cudaMalloc(&d_glut, sizeof(float) * lsz), "cudaMalloc");
+        CheckCuda(cudaMalloc(&d_beads, sizeof(int) * n), "cudaMalloc");
+        std::vector<int> hb(n);
+        for (int i = 0; i < n; i++) hb[i] = i % beads;
+        CheckCuda(cudaMemcpyAsync(d_beads, hb.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st), "upload beads");
+        // bead positions
+        std::vector<float> xy(2 * (size_t)n);
+        if (d_xy) {
+            CheckCuda(cudaMemcpyAsync(xy.data(), d_xy, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost, st), "positions");
+        } else {
+            TrackParams Q = P;
+            Q.mode = kLT_QI | (P.mode & kLT_ClearFirstFourPixels);
+            Q.qi_rweights = nullptr;  // BuildLUT's QI runs without radial weights (QueuedCPUTracker.cpp:603)
+            plan_smem(Q);
+            CheckCuda(cudaMalloc(&d_res, sizeof(LocalizationResult) * n), "cudaMalloc");
+            CheckCuda(cudaStreamWaitEvent(st, lut_ready_, 0), "cudaStreamWaitEvent");
+            CheckCuda(launch_localize(Q, static_cast<const uint8_t *>(d_stack), pitch, roi_stride, nullptr, nullptr, n,
+                                      d_res, st),
+                      "localize launch");
+            launches_++;
+            std::vector<LocalizationResult> res(n);
+            CheckCuda(cudaMemcpyAsync(res.data(), d_res, sizeof(LocalizationResult) * n, cudaMemcpyDeviceToHost, st),
+                      "download positions");
+            CheckCuda(cudaStreamSynchronize(st), "positions");
+            for (int i = 0; i < n; i++) {
+                xy[2 * i] = res[i].pos.x;
+                xy[2 * i + 1] = res[i].pos.y;
+            }
+        }
+        CheckCuda(cudaStreamSynchronize(st), "positions");
+        std::vector<float> xyz(3 * (size_t)n), cost(n), grad(3 * (size_t)n), glut(lsz);
+        std::vector<double> H(lsz), G(lsz);
+        for (int it = 0; it <= iterations; it++) {
+            for (int k = 0; k < planes; k++)
+                for (int b = 0; b < beads; b++) {
+                    const int i = k * beads + b;
+                    xyz[3 * i] = xy[2 * i];
+                    xyz[3 * i + 1] = xy[2 * i + 1];
+                    xyz[3 * i + 2] = (float)(k + d[k]);
+                }
+            CheckCuda(cudaMemcpyAsync(d_xyz, xyz.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice, st), "xyz");
+            CheckCuda(cudaMemsetAsync(d_glut, 0, sizeof(float) * lsz, st), "clear gradient");
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                P = Params(pdt);
+            }
+            CheckCuda(cudaStreamWaitEvent(st, lut_ready_, 0), "cudaStreamWaitEvent");
+            CheckCuda(launch_zcost_grad(P, static_cast<const uint8_t *>(d_stack), pitch, roi_stride, n, d_xyz, d_beads,
+                                        d_cost, d_grad, d_glut, st),
+                      "cost gradient launch");
+            launches_++;
+            CheckCuda(cudaMemcpyAsync(cost.data(), d_cost, sizeof(float) * n, cudaMemcpyDeviceToHost, st), "cost");
+            CheckCuda(cudaMemcpyAsync(grad.data(), d_grad, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, st), "grad");
+            CheckCuda(cudaMemcpyAsync(glut.data(), d_glut, sizeof(float) * lsz, cudaMemcpyDeviceToHost, st), "glut");
+            CheckCuda(cudaStreamSynchronize(st), "cost gradient");
+            // data term + smoothness term and its gradient / diagonal curvature
+            double E = 0;
+            for (int i = 0; i < n; i++) E += cost[i];
+            std::fill(G.begin(), G.end(), 0.0);
+            std::fill(H.begin(), H.end(), 0.0);
+            for (int b = 0; b < beads; b++)
+                for (int k = 1; k + 1 < planes; k++)
+                    for (int r = 0; r < nb; r++) {
+                        const size_t i0 = ((size_t)b * planes + k) * nb + r;
+                        const double d2 = (double)L[i0 + nb] - 2.0 * L[i0] + L[i0 - nb];
+                        E += smoothness * d2 * d2;
+                        G[i0 - nb] += 2 * smoothness * d2;
+                        G[i0] += -4 * smoothness * d2;
+                        G[i0 + nb] += 2 * smoothness * d2;
+                        H[i0 - nb] += 2 * smoothness;
+                        H[i0] += 8 * smoothness;
+                        H[i0 + nb] += 2 * smoothness;
+                    }
+            if (cost_history) cost_history[it] = (float)E;
+            if (it == iterations) break;
+            // plane offsets: Gauss-Newton on the data term, gauge-fixed
+            std::vector<double> dnew(d);
+            for (int k = 0; k < planes; k++) {
+                double gk = 0, hk = 0;
+                const double z = k + d[k];
+                const int iz = std::max(0, std::min(planes - 2, (int)std::floor(z)));
+                for (int b = 0; b < beads; b++) {
+                    gk += grad[3 * (k * beads + b) + 2];
+                    const float *l0 = &L[((size_t)b * planes + iz) * nb];
+                    for (int r = 0; r < nb; r++) {
+                        const double dl = (double)l0[nb + r] - l0[r];
+                        hk += 2 * w2[r] * dl * dl;
+                    }
+                }
+                if (hk > 0) dnew[k] = d[k] - std::max(-0.5, std::min(0.5, gk / hk));
+            }
+            double sk = 0, skk = 0, sd = 0, skd = 0;
+            for (int k = 0; k < planes; k++) {
+                sk += k;
+                skk += (double)k * k;
+                sd += dnew[k];
+                skd += k * dnew[k];
+            }
+            const double den = planes * skk - sk * sk;
+            const double slope = den != 0 ? (planes * skd - sk * sd) / den : 0.0, icpt = (sd - slope * sk) / planes;
+            for (int k = 0; k < planes; k++) dnew[k] -= icpt + slope * k;
+            // LUT step: data curvature from the z each ROI was scored at
+            for (int k = 0; k < planes; k++) {
+                const double z = k + d[k];
+                const int iz = std::max(0, std::min(planes - 2, (int)std::floor(z)));
+                const double fz = z - iz;
+                for (int b = 0; b < beads; b++) {
+                    double *h0 = &H[((size_t)b * planes + iz) * nb];
+                    for (int r = 0; r < nb; r++) {
+                        h0[r] += 2 * w2[r] * (1 - fz) * (1 - fz);
+                        h0[nb + r] += 2 * w2[r] * fz * fz;
+                    }
+                }
+            }
+            double hmax = 0;
+            for (double h : H) hmax = std::max(hmax, h);
+            for (size_t i = 0; i < lsz; i++) {
+                const double g = G[i] + glut[i];
+                L[i] = (float)(L[i] - 0.7 * g / (H[i] + 1e-6 * hmax + 1e-30));
+            }
+            if (normalize)
+                for (size_t row = 0; row < (size_t)beads * planes; row++) {
+                    float *p = &L[row * nb];
+                    double m = 0, ss = 0;
+                    for (int r = 0; r < nb; r++) m += p[r];
+                    m /= nb;
+                    for (int r = 0; r < nb; r++) ss += (p[r] - m) * (p[r] - m);
+                    const double inv = ss > 0 ? 1.0 / std::sqrt(ss / nb) : 1.0;
+                    for (int r = 0; r < nb; r++) p[r] = (float)((p[r] - m) * inv);
+                }
+            d = dnew;
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                CheckCuda(cudaMemcpyAsync(d_lut_, L.data(), sizeof(float) * lsz, cudaMemcpyHostToDevice, lut_stream_),
+                          "upload Z-LUT");
+                tc_lut_stale_ = true;
+                CheckCuda(cudaEventRecord(lut_ready_, lut_stream_), "cudaEventRecord");
+            }
+            CheckCuda(cudaStreamSynchronize(lut_stream_), "upload Z-LUT");
+        }
+    } catch (...) {
+        release();
+        throw;
+    }
+    release();
+    if (plane_z)
+        for (int k = 0; k < planes; k++) plane_z[k] = (float)(k + d[k]);
+}
+
 // LT_B200_JointRefine: a joint Gauss-Newton pass follows the Z fit when the mode has one.
 bool Tracker::RefineAfterZ(const TrackParams &P)
 {

@@ -80,6 +80,8 @@ class Tracker : public QueuedTracker {
     int LocalizeDeviceNoAlloc(const void *d_pixels, int pitch, int64_t roi_stride, int pdt, int count,
                               const LocalizationJob *d_jobs, LocalizationResult *d_results, cudaStream_t stream,
                               void *scratch, size_t scratch_bytes);
+    void RefineZLUT(const void *d_stack, int pitch, int64_t roi_stride, int pdt, int beads, int planes, const float *d_xy,
+                    int iterations, float smoothness, float *plane_z, float *cost_history);
     int ZLUTCostGradient(const void *d_pixels, int pitch, int64_t roi_stride, int pdt, int count, const float *d_xyz,
                          const int *d_beads, float *d_cost, float *d_grad, float *d_glut, cudaStream_t stream);
     int64_t LaunchCount() const { return launches_.load(); }

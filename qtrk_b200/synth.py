@@ -244,3 +244,27 @@ def bead_frame(w: int = 320, h: int = 256, n_beads: int = 12, roi: int = 32, see
         frame += 100.0 * profile(r, z) * (r < roi)
     frame = np.maximum(frame + rng.normal(0, noise, frame.shape), 0)
     return frame.astype(np.float32), centres
+
+
+def calibration_stack(nbeads: int = 16, planes: int = 60, jitter: float = 0.3, n_test: int = 400, seed: int = 8,
+                      w: int = 80):
+    """A calibration stack whose stage positions are off: plane k is recorded at z = k + d_k
+    (d ~ N(0, jitter) planes), profile parameter 0.25 z; 80x80 u16 ROIs of nbeads beads (centres
+    40 + U(+-2)), 200 + 2000 p + Poisson clipped to 4095; plus n_test held-out ROIs of the same beads
+    at z ~ U[5, planes - 6]. Returns dict(settings, stack (planes, nbeads, w, w) u16, offsets (planes,),
+    centres (nbeads, 2), test (n_test, w, w) u16, test_bead, test_z)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    cx = w / 2 + rng.uniform(-2, 2, nbeads)
+    cy = w / 2 + rng.uniform(-2, 2, nbeads)
+    off = rng.normal(0, jitter, planes)
+    stack = np.empty((planes, nbeads, w, w), np.uint16)
+    for k in range(planes):
+        lam = render(w, w, cx, cy, np.full(nbeads, 0.25 * (k + off[k])), 200.0, 2000.0, dtype=np.float32)
+        stack[k] = np.minimum(rng.poisson(lam), 4095).astype(np.uint16)
+    tb = rng.integers(0, nbeads, n_test)
+    tz = rng.uniform(5, planes - 6, n_test)
+    lam = render(w, w, cx[tb], cy[tb], 0.25 * tz, 200.0, 2000.0, dtype=np.float32)
+    test = np.minimum(rng.poisson(lam), 4095).astype(np.uint16)
+    s = config4_stack(1, 1, noise=False)[0]
+    return dict(settings=s, stack=stack, offsets=off, centres=np.stack([cx, cy], 1), test=test, test_bead=tb,
+                test_z=tz)

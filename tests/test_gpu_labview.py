@@ -181,6 +181,7 @@ def test_result_manager_and_device_info(tmp_path):
         L.qtrk_destroy(C.c_void_p(t), C.byref(lv.ErrorCluster()))
     assert len((tmp_path / "r.txt").read_text().splitlines()) == 8
     # simulate_tracking on a fresh instance with the golden LUT
+    e = lv.ErrorCluster()
     t = _create(L, s)
     try:
         lut_h = lv.handle(np.ascontiguousarray(g["lut"], np.float32))
