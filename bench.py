@@ -118,7 +118,7 @@ class ClockSampler:
 def make_workload(n: int, seed: int):
     from qtrk_b200 import synth
 
-    return synth.config2(n, seed=seed)
+    return synth.roi100_u16(n, seed=seed)
 
 
 def build_lut_on_gpu(wl):
@@ -385,7 +385,7 @@ def run_reference_arm(args) -> int:
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * args.sample / value, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "config2: 100x100 u16 ROIs, COM + QI(4 it, 64x51/quadrant) + Z-LUT 200x64 (206 angles)",
+        "config": {"workload": "100x100 u16 ROIs, COM + QI(4 it, 64x51/quadrant) + Z-LUT 200x64 (206 angles)",
                    "rois_per_step": args.sample},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                          "sample": f"{args.sample} ROIs per step of the same seeded workload, QueuedCPUTracker "
@@ -432,7 +432,7 @@ def main(argv=None) -> int:
     s.cuda_device = dev.index
     trk = QTrkInstance(s)
     # One LUT per bead: QTrkScheduleFrame gives ROI i the LUT of bead i (QueuedTracker.cpp:105),
-    # so the e2e frame path needs N_ROIS LUT rows; all are copies of the config's 200x64 LUT. The
+    # so the e2e frame path needs N_ROIS LUT rows; all are copies of the workload's 200x64 LUT. The
     # device-resident path passes no jobs (zlutIndex 0) and reads the first copy.
     if args.ncu:
         trk.SetRadialZLUT(lut)  # profiler runs use the device path only: keep the capture small
@@ -574,7 +574,7 @@ def main(argv=None) -> int:
     peaks, peak_kind = measured_peaks()
     achieved = BYTES_PER_ROI * N_ROIS / (kernel_ms / 1e3) / 1e9
     traffic = None
-    tfile = ROOT / "profiles" / "localize_config2_traffic.json"
+    tfile = ROOT / "profiles" / "localize_100x100_u16_traffic.json"
     if tfile.exists():
         traffic = json.loads(tfile.read_text()).get("dram_bytes_per_launch")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
@@ -609,8 +609,8 @@ def main(argv=None) -> int:
     line = {
         "metric": METRIC, "value": methods[chosen]["rois_per_s"], "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": methods[chosen]["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic (seeded Poisson bead images, config2 shapes)",
-        "config": {"workload": "config2: 10,000 ROIs/step of 100x100 u16; COM + QI (4 it, 64 radial x 51 angular "
+        "dtype": "f32", "data": "synthetic (seeded Poisson bead images, 100x100 u16 bead ROIs)",
+        "config": {"workload": "10,000 ROIs/step of 100x100 u16; COM + QI (4 it, 64 radial x 51 angular "
                                "per quadrant) + Z-LUT 200 planes x 64 bins (206 angles); Z match form = methods.chosen",
                    "rois_per_step": N_ROIS, "lut_planes": 200, "l2": "inputs larger than L2 (200 MB per step)",
                    "parallelism": f"replicas x{ws}"},

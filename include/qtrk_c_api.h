@@ -407,7 +407,8 @@ QTRK_API struct ResultManager *QTRK_CALLCONV QTrkB200RMCreateNamed(const char *f
  * each frame's ROI band to the lane and replays a CUDA graph holding the localization kernel and
  * the result copy (one graph per lane, instance and power-of-two ROI-count bucket). A frame's
  * results are the ones QTrkScheduleFrame gives for it: ROIs outside the frame are skipped and
- * result i carries zlutIndex = i + job->zlutIndex. The tensor-core Z match is not used here.
+ * result i carries zlutIndex = i + job->zlutIndex. The graphs hold the plain Z match: the tensor-core
+ * match and the joint refinement (LT_B200_ZMatchBF16, LT_B200_JointRefine) are not applied here.
  */
 typedef struct QTrkB200ServeStats {
     int64_t frames;            /* frames completed */

@@ -1,4 +1,4 @@
-"""Seeded synthetic bead images for the five benchmark configurations.
+"""Seeded synthetic bead images for the benchmark workloads (ROI stacks, frames, calibration stacks).
 
 No public dataset is involved: the reference measures on its own generated images
 (cputrack-test/SharedTests.h:343-416 renders ROIs from a LUT and adds Poisson noise).
@@ -8,7 +8,7 @@ Here the radial bead profile is the analytic family
 
 rendered at pixel centres (r measured from the bead centre in pixel coordinates, the
 convention of the reference's samplers), scaled, clamped at zero and Poisson-sampled
-with numpy's PCG64 generator seeded per configuration. The Z-LUT is built through the
+with numpy's PCG64 generator seeded per workload. The Z-LUT is built through the
 tracker's own BeginLUT/BuildLUT/FinalizeLUT from noise-free images clamped the same way
 (cputrack-test/SharedTests.h:35-65 builds its LUTs the same way).
 """
@@ -51,7 +51,7 @@ class Workload:
     extra: dict = field(default_factory=dict)
 
 
-def settings_config1(**kw) -> abi.QTrkSettings:
+def settings_roi60(**kw) -> abi.QTrkSettings:
     """60x60 ROIs, QI radius 3-28 px, 64 angular steps per quadrant, 40 radial steps
     (rounded to 32 by QTrkComputedConfig::Update, cputrack/QueuedTracker.cpp:20), Z-LUT
     40 bins over radius 3-28, 4 QI iterations."""
@@ -64,7 +64,7 @@ def settings_config1(**kw) -> abi.QTrkSettings:
     return s
 
 
-def settings_config2(**kw) -> abi.QTrkSettings:
+def settings_roi100(**kw) -> abi.QTrkSettings:
     """100x100 ROIs, radius 3-47 px: QI 64 radial steps x 51 angular steps per quadrant,
     Z-LUT 64 bins x 206 angles, 4 QI iterations."""
     s = abi.settings(width=100, height=100, qi_iterations=4, qi_minradius=3.0, qi_roi_coverage=0.94,
@@ -78,7 +78,7 @@ def settings_config2(**kw) -> abi.QTrkSettings:
 MODE_QI_Z = abi.LT_QI | abi.LT_LocalizeZ | abi.LT_NormalizeProfile
 
 
-def config1(n: int = 1000, seed: int = 1) -> Workload:
+def roi60_f32(n: int = 1000, seed: int = 1) -> Workload:
     """1,000 ROIs 60x60 f32: centre (30,30)+U(+-3), z ~ U[5,45] planes, 10 + 100 p_z(r) + Poisson;
     Z-LUT 50 planes, plane k <-> z = k."""
     rng = np.random.Generator(np.random.PCG64(seed))
@@ -94,11 +94,11 @@ def config1(n: int = 1000, seed: int = 1) -> Workload:
     planes = 50
     kz = np.arange(planes, dtype=np.float64)
     stack = render(w, h, np.full(planes, w / 2), np.full(planes, h / 2), kz, 10.0, 100.0).astype(np.float32)
-    return Workload("config1-60x60-f32", settings_config1(), MODE_QI_Z, rois, np.stack([cx, cy, z], 1),
+    return Workload("roi60-f32", settings_roi60(), MODE_QI_Z, rois, np.stack([cx, cy, z], 1),
                     stack[:, None], np.array([[w / 2, h / 2]], np.float32))
 
 
-def config2(n: int = 10000, seed: int = 2) -> Workload:
+def roi100_u16(n: int = 10000, seed: int = 2) -> Workload:
     """10,000 ROIs 100x100 u16 (12-bit): 200 + 2000 p(r; 0.25 z) + Poisson, clipped to 4095;
     centre (50,50)+U(+-3), z ~ U[10,190] planes; Z-LUT 200 planes x 64 bins, plane k <-> 0.25 k."""
     rng = np.random.Generator(np.random.PCG64(seed))
@@ -114,7 +114,7 @@ def config2(n: int = 10000, seed: int = 2) -> Workload:
     planes = 200
     kz = 0.25 * np.arange(planes, dtype=np.float64)
     stack = render(w, h, np.full(planes, w / 2), np.full(planes, h / 2), kz, 200.0, 2000.0).astype(np.float32)
-    return Workload("config2-100x100-u16", settings_config2(), MODE_QI_Z, rois, np.stack([cx, cy, z], 1),
+    return Workload("roi100-u16", settings_roi100(), MODE_QI_Z, rois, np.stack([cx, cy, z], 1),
                     stack[:, None], np.array([[w / 2, h / 2]], np.float32))
 
 
@@ -131,7 +131,7 @@ def gaussian_spots(n: int, w: int, cx, cy, sigma: float, photons, bg: float) -> 
     return bg + photons[:, None, None] * dy[:, :, None] * dx[:, None, :]
 
 
-def config3(n: int = 100000, seed: int = 3) -> Workload:
+def gauss16_f32(n: int = 100000, seed: int = 3) -> Workload:
     """100,000 ROIs 16x16 f32: integrated Gaussian sigma 1.5, photons log-U[500,5000],
     background 10 photons/px, Poisson; centre 8 + U(+-2)."""
     rng = np.random.Generator(np.random.PCG64(seed))
@@ -145,11 +145,11 @@ def config3(n: int = 100000, seed: int = 3) -> Workload:
         rois[a:b] = rng.poisson(gaussian_spots(b - a, w, cx[a:b], cy[a:b], 1.5, ph[a:b], 10.0)).astype(np.float32)
     s = abi.settings(width=16, height=16, gauss2D_sigma=1.5, gauss2D_iterations=8, cuda_device=-2, numThreads=-1,
                      qi_minradius=1, zlut_minradius=1)
-    return Workload("config3-16x16-gauss", s, abi.LT_Gaussian2D, rois,
+    return Workload("gauss16-f32", s, abi.LT_Gaussian2D, rois,
                     np.stack([cx, cy, np.zeros(n)], 1), extra={"photons": ph, "bg": 10.0, "sigma": 1.5})
 
 
-def config4_stack(nbeads: int = 256, planes: int = 200, seed: int = 4, noise: bool = True) -> tuple:
+def calib_stack_80x80(nbeads: int = 256, planes: int = 200, seed: int = 4, noise: bool = True) -> tuple:
     """Calibration stack: nbeads x planes ROIs of 80x80 u16, bead b at 40 + U(+-2) (fixed over z),
     plane k <-> profile parameter 0.25 k; 200 + 2000 p + Poisson, clipped to 4095.
     Returns (settings, stack (planes, nbeads, 80, 80) u16, centres (nbeads, 2))."""
@@ -181,8 +181,8 @@ class ServedCamera:
 
 
 def settings_square(w: int, **kw) -> abi.QTrkSettings:
-    """w x w ROIs with the radius span of settings_config2 scaled to the ROI (3 px to 0.47 w)."""
-    s = settings_config2(width=w, height=w)
+    """w x w ROIs with the radius span of settings_roi100 scaled to the ROI (3 px to 0.47 w)."""
+    s = settings_roi100(width=w, height=w)
     for k, v in kw.items():
         setattr(s, k, v)
     return s
@@ -265,6 +265,6 @@ def calibration_stack(nbeads: int = 16, planes: int = 60, jitter: float = 0.3, n
     tz = rng.uniform(5, planes - 6, n_test)
     lam = render(w, w, cx[tb], cy[tb], 0.25 * tz, 200.0, 2000.0, dtype=np.float32)
     test = np.minimum(rng.poisson(lam), 4095).astype(np.uint16)
-    s = config4_stack(1, 1, noise=False)[0]
+    s = calib_stack_80x80(1, 1, noise=False)[0]
     return dict(settings=s, stack=stack, offsets=off, centres=np.stack([cx, cy], 1), test=test, test_bead=tb,
                 test_z=tz)

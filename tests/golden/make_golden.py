@@ -39,7 +39,7 @@ def main() -> None:
     ref = RefOracle()
 
     # --- config 1 shape: 60x60 float, QI(32 x 64, 4 it) + Z (50 planes x 40 bins) ---
-    wl = synth.config1(24, seed=101)
+    wl = synth.roi60_f32(24, seed=101)
     lut = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
     res = ref.track(wl.settings, wl.mode, wl.rois, lut)
     res_com = ref.track(wl.settings, abi.LT_OnlyCOM, wl.rois)
@@ -51,25 +51,25 @@ def main() -> None:
                                wl.settings.zlut_minradius, cc.zlut_maxradius, True)
     z0, scores0 = ref.lut_compare(prof0, lut[0])
     np.savez_compressed(
-        HERE / "config1_60x60_f32.npz", settings=settings_dict(wl.settings), mode=wl.mode,
+        HERE / "roi60_f32.npz", settings=settings_dict(wl.settings), mode=wl.mode,
         rois=wl.rois.astype(np.uint16), lut=lut, qi_weights=rw, prof0=prof0, scores0=scores0, z0=np.float32(z0),
         **results_arrays(res), **results_arrays(res_com, "com_only_"), **results_arrays(res_qi, "qi_only_"))
 
     # --- config 2 shape: 100x100 u16, QI(64 x 51) + Z (200 planes x 64 bins) ---
-    wl2 = synth.config2(12, seed=102)
+    wl2 = synth.roi100_u16(12, seed=102)
     lut2 = ref.build_lut(wl2.settings, wl2.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl2.lut_known_pos)
     res2 = ref.track(wl2.settings, wl2.mode, wl2.rois, lut2)
-    np.savez_compressed(HERE / "config2_100x100_u16.npz", settings=settings_dict(wl2.settings), mode=wl2.mode,
+    np.savez_compressed(HERE / "roi100_u16.npz", settings=settings_dict(wl2.settings), mode=wl2.mode,
                         rois=wl2.rois, lut=lut2, **results_arrays(res2))
 
     # --- config 3 shape: 16x16 Gaussian spots, reference 4-parameter MLE (8 iterations) ---
-    wl3 = synth.config3(32, seed=103)
+    wl3 = synth.gauss16_f32(32, seed=103)
     res3 = ref.track(wl3.settings, abi.LT_Gaussian2D, wl3.rois)
-    np.savez_compressed(HERE / "config3_16x16_gauss.npz", settings=settings_dict(wl3.settings),
+    np.savez_compressed(HERE / "gauss16_f32.npz", settings=settings_dict(wl3.settings),
                         mode=abi.LT_Gaussian2D, rois=wl3.rois.astype(np.uint16), **results_arrays(res3))
 
     # --- BuildLUT through COM + QI (no known positions), 3 beads x 12 planes of 80x80 u16 ---
-    s4, stack4, _ = synth.config4_stack(nbeads=3, planes=12, seed=104, noise=False)
+    s4, stack4, _ = synth.calib_stack_80x80(nbeads=3, planes=12, seed=104, noise=False)
     lut4 = ref.build_lut(s4, stack4, abi.BUILDLUT_NORMALIZE, known_pos=None)
     lut4_raw = ref.build_lut(s4, stack4, 0, known_pos=None, finalize=False)
     np.savez_compressed(HERE / "buildlut_80x80_u16.npz", settings=settings_dict(s4), stack=stack4, lut=lut4,

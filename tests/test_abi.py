@@ -66,7 +66,7 @@ int main(void) {
 
 
 def test_computed_config_matches_reference(qlib, ref):
-    for s in [synth.settings_config1(), synth.settings_config2(), abi.settings(), abi.settings(width=37, height=37)]:
+    for s in [synth.settings_roi60(), synth.settings_roi100(), abi.settings(), abi.settings(width=37, height=37)]:
         a = abi.QTrkComputedConfig()
         qlib.QTrkGetComputedConfig(C.byref(s), C.byref(a))
         b = ref.computed_config(s)
@@ -149,7 +149,7 @@ def _gpu_present() -> bool:
 def test_create_without_gpu_fails_cleanly(qlib):
     from qtrk_b200 import tracker
 
-    s = synth.settings_config1()
+    s = synth.settings_roi60()
     h = qlib.QTrkCreateInstance(C.byref(s))
     assert not h
     assert "CUDA" in tracker.last_error() or "device" in tracker.last_error()

@@ -43,7 +43,7 @@ def _cost_grad(t, d_rois, xyz, beads=None, glut=None):
 
 
 def _setup(weights=False):
-    g = load("config1_60x60_f32.npz")
+    g = load("roi60_f32.npz")
     s, lut, mode = g["settings"], np.ascontiguousarray(g["lut"], np.float32), int(g["mode"])
     rois = g["rois"].astype(np.float32)
     t = QTrkInstance(s)
@@ -204,7 +204,7 @@ def test_joint_refine_mode_matches_oracle(port):
 
 def test_joint_refine_accuracy_vs_plain_fit():
     """On 2,000 synthetic 60x60 ROIs with known truth: refined z no worse than the 7-point fit."""
-    wl = synth.config1(2000, seed=77)
+    wl = synth.roi60_f32(2000, seed=77)
     with QTrkInstance(wl.settings) as t:
         t.SetRadialZLUTSize(1, wl.lut_stack.shape[0])
         t.BeginLUT(abi.BUILDLUT_NORMALIZE)

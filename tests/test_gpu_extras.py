@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 
 def test_zlut_bias_table(port):
     """QueuedTracker::ZLUTBiasCorrection (QueuedTracker.cpp:115-140) applied on the device."""
-    g = load("config1_60x60_f32.npz")
+    g = load("roi60_f32.npz")
     rois = g["rois"].astype(np.float32)
     planes = g["lut"].shape[1]
     rng = np.random.default_rng(5)
@@ -58,7 +58,7 @@ def test_gaussian_4p_cta_kernel_matches_reference(ref):
 
 def test_gaussian_5p_matches_fp64_oracle_and_crlb(port):
     """5-parameter (x, y, I0, bg, sigma) full-Newton MLE vs the FP64 oracle and the Cramer-Rao bound."""
-    wl = synth.config3(600, seed=52)
+    wl = synth.gauss16_f32(600, seed=52)
     s = wl.settings
     s.gauss2D_iterations = 10
     with QTrkInstance(s) as t:
@@ -137,7 +137,7 @@ def test_find_beads_large_frame():
 def test_compute_zlut_bias_table_matches_reference(ref, spline, smp):
     """QTrkB200ComputeZLUTBiasTable (images rendered and localized on the GPU) against the
     reference's QueuedTracker::ComputeZBiasCorrection; the table is installed as the bias table."""
-    g = load("config1_60x60_f32.npz")
+    g = load("roi60_f32.npz")
     s, lut = g["settings"], np.ascontiguousarray(g["lut"], np.float32)
     two = np.ascontiguousarray(np.concatenate([lut, lut[:, ::-1]]))  # 2 beads, the second reversed in z
     bias_planes = 100

@@ -39,7 +39,7 @@ def _wait(L, t, n):
 
 def test_queue_and_results_match_c_abi():
     L = lv.lv_library()
-    g = load("config1_60x60_f32.npz")
+    g = load("roi60_f32.npz")
     s, lut, mode = g["settings"], np.ascontiguousarray(g["lut"], np.float32), int(g["mode"])
     rois = g["rois"].astype(np.float32)  # 24 ROIs
     t = _create(L, s)
@@ -80,7 +80,7 @@ def test_queue_and_results_match_c_abi():
 
 def test_build_lut_bias_table_and_find_beads():
     L = lv.lv_library()
-    wl = synth.config2(1, seed=23)
+    wl = synth.roi100_u16(1, seed=23)
     s = wl.settings
     t = _create(L, s)
     e = lv.ErrorCluster()
@@ -148,7 +148,7 @@ def test_result_manager_and_device_info(tmp_path):
     di.name = lv.new_lstr()
     L.qtrkcuda_get_device(0, C.byref(di), C.byref(e))
     assert di.major == 10 and di.multiProcCount >= 100 and "B200" in lv.lstr(di.name)
-    g = load("config1_60x60_f32.npz")
+    g = load("roi60_f32.npz")
     s = g["settings"]
     rois = g["rois"].astype(np.float32)[:24]  # the fixture's 24 ROIs: 8 frames of 3 beads
     t = _create(L, s)

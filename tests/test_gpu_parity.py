@@ -50,16 +50,16 @@ def check_results(gpu, pos, com, err, mean=None, tol_xy=TOL_QI, tol_z=TOL_Z):
         np.testing.assert_allclose(gpu["imageMean"], mean, rtol=1e-6)
 
 
-def test_golden_config1_qi_z():
-    g = load("config1_60x60_f32.npz")
+def test_golden_roi60_qi_z():
+    g = load("roi60_f32.npz")
     with make_tracker(g["settings"], int(g["mode"]), g["lut"]) as t:
         r = t.Localize(g["rois"].astype(np.float32))
         assert t.KernelLaunchCount() >= 1
     check_results(r, g["pos"], g["com"], g["error"], g["mean"])
 
 
-def test_golden_config1_com_and_qi_only():
-    g = load("config1_60x60_f32.npz")
+def test_golden_roi60_com_and_qi_only():
+    g = load("roi60_f32.npz")
     rois = g["rois"].astype(np.float32)
     with make_tracker(g["settings"], abi.LT_OnlyCOM) as t:
         r = t.Localize(rois)
@@ -70,15 +70,15 @@ def test_golden_config1_com_and_qi_only():
     check_results(r, g["qi_only_pos"], g["qi_only_com"], g["qi_only_error"])
 
 
-def test_golden_config2_u16():
-    g = load("config2_100x100_u16.npz")
+def test_golden_roi100_u16():
+    g = load("roi100_u16.npz")
     with make_tracker(g["settings"], int(g["mode"]), g["lut"]) as t:
         r = t.Localize(g["rois"])
     check_results(r, g["pos"], g["com"], g["error"], g["mean"])
 
 
 def test_golden_gaussian_4p():
-    g = load("config3_16x16_gauss.npz")
+    g = load("gauss16_f32.npz")
     with make_tracker(g["settings"], int(g["mode"])) as t:
         r = t.Localize(g["rois"].astype(np.float32))
     assert np.abs(r["pos"][:, :2] - g["pos"][:, :2]).max() < TOL_QI
@@ -100,8 +100,8 @@ def test_golden_buildlut_com_qi_path():
     assert np.abs(lut - g["lut"]).max() < 2e-3
 
 
-def test_reference_pipeline_config1(ref):
-    wl = synth.config1(300, seed=21)
+def test_reference_pipeline_roi60(ref):
+    wl = synth.roi60_f32(300, seed=21)
     lut = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
     r_ref = ref.track(wl.settings, wl.mode, wl.rois, lut)
     with make_tracker(wl.settings, wl.mode, lut) as t:
@@ -109,8 +109,8 @@ def test_reference_pipeline_config1(ref):
     check_results(r, r_ref["pos"], r_ref["firstGuess"], r_ref["error"], r_ref["imageMean"])
 
 
-def test_reference_pipeline_config2(ref):
-    wl = synth.config2(150, seed=22)
+def test_reference_pipeline_roi100(ref):
+    wl = synth.roi100_u16(150, seed=22)
     lut = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
     r_ref = ref.track(wl.settings, wl.mode, wl.rois, lut)
     with make_tracker(wl.settings, wl.mode, lut) as t:
@@ -119,7 +119,7 @@ def test_reference_pipeline_config2(ref):
 
 
 def test_buildlut_known_pos_matches_reference(ref):
-    wl = synth.config2(1, seed=23)
+    wl = synth.roi100_u16(1, seed=23)
     lut_ref = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
     with QTrkInstance(wl.settings) as t:
         t.SetRadialZLUTSize(1, wl.lut_stack.shape[0])
@@ -133,9 +133,9 @@ def test_buildlut_known_pos_matches_reference(ref):
 
 def test_modes_and_options_match_reference(ref):
     """com_bgcorrection, ClearFirstFourPixels, radial weights, unnormalised profiles, u8 input."""
-    wl = synth.config1(64, seed=24)
+    wl = synth.roi60_f32(64, seed=24)
     lut = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
-    s = synth.settings_config1(com_bgcorrection=0.7)
+    s = synth.settings_roi60(com_bgcorrection=0.7)
     w = np.linspace(0.3, 1.0, lut.shape[2]).astype(np.float32)
     u8 = np.clip(wl.rois, 0, 255).astype(np.uint8)
     for mode, rois, weights in [
@@ -152,7 +152,7 @@ def test_modes_and_options_match_reference(ref):
 
 
 def test_per_bead_luts_and_zlut_index(ref):
-    wl = synth.config1(40, seed=25)
+    wl = synth.roi60_f32(40, seed=25)
     lut1 = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
     lut = np.concatenate([lut1, lut1[:, ::-1].copy(), lut1 * 0.5], axis=0)
     idx = np.arange(40) % 3
@@ -165,7 +165,7 @@ def test_per_bead_luts_and_zlut_index(ref):
 
 def test_schedule_frame_matches_crops(ref):
     """QTrkScheduleFrame crops on the device; results equal per-ROI scheduling; out-of-frame ROIs skipped."""
-    wl = synth.config1(12, seed=26)
+    wl = synth.roi60_f32(12, seed=26)
     lut1 = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
     lut = np.ascontiguousarray(np.concatenate([lut1] * 12))  # ScheduleFrame sets zlutIndex = i
     frame = np.zeros((200, 260), np.float32)
@@ -209,7 +209,7 @@ def test_schedule_frame_pinned_and_large(ref):
     """A frame larger than one staging slot is split into row bands; pinned frames are DMA'd directly."""
     import torch
 
-    wl = synth.config2(8, seed=27)
+    wl = synth.roi100_u16(8, seed=27)
     lut = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
     n_side = 60
     frame = torch.empty((n_side * 100, n_side * 100), dtype=torch.int16).pin_memory().numpy().view(np.uint16)
@@ -236,7 +236,7 @@ def test_schedule_frame_pinned_and_large(ref):
 
 def test_queue_semantics():
     """FIFO results, queue length, idle state, ClearResults, batches larger than one slot."""
-    wl = synth.config1(5000, seed=28)
+    wl = synth.roi60_f32(5000, seed=28)
     with make_tracker(wl.settings, abi.LT_QI) as t:
         assert t.IsIdle() and t.GetQueueLength() == 0
         t.ScheduleStack(wl.rois[:10])
@@ -264,7 +264,7 @@ def test_queue_semantics():
 
 
 def test_edge_cases():
-    s = synth.settings_config1()
+    s = synth.settings_roi60()
     rois = np.zeros((4, 60, 60), np.float32)
     rois[1] = 7.0                       # flat: COM is NaN -> ROI centre (QueuedCPUTracker.cpp:294-295)
     rois[2, 0:10, 0:10] = 1000.0        # bright corner: QI walks into the boundary
@@ -284,7 +284,7 @@ def test_edge_cases():
 def test_device_resident_entry_matches_host_path():
     import torch
 
-    g = load("config2_100x100_u16.npz")
+    g = load("roi100_u16.npz")
     rois = g["rois"]
     with make_tracker(g["settings"], int(g["mode"]), g["lut"]) as t:
         host = t.Localize(rois)
@@ -299,7 +299,7 @@ def test_device_resident_entry_matches_host_path():
 
 
 def test_compute_radial_profile_export_matches_reference(qlib, ref):
-    g = load("config2_100x100_u16.npz")
+    g = load("roi100_u16.npz")
     img = g["rois"][0].astype(np.float32)
     for norm in (False, True):
         a = np.zeros(64, np.float32)
@@ -313,9 +313,9 @@ def test_compute_radial_profile_export_matches_reference(qlib, ref):
 
 
 @pytest.mark.slow
-def test_full_size_config2_properties(ref):
+def test_full_size_roi100_properties(ref):
     """10,000 ROIs of 100x100 u16: every result present, FIFO, parity on a sample, accuracy vs truth."""
-    wl = synth.config2(10000, seed=2)
+    wl = synth.roi100_u16(10000, seed=2)
     lut = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
     with make_tracker(wl.settings, wl.mode, lut) as t:
         r = t.Localize(wl.rois, timeout_s=300)

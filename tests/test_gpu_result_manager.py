@@ -23,7 +23,7 @@ def _schedule(t, rois):
 
 
 def test_result_manager_on_gpu_tracker(tmp_path):
-    wl = synth.config1(N_BEADS * N_FRAMES, seed=43)
+    wl = synth.roi60_f32(N_BEADS * N_FRAMES, seed=43)
     cfg = rmm.config(N_BEADS, 1, scaling=(0.065, 0.065, 1.0), offset=(0.5, -0.5, 0.0), write_interval=7)
     with QTrkInstance(wl.settings) as t, rmm.ResultManager(str(tmp_path / "r.txt"), str(tmp_path / "i.txt"), cfg) as rm:
         t.SetLocalizationMode(abi.LT_QI)

@@ -41,7 +41,7 @@ def _u8_workload(n, seed):
     rois = np.minimum(rng.poisson(synth.render(w, w, cx, cy, z, 10.0, 100.0)), 255).astype(np.uint8)
     kz = np.arange(40, dtype=np.float64)
     stack = synth.render(w, w, np.full(40, w / 2), np.full(40, w / 2), kz, 10.0, 100.0).astype(np.float32)
-    s = synth.settings_config1(width=40, height=40)
+    s = synth.settings_roi60(width=40, height=40)
     return s, rois, stack
 
 
@@ -69,14 +69,14 @@ def fleet():
     """Four instances (each with its own LUT) and four frames for each."""
     insts, frames = [], []
     # A: 60x60 f32, QI + Z
-    wl = synth.config1(48, seed=71)
+    wl = synth.roi60_f32(48, seed=71)
     A = QTrkInstance(wl.settings)
     A.SetLocalizationMode(wl.mode)
     A.SetRadialZLUT(_lut_from_stack(wl.settings, wl.mode, wl.lut_stack[:, 0], 13))
     insts.append(A)
     frames.append([_frame_of(wl.rois[12 * k:12 * k + 12], 3, k) for k in range(4)])
     # B: 100x100 u16, QI + Z
-    wl = synth.config2(120, seed=72)
+    wl = synth.roi100_u16(120, seed=72)
     B = QTrkInstance(wl.settings)
     B.SetLocalizationMode(wl.mode)
     B.SetRadialZLUT(_lut_from_stack(wl.settings, wl.mode, wl.lut_stack[:, 0], 31))
@@ -90,7 +90,7 @@ def fleet():
     insts.append(C_)
     frames.append([_frame_of(rois[20 * k:20 * k + 20], 2, 20 + k) for k in range(4)])
     # D: 16x16 f32, Gaussian 2D (warp-per-ROI kernel), no LUT
-    wl = synth.config3(200, seed=74)
+    wl = synth.gauss16_f32(200, seed=74)
     D = QTrkInstance(wl.settings)
     D.SetLocalizationMode(wl.mode)
     insts.append(D)

@@ -49,8 +49,8 @@ def gpu_lut(wl):
         return t.GetRadialZLUT()
 
 
-def test_tensor_core_matches_plain_config2():
-    wl = synth.config2(3000, seed=31)
+def test_tensor_core_matches_plain_roi100():
+    wl = synth.roi100_u16(3000, seed=31)
     lut = gpu_lut(wl)
     plain, n0 = run(wl.settings, wl.mode, lut, wl.rois)
     tc, n1 = run(wl.settings, wl.mode | TC, lut, wl.rois)
@@ -58,15 +58,15 @@ def test_tensor_core_matches_plain_config2():
     assert n1 > n0   # the Z-match kernel (and the BF16 LUT preparation) ran
 
 
-def test_tensor_core_golden_config2():
-    g = load("config2_100x100_u16.npz")
+def test_tensor_core_golden_roi100():
+    g = load("roi100_u16.npz")
     tc, _ = run(g["settings"], int(g["mode"]) | TC, g["lut"], g["rois"])
     assert np.abs(tc["pos"][:, 2] - g["pos"][:, 2]).max() < 0.01
     assert np.abs(tc["pos"][:, :2] - g["pos"][:, :2]).max() < 1e-3
 
 
 def test_tensor_core_per_bead_groups_and_invalid_bead():
-    wl = synth.config1(900, seed=32)
+    wl = synth.roi60_f32(900, seed=32)
     lut1 = gpu_lut(wl)
     lut = np.ascontiguousarray(np.concatenate([lut1, lut1[:, ::-1], 0.5 * lut1 + 0.1, lut1[:, ::2].repeat(2, 1)[:, :50]]))
     idx = np.random.default_rng(3).integers(-1, 5, 900)   # -1 and 4 are outside the 4-bead LUT
@@ -78,7 +78,7 @@ def test_tensor_core_per_bead_groups_and_invalid_bead():
 
 def test_tensor_core_many_planes_and_weights():
     # 300 planes -> two N chunks of the MMA; 40 bins -> K padded to 48
-    wl = synth.config1(600, seed=33)
+    wl = synth.roi60_f32(600, seed=33)
     lut50 = gpu_lut(wl)
     zz = np.linspace(0, 49, 300)
     i0 = np.minimum(zz.astype(int), 48)
@@ -93,7 +93,7 @@ def test_tensor_core_many_planes_and_weights():
 def test_tensor_core_device_entry():
     import torch
 
-    wl = synth.config2(1000, seed=34)
+    wl = synth.roi100_u16(1000, seed=34)
     lut = gpu_lut(wl)
     out = {}
     for name, mode in (("plain", wl.mode), ("tc", wl.mode | TC)):

@@ -43,7 +43,7 @@ def test_create_without_gpu_fills_error_cluster():
     L.qtrk_create.restype = C.c_void_p
     e = lv.ErrorCluster()
     warn = lv.new_lstr()
-    s = synth.settings_config1()
+    s = synth.settings_roi60()
     t = L.qtrk_create(C.byref(s), C.c_void_p(warn), C.byref(e))
     assert not t and e.status == 1 and e.code == 5000 and "CUDA" in lv.lstr(e.message)
     e2 = lv.ErrorCluster()
@@ -90,7 +90,7 @@ def test_read_timestamp():
 
 def test_image_generators_match_reference(ref):
     L = lv.lv_library()
-    g = np.load(ROOT / "tests" / "golden" / "config1_60x60_f32.npz")
+    g = np.load(ROOT / "tests" / "golden" / "roi60_f32.npz")
     lut = np.ascontiguousarray(g["lut"][0], np.float32)
     img_h, lut_h = lv.handle(np.zeros((60, 60), np.float32)), lv.handle(lut)
     radii = np.array([3.0, 28.0], np.float32)
@@ -118,9 +118,9 @@ def test_compute_fisher_matches_reference(ref):
     """Same libc rand() seed: the same sample positions, the same averaged Fisher matrix."""
     L = lv.lv_library()
     libc = C.CDLL(None)
-    g = np.load(ROOT / "tests" / "golden" / "config1_60x60_f32.npz")
+    g = np.load(ROOT / "tests" / "golden" / "roi60_f32.npz")
     lut = np.ascontiguousarray(g["lut"][0], np.float32)
-    s = synth.settings_config1()
+    s = synth.settings_roi60()
     cc = abi.QTrkComputedConfig()
     ref.lib.QTrkGetComputedConfig(C.byref(s), C.byref(cc))
     fis, inv = lv.empty_handle(np.float32, 2), lv.empty_handle(np.float32, 2)

@@ -20,9 +20,9 @@ TOL_Z = 0.01      # planes
 
 
 def _settings_grid():
-    yield synth.settings_config1()
-    yield synth.settings_config2()
-    yield synth.config4_stack(1, 1)[0]
+    yield synth.settings_roi60()
+    yield synth.settings_roi100()
+    yield synth.calib_stack_80x80(1, 1)[0]
     for w in (16, 31, 40, 64, 100, 128, 150):
         for cov in (0.5, 0.7, 1.0, 3.0):
             yield abi.settings(width=w, height=w, qi_radial_coverage=cov * 1.3, qi_angular_coverage=cov,
@@ -56,7 +56,7 @@ def test_radial_bin_window(ref, port):
 
 
 def test_com_matches_reference(ref, port):
-    wl = synth.config1(16, seed=7)
+    wl = synth.roi60_f32(16, seed=7)
     for bg in (0.0, 0.5, 1.5):
         for img in wl.rois[:8]:
             a = ref.com(img, bg)
@@ -66,7 +66,7 @@ def test_com_matches_reference(ref, port):
 
 
 def test_qi_matches_reference(ref, port):
-    wl = synth.config1(12, seed=8)
+    wl = synth.roi60_f32(12, seed=8)
     cc = port.computed_config(wl.settings)
     w = ref.radial_bin_window(cc.qi_radialsteps)
     for img in wl.rois:
@@ -81,7 +81,7 @@ def test_qi_matches_reference(ref, port):
 
 def test_qi_angstep_factor_quirk(ref, port):
     """qi_angstep_factor != 1 exercises the truncated stride of cpu_tracker.cpp:655-657."""
-    wl = synth.config1(4, seed=9)
+    wl = synth.roi60_f32(4, seed=9)
     cc = port.computed_config(wl.settings)
     for f in (1.5, 2.0, 0.8):
         for img in wl.rois:
@@ -94,7 +94,7 @@ def test_qi_angstep_factor_quirk(ref, port):
 
 @pytest.mark.parametrize("normalize", [False, True])
 def test_radial_profile_matches_reference(ref, port, normalize):
-    wl = synth.config2(4, seed=10)
+    wl = synth.roi100_u16(4, seed=10)
     cc = port.computed_config(wl.settings)
     img = wl.rois[0].astype(np.float32)
     com = ref.com(img)
@@ -124,7 +124,7 @@ def test_lut_compare_matches_reference(ref, port):
 
 
 def test_gauss2d_matches_reference(ref, port):
-    wl = synth.config3(16, seed=12)
+    wl = synth.gauss16_f32(16, seed=12)
     for img in wl.rois:
         com = ref.com(img)
         a = ref.gauss2d(img, com[:2], 8, 1.5)
@@ -134,7 +134,7 @@ def test_gauss2d_matches_reference(ref, port):
 
 def test_pipeline_matches_reference(ref, port):
     """QueuedCPUTracker::ProcessJob end to end (QI + Z, normalised profiles)."""
-    wl = synth.config1(60, seed=13)
+    wl = synth.roi60_f32(60, seed=13)
     cc = port.computed_config(wl.settings)
     lut = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
     r = ref.track(wl.settings, wl.mode, wl.rois, lut)
@@ -152,7 +152,7 @@ def test_pipeline_matches_reference(ref, port):
 
 
 def test_build_lut_matches_reference(ref, port):
-    s, stack, centres = synth.config4_stack(nbeads=2, planes=6, seed=14)
+    s, stack, centres = synth.calib_stack_80x80(nbeads=2, planes=6, seed=14)
     cc = port.computed_config(s)
     for known in (None, centres):
         a = ref.build_lut(s, stack, abi.BUILDLUT_NORMALIZE, known_pos=known)
@@ -162,8 +162,8 @@ def test_build_lut_matches_reference(ref, port):
 
 # ---- golden fixtures (outputs of the reference build, committed) ----
 
-def test_port_reproduces_golden_config1(port):
-    g = load("config1_60x60_f32.npz")
+def test_port_reproduces_golden_roi60(port):
+    g = load("roi60_f32.npz")
     cc = port.computed_config(g["settings"])
     p = port.localize(cc, int(g["mode"]), g["rois"].astype(np.float32), g["lut"])
     assert np.abs(g["pos"][:, :2] - p[:, :2]).max() < TOL_QI
@@ -174,8 +174,8 @@ def test_port_reproduces_golden_config1(port):
     assert np.abs(g["com_only_pos"][:, :2] - pc[:, :2]).max() < TOL_COM
 
 
-def test_port_reproduces_golden_config2(port):
-    g = load("config2_100x100_u16.npz")
+def test_port_reproduces_golden_roi100(port):
+    g = load("roi100_u16.npz")
     cc = port.computed_config(g["settings"])
     p = port.localize(cc, int(g["mode"]), g["rois"], g["lut"])
     assert np.abs(g["pos"][:, :2] - p[:, :2]).max() < TOL_QI
@@ -183,7 +183,7 @@ def test_port_reproduces_golden_config2(port):
 
 
 def test_port_reproduces_golden_gauss(port):
-    g = load("config3_16x16_gauss.npz")
+    g = load("gauss16_f32.npz")
     cc = port.computed_config(g["settings"])
     p = port.localize(cc, int(g["mode"]), g["rois"].astype(np.float32))
     assert np.abs(g["pos"][:, :2] - p[:, :2]).max() < 1e-3

@@ -17,7 +17,7 @@ N_BEADS, N_FRAMES = 4, 12
 
 
 def _rois():
-    wl = synth.config1(N_BEADS * N_FRAMES, seed=41)
+    wl = synth.roi60_f32(N_BEADS * N_FRAMES, seed=41)
     return wl.settings, wl.rois  # ROI f*N_BEADS + b is bead b of frame f
 
 

@@ -32,7 +32,7 @@ def _results(buf) -> np.ndarray:
 def test_no_alloc_entry_matches_device_entry():
     import torch
 
-    wl = synth.config2(600, seed=41)
+    wl = synth.roi100_u16(600, seed=41)
     with QTrkInstance(wl.settings) as t:
         t.SetRadialZLUTSize(1, wl.lut_stack.shape[0])
         t.BeginLUT(abi.BUILDLUT_NORMALIZE)
