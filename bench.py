@@ -287,6 +287,130 @@ def serve_saturated(server, lib, cams, rounds: int) -> dict:
             "rois_per_s": st.rois / st.elapsed_s, "elapsed_s": st.elapsed_s}
 
 
+def _timed(stream, fn, steps: int, warmup: int) -> float:
+    """Mean milliseconds per call of fn() on `stream` (CUDA events, after warm-up)."""
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def gpu_calibration_stack(dev, nbeads: int, planes: int, w: int = 80, seed: int = 4):
+    """The calibration stack of the BuildLUT workload rendered on the GPU: bead b at 40 + U(+-2),
+    plane k at profile parameter 0.25 k, 200 + 2000 p + Poisson clipped to 4095, u16. Returns
+    (device tensor (planes, nbeads, w, w) int16 holding u16 bits, centres)."""
+    import torch
+
+    g = torch.Generator(device=dev).manual_seed(seed)
+    c = w / 2 + (torch.rand(nbeads, 2, device=dev, generator=g) * 4 - 2)
+    ys = torch.arange(w, device=dev, dtype=torch.float32)
+    out = torch.empty((planes, nbeads, w, w), dtype=torch.int16, device=dev)
+    for k in range(planes):
+        zp = 0.25 * k
+        r = torch.sqrt((ys[None, None, :] - c[:, 0, None, None]) ** 2 + (ys[None, :, None] - c[:, 1, None, None]) ** 2)
+        sg, per = 4.0 + 0.1 * zp, 6.0 + 0.05 * zp
+        lam = (200.0 + 2000.0 * torch.exp(-r * r / (2 * sg * sg)) * torch.cos(2 * np.pi * r / per)).clamp_min(0)
+        out[k] = torch.poisson(lam, generator=g).clamp_max(4095).to(torch.int16)
+    return out, c.cpu().numpy()
+
+
+def workloads_bench(dev, steps: int, warmup: int) -> dict:
+    """The other workloads: the Gaussian MLE (100,000 16x16 f32 ROIs, 4- and 5-parameter forms), BuildLUT
+    of a 256-bead x 200-plane 80x80 u16 calibration stack from host memory, the adjoint over that stack,
+    and 20 iterations of LUT refinement on it."""
+    import torch
+
+    from qtrk_b200 import abi, synth
+    from qtrk_b200.tracker import QTrkInstance
+
+    out = {}
+    launches = 0
+    stream = torch.cuda.current_stream(dev)
+    # ---- Gaussian MLE ----
+    n = 100000
+    wl = synth.gauss16_f32(n, seed=3)
+    d_rois = torch.from_numpy(wl.rois).to(dev)
+    d_res = torch.empty(n * 52, dtype=torch.uint8, device=dev)
+    s = wl.settings
+    s.cuda_device = dev.index
+    for name, mode in (("gauss_mle_4p", abi.LT_Gaussian2D), ("gauss_mle_5p", abi.LT_Gaussian2D | abi.LT_B200_Gaussian5P)):
+        with QTrkInstance(s) as t:
+            t.SetLocalizationMode(mode)
+            l0 = t.KernelLaunchCount()
+            ms = _timed(stream, lambda: t.LocalizeDevice(d_rois.data_ptr(), 64, 1024, abi.QTrkFloat, n, d_res.data_ptr(),
+                                                         stream=stream.cuda_stream), steps, warmup)
+            launches += t.KernelLaunchCount() - l0
+        res = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=abi.RESULT_DTYPE)
+        err = np.hypot(res["pos"][:, 0] - wl.true_xyz[:, 0], res["pos"][:, 1] - wl.true_xyz[:, 1])
+        out[name] = {"workload": f"{n:,} ROIs 16x16 f32, sigma 1.5, 8 iterations, device-resident",
+                     "rois_per_s": n / (ms / 1e3), "ms_per_launch": ms,
+                     "median_xy_err_nm_vs_truth": float(np.nanmedian(err) * PIXEL_NM),
+                     "non_finite_fraction": float(np.mean(~np.isfinite(err)))}
+    del d_rois, d_res
+    # ---- BuildLUT / adjoint / LUT refinement on a 256 x 200 calibration stack ----
+    nbeads, planes = 256, 200
+    d_stack, _ = gpu_calibration_stack(dev, nbeads, planes)
+    host = torch.empty(d_stack.shape, dtype=torch.int16).pin_memory()
+    host.copy_(d_stack)
+    hs = host.numpy().view(np.uint16)
+    cs = synth.calib_stack_80x80(1, 1, noise=False)[0]
+    cs.cuda_device = dev.index
+    with QTrkInstance(cs) as t:
+        t.SetLocalizationMode(synth.MODE_QI_Z)
+        t.SetRadialZLUTSize(nbeads, planes)
+        l0 = t.KernelLaunchCount()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        t.BeginLUT(abi.BUILDLUT_NORMALIZE)
+        for k in range(planes):
+            t.BuildLUT(hs[k], k)
+        t.FinalizeLUT()
+        lut = t.GetRadialZLUT()  # waits for the LUT
+        build_s = time.perf_counter() - t0
+        out["buildlut_256x200_80x80_u16"] = {
+            "workload": "BeginLUT / 200 x BuildLUT(256 ROIs 80x80 u16 from pinned host memory) / FinalizeLUT",
+            "rois_per_s": nbeads * planes / build_s, "seconds": build_s, "lut_shape": list(lut.shape)}
+        flat = d_stack.view(-1, 80, 80)
+        xyz = torch.zeros(nbeads * planes, 3, device=dev)
+        xyz[:, 0] = 40.0
+        xyz[:, 1] = 40.0
+        xyz[:, 2] = torch.arange(planes, device=dev, dtype=torch.float32).repeat_interleave(nbeads)
+        beads = torch.arange(nbeads, device=dev, dtype=torch.int32).repeat(planes)
+        cost = torch.empty(nbeads * planes, device=dev)
+        grad = torch.empty(nbeads * planes, 3, device=dev)
+        glut = torch.zeros(lut.size, device=dev)
+
+        def adjoint():
+            t.lib.QTrkB200ZLUTCostGradient(t.handle, flat.data_ptr(), 160, 12800, abi.QTrkU16, nbeads * planes,
+                                           xyz.data_ptr(), beads.data_ptr(), cost.data_ptr(), grad.data_ptr(),
+                                           glut.data_ptr(), stream.cuda_stream)
+
+        ms = _timed(stream, adjoint, max(3, steps // 10), warmup)
+        out["adjoint_256x200_80x80_u16"] = {"workload": "cost + d/dxyz + d/dLUT of 51,200 ROIs 80x80 u16 (device)",
+                                            "rois_per_s": nbeads * planes / (ms / 1e3), "ms_per_launch": ms}
+        iters = 20
+        hist = np.zeros(iters + 1, np.float32)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        t.lib.QTrkB200RefineZLUT(t.handle, flat.data_ptr(), 160, 12800, abi.QTrkU16, nbeads, planes, None, iters,
+                                 C.c_float(3.0), None, hist.ctypes.data_as(C.c_void_p))
+        ref_s = time.perf_counter() - t0
+        out["lut_refine_256x200"] = {"workload": "QTrkB200RefineZLUT, 20 iterations, smoothness 3, 51,200 ROIs",
+                                     "seconds": ref_s, "seconds_per_iteration": ref_s / iters,
+                                     "objective_first": float(hist[0]), "objective_last": float(hist[-1])}
+        launches += t.KernelLaunchCount() - l0
+    out["gpu_launches"] = int(launches)
+    return out
+
+
 def serving_bench(dev, main_trk, main_rois, seconds: float, fps: float) -> dict:
     """The serving workload (four instances: 40/64/100/128 px, 2000/1000/300/50 beads per frame,
     u8/u16, LUTs of 100-200 planes, Poisson arrivals at `fps` per instance), plus one 100x100 u16
@@ -409,6 +533,7 @@ def main(argv=None) -> int:
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="timed seconds of each paced serving run")
     ap.add_argument("--fps", type=float, default=500.0, help="frame rate per instance in the serving runs")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-workloads", action="store_true", help="skip the Gaussian / BuildLUT / adjoint workloads")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -569,6 +694,9 @@ def main(argv=None) -> int:
     serving = None
     if rank == 0 and ws == 1 and not args.ncu and not args.no_serving:
         serving = serving_bench(dev, trk, wl.rois, args.serve_seconds, args.fps)
+    workloads = None
+    if rank == 0 and ws == 1 and not args.ncu and not args.no_workloads:
+        workloads = workloads_bench(dev, args.steps, args.warmup)
 
     # ---- roofline of the localization kernel ----
     peaks, peak_kind = measured_peaks()
@@ -616,9 +744,11 @@ def main(argv=None) -> int:
                    "parallelism": f"replicas x{ws}"},
         "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu_baseline,
         "gpu_launches": int(launches_value + launches_tc + launches_e2e +
-                            (serving["gpu_launches"] if serving else 0)),
+                            (serving["gpu_launches"] if serving else 0) +
+                            (workloads["gpu_launches"] if workloads else 0)),
         "clocks": clocks, "accuracy": accuracy, "methods": methods, "serving": serving,
         "p99_frame_latency_ms": serving["single_100x100_u16_1000beads"]["p99_ms"] if serving else None,
+        "workloads": workloads,
     }
     trk.Destroy()
     if ws > 1:
