@@ -266,8 +266,11 @@ Tracker::Tracker(const QTrkSettings &settings)
     CheckCuda(cudaHostGetDevicePointer((void **)&d_err_, h_err_, 0), "cudaHostGetDevicePointer");
     CheckCuda(cudaStreamCreateWithFlags(&lut_stream_, cudaStreamNonBlocking), "cudaStreamCreate(lut)");
     CheckCuda(cudaEventCreateWithFlags(&lut_ready_, cudaEventDisableTiming), "cudaEventCreate");
-    for (int b = 0; b < 2; b++)
+    CheckCuda(cudaStreamCreateWithFlags(&lut_copy_stream_, cudaStreamNonBlocking), "cudaStreamCreate(lut copy)");
+    for (int b = 0; b < 2; b++) {
         CheckCuda(cudaEventCreateWithFlags(&lut_stage_free_[b], cudaEventDisableTiming), "cudaEventCreate");
+        CheckCuda(cudaEventCreateWithFlags(&lut_copy_done_[b], cudaEventDisableTiming), "cudaEventCreate");
+    }
     CheckCuda(cudaEventRecord(lut_ready_, lut_stream_), "cudaEventRecord");
     AllocateSlots();
     register_tracker(this);
@@ -309,6 +312,7 @@ Tracker::~Tracker()
         cudaFreeHost(h_lut_stage_[b]);
         cudaFree(d_lut_stage_[b]);
         if (lut_stage_free_[b]) cudaEventDestroy(lut_stage_free_[b]);
+        if (lut_copy_done_[b]) cudaEventDestroy(lut_copy_done_[b]);
     }
     cudaFree(d_qdirs_);
     cudaFree(d_zdirs_);
@@ -327,6 +331,7 @@ Tracker::~Tracker()
     cudaFreeHost(h_err_);
     if (lut_ready_) cudaEventDestroy(lut_ready_);
     if (lut_stream_) cudaStreamDestroy(lut_stream_);
+    if (lut_copy_stream_) cudaStreamDestroy(lut_copy_stream_);
 }
 
 TrackParams Tracker::Params(int pdt) const
@@ -1346,11 +1351,29 @@ void Tracker::BuildLUT(const void *data, int pitch, int pdt, int plane, const ve
     const int b = lut_stage_next_;
     lut_stage_next_ ^= 1;
     CheckCuda(cudaEventSynchronize(lut_stage_free_[b]), "cudaEventSynchronize");
-    std::memcpy(h_lut_stage_[b], data, bytes);
-    if (known_pos) std::memcpy(h_lut_stage_[b] + kp_off, known_pos, sizeof(float2) * nb);
-    CheckCuda(cudaMemcpyAsync(d_lut_stage_[b], h_lut_stage_[b], known_pos ? need : bytes, cudaMemcpyHostToDevice,
-                              lut_stream_),
-              "H2D LUT stack");
+    // A pinned stack is DMA'd straight from the caller's buffer on a copy stream, so that the copy
+    // of this plane overlaps the kernel of the previous one; the call returns once the copy is done
+    // (the caller may reuse the buffer, as after the reference's synchronous BuildLUT). A pageable
+    // stack goes through the pinned staging buffer.
+    const bool pinned = IsPinned(data);
+    if (pinned) {
+        CheckCuda(cudaMemcpyAsync(d_lut_stage_[b], data, bytes, cudaMemcpyHostToDevice, lut_copy_stream_),
+                  "H2D LUT stack");
+        if (known_pos) {
+            std::memcpy(h_lut_stage_[b] + kp_off, known_pos, sizeof(float2) * nb);
+            CheckCuda(cudaMemcpyAsync(d_lut_stage_[b] + kp_off, h_lut_stage_[b] + kp_off, sizeof(float2) * nb,
+                                      cudaMemcpyHostToDevice, lut_copy_stream_),
+                      "H2D known positions");
+        }
+        CheckCuda(cudaEventRecord(lut_copy_done_[b], lut_copy_stream_), "cudaEventRecord");
+        CheckCuda(cudaStreamWaitEvent(lut_stream_, lut_copy_done_[b], 0), "cudaStreamWaitEvent");
+    } else {
+        std::memcpy(h_lut_stage_[b], data, bytes);
+        if (known_pos) std::memcpy(h_lut_stage_[b] + kp_off, known_pos, sizeof(float2) * nb);
+        CheckCuda(cudaMemcpyAsync(d_lut_stage_[b], h_lut_stage_[b], known_pos ? need : bytes, cudaMemcpyHostToDevice,
+                                  lut_stream_),
+                  "H2D LUT stack");
+    }
     TrackParams P = Params(pdt);
     P.mode = 0;  // BuildLUT runs COM/QI/profile without the per-job mode bits
     CheckCuda(launch_build_lut(P, d_lut_stage_[b], pitch, nb, plane,
@@ -1361,6 +1384,7 @@ void Tracker::BuildLUT(const void *data, int pitch, int pdt, int plane, const ve
     CheckCuda(cudaEventRecord(lut_stage_free_[b], lut_stream_), "cudaEventRecord");
     CheckCuda(cudaEventRecord(lut_ready_, lut_stream_), "cudaEventRecord");
     tc_lut_stale_ = true;
+    if (pinned) CheckCuda(cudaEventSynchronize(lut_copy_done_[b]), "cudaEventSynchronize(LUT copy)");
 }
 
 // QueuedCPUTracker::FinalizeLUT, QueuedCPUTracker.cpp:648-659.

@@ -153,6 +153,8 @@ class Tracker : public QueuedTracker {
     uint8_t *d_lut_stage_[2] = {nullptr, nullptr};
     float2 *d_known_[2] = {nullptr, nullptr};
     cudaEvent_t lut_stage_free_[2] = {nullptr, nullptr};
+    cudaStream_t lut_copy_stream_ = nullptr;          // H2D of pinned BuildLUT stacks
+    cudaEvent_t lut_copy_done_[2] = {nullptr, nullptr};
     size_t lut_stage_bytes_ = 0;
     int lut_stage_next_ = 0;
 

@@ -167,3 +167,27 @@ def test_compute_zlut_bias_table_matches_reference(ref, spline, smp):
     assert np.abs(got - want).max() < 0.01, np.abs(got - want).max()
     assert np.array_equal(with_table["pos"], again["pos"])
     assert not np.array_equal(with_table["pos"][:, 2], plain["pos"][:, 2])
+
+
+def test_buildlut_pinned_and_pageable_agree():
+    """BuildLUT from a pinned stack (DMA on the copy stream, overlapping the previous plane's
+    kernel) gives the LUT that the same stack from pageable memory gives; the buffer may be reused
+    as soon as the call returns."""
+    import torch
+
+    s, stack, centres = synth.calib_stack_80x80(nbeads=8, planes=30, seed=15)
+    pinned = torch.empty(stack.shape, dtype=torch.int16).pin_memory().numpy().view(np.uint16)
+    luts = []
+    for src in ("pageable", "pinned"):
+        with QTrkInstance(s) as t:
+            t.SetRadialZLUTSize(8, 30)
+            t.BeginLUT(abi.BUILDLUT_NORMALIZE)
+            for k in range(30):
+                if src == "pinned":
+                    pinned[0] = stack[k]  # one pinned plane buffer, overwritten after every call
+                    t.BuildLUT(pinned[0], k, known_pos=centres if k % 2 else None)
+                else:
+                    t.BuildLUT(stack[k].copy(), k, known_pos=centres if k % 2 else None)
+            t.FinalizeLUT()
+            luts.append(t.GetRadialZLUT())
+    assert np.array_equal(luts[0], luts[1])
