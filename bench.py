@@ -684,6 +684,13 @@ def main(argv=None) -> int:
                "d2h_bytes_per_step": int(N_ROIS * 52),
                "path": "QTrkScheduleFrame(pinned 10000x10000 u16 frame, one LUT copy per bead) + QTrkFlush + "
                        "QTrkFetchResults"}
+        # the host->device copy rate of this box for the same pinned frame (one plain copy): the
+        # e2e path cannot be faster than moving the frame
+        d_frame = torch.empty_like(frame_t, device=dev)
+        copy_ms = _timed(stream, lambda: d_frame.copy_(frame_t, non_blocking=True), 5, 2)
+        e2e["pinned_h2d_copy_gbs"] = frame.nbytes / (copy_ms / 1e3) / 1e9
+        e2e["frame_copy_bound_rois_per_s"] = N_ROIS / (copy_ms / 1e3)
+        del d_frame
         res_e2e = abi.results_to_numpy(buf, N_ROIS)
         res_e2e = res_e2e[np.argsort(res_e2e["zlutIndex"])]
         assert np.array_equal(res_e2e["pos"], res_dev["pos"]), "e2e and device-resident results differ"
