@@ -292,6 +292,20 @@ QTRK_API int QTRK_CALLCONV QTrkB200ZLUTCostGradient(struct QueuedTracker *qtrk, 
                                                     float *d_grad_xyz, float *d_grad_lut, void *stream);
 
 /*
+ * The adjoint of the 2D Gaussian MLE. No counterpart in the reference. For `count` device-resident
+ * ROIs (layout as QTrkB200LocalizeDevice) and device parameters d_params[5i..5i+4] = (x, y, I0, bg,
+ * sigma), the Poisson negative log-likelihood of the integrated-Gaussian spot model the
+ * 5-parameter MLE (LT_B200_Gaussian5P) fits,
+ *   NLL_i = sum_pixels mu - I ln mu,  mu = bg + I0 DX(x, sigma) DY(y, sigma)   (ln I! dropped),
+ * into d_nll[i] and its gradient with respect to the 5 parameters into d_grad[5i..5i+4]. Pixel
+ * calibration images and factors apply as in localization. Asynchronous on `stream`; 0 or < 0.
+ */
+QTRK_API int QTRK_CALLCONV QTrkB200GaussianNLLGradient(struct QueuedTracker *qtrk, const void *d_pixels, int pitch,
+                                                       int64_t roi_stride_bytes, QTRK_PixelDataType_t pdt, int count,
+                                                       const float *d_params, float *d_nll, float *d_grad,
+                                                       void *stream);
+
+/*
  * Z-LUT refinement from a calibration stack. No counterpart in the reference. The device stack
  * holds `planes` x `beads` ROIs, ROI (plane k, bead b) at d_stack + (k * beads + b) * roi_stride_bytes
  * (the order BuildLUT is fed in); the instance's LUT must have `beads` x `planes` rows (typically the

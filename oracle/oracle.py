@@ -218,6 +218,7 @@ class PortOracle:
             "oracle_joint_refine": (None, [_f64p, C.c_int, C.c_int, C.c_double, _f64p, _f32p, C.c_int, C.c_int,
                                            C.c_int, C.c_double, C.c_double, P, C.c_int, C.c_int]),
             "oracle_zlut_bias_correct": (C.c_double, [C.c_double, C.c_int, _f32p, C.c_int, C.c_int, C.c_int]),
+            "oracle_gauss_nll_grad": (C.c_double, [_f64p, C.c_int, C.c_int, _f64p, _f64p]),
             "oracle_find_beads": (C.c_int, [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
                                             C.c_float, P, C.c_int, P]),
         }
@@ -349,6 +350,13 @@ class PortOracle:
         self.lib.oracle_joint_refine(img, img.shape[1], img.shape[0], mean, io, lut, lut.shape[0], lut.shape[1],
                                      angsteps, minr, maxr, _ptr(w), int(normalize), steps)
         return io
+
+    def gauss_nll_grad(self, img, params):
+        """(NLL, gradient (5,)) of the integrated-Gaussian Poisson model at params (x, y, I0, bg, sigma)."""
+        img = np.ascontiguousarray(img, np.float64)
+        p = np.ascontiguousarray(params, np.float64)
+        g = np.zeros(5)
+        return self.lib.oracle_gauss_nll_grad(img, img.shape[1], img.shape[0], p, g), g
 
     def find_beads(self, img, sample_corner, roi, rel_dist, similarity, return_conv=False):
         """QTrkFindBeads restated (FP64 convolution); returns (n, 2) int ROI corners [, conv map]."""

@@ -582,6 +582,32 @@ ORACLE_API void oracle_gauss5(const double *img, int w, int h, const double *ini
 }
 
 /*
+ * Poisson negative log-likelihood of the integrated-Gaussian spot model of the 5-parameter MLE,
+ *   NLL(p) = sum_pixels mu - I ln mu,   mu = bg + I0 DX(x, sigma) DY(y, sigma),
+ * (the ln I! term dropped) with p = {x, y, I0, bg, sigma}, and its gradient
+ *   dNLL/dp = sum (1 - I / mu) dmu/dp.  Returns NLL; grad receives the 5 derivatives.
+ */
+ORACLE_API double oracle_gauss_nll_grad(const double *img, int w, int h, const double *p, double *grad)
+{
+    double nll = 0, g[5] = {0, 0, 0, 0, 0};
+    for (int y = 0; y < h; y++) {
+        double DY, dDy, dDsy;
+        gauss_pixel(y, 0, p[1], 0, p[4], &DY, &dDy, &dDsy, 1);
+        for (int x = 0; x < w; x++) {
+            double DX, dDx, dDsx;
+            gauss_pixel(x, 0, p[0], 0, p[4], &DX, &dDx, &dDsx, 0);
+            double mu = p[3] + p[2] * DX * DY;
+            double j[5] = {p[2] * dDx * DY, p[2] * DX * dDy, DX * DY, 1.0, p[2] * (dDsx * DY + DX * dDsy)};
+            double I = img[y * w + x];
+            nll += mu - I * log(mu);
+            for (int a = 0; a < 5; a++) g[a] += (1.0 - I / mu) * j[a];
+        }
+    }
+    for (int a = 0; a < 5; a++) grad[a] = g[a];
+    return nll;
+}
+
+/*
  * Radial-profile-to-LUT cost and its analytic gradient (the adjoint of the GPU library).
  * p(x, y) is the radial profile of utils.cpp:275-320 at (x, y): per bin the mean of the
  * in-bounds bilinear samples over `angsteps` directions, or `mean` when at most 4 samples are

@@ -355,6 +355,65 @@ __global__ void __launch_bounds__(kAdjThreads) joint_refine_kernel(TrackParams P
     }
 }
 
+// Gaussian-MLE adjoint: Poisson NLL = sum mu - I ln mu of the 5-parameter integrated-Gaussian
+// model (the model gauss5_mle fits, erff per column/row, FP32 per pixel, FP64 sums) and its
+// gradient sum (1 - I/mu) dmu/dp for p = (x, y, I0, bg, sigma) = params[5 roi ..]. One block per ROI.
+__global__ void __launch_bounds__(kAdjThreads) gauss_nll_grad_kernel(TrackParams P, const uint8_t *__restrict__ pixels,
+                                                                     int pitch, int64_t roi_stride, int count,
+                                                                     const float *__restrict__ params,
+                                                                     float *__restrict__ nll, float *__restrict__ grad)
+{
+    extern __shared__ __align__(16) uint8_t smem[];
+    const int roi = blockIdx.x;
+    if (roi >= count) return;
+    const int W = P.width, H = P.height;
+    float *img = reinterpret_cast<float *>(smem);
+    float *col = img + ((W * H + 3) & ~3);
+    float *row = col + 3 * W;
+    double *red = reinterpret_cast<double *>(smem + (((size_t)((W * H + 3) & ~3) + 3 * (W + H)) * 4 + 15) / 16 * 16);
+    BlockGroup g{red};
+    load_roi(g, img, pixels + (int64_t)roi * roi_stride, pitch, P, 0);
+    float p[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) p[k] = params[5 * roi + k];
+    const float s = p[4];
+    const float k1 = 1.0f / (sqrtf(2.0f) * s);
+    const float k2 = 1.0f / (sqrtf(2 * 3.14159265359f) * s);
+    for (int c = threadIdx.x; c < W + H; c += blockDim.x) {
+        const bool is_col = c < W;
+        const int cc = is_col ? c : c - W;
+        const float pc = is_col ? p[0] : p[1];
+        const float a0 = (cc - pc + .5f) * k1, a1 = (cc - pc - .5f) * k1;
+        const float e0 = expf(-a0 * a0), e1 = expf(-a1 * a1);
+        float *t = is_col ? col + 3 * cc : row + 3 * cc;
+        t[0] = 0.5f * (erff(a0) - erff(a1));
+        t[1] = (e1 - e0) * k2;
+        t[2] = ((cc - pc - .5f) * e1 - (cc - pc + .5f) * e0) * k2 / s;
+    }
+    __syncthreads();
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < W * H; i += blockDim.x) {
+        const int y = i / W, x = i - y * W;
+        const float DX = col[3 * x], dX = col[3 * x + 1], sX = col[3 * x + 2];
+        const float DY = row[3 * y], dY = row[3 * y + 1], sY = row[3 * y + 2];
+        const float mu = p[3] + p[2] * DX * DY;
+        const float I = img[i];
+        const float f = 1.0f - I / mu;
+        acc[0] += (double)(mu - I * logf(mu));
+        acc[1] += (double)(f * p[2] * dX * DY);
+        acc[2] += (double)(f * p[2] * DX * dY);
+        acc[3] += (double)(f * DX * DY);
+        acc[4] += (double)f;
+        acc[5] += (double)(f * p[2] * (sX * DY + DX * sY));
+    }
+    g.sum(acc);
+    if (threadIdx.x == 0) {
+        nll[roi] = (float)acc[0];
+#pragma unroll
+        for (int k = 0; k < 5; k++) grad[5 * roi + k] = (float)acc[1 + k];
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_zcost_grad(const TrackParams &P, const uint8_t *pixels, int pitch, int64_t roi_stride, int count,
@@ -367,6 +426,18 @@ cudaError_t launch_zcost_grad(const TrackParams &P, const uint8_t *pixels, int p
     if (e != cudaSuccess) return e;
     zcost_grad_kernel<<<count, kAdjThreads, smem, stream>>>(P, pixels, pitch, roi_stride, count, xyz, beads, cost, grad,
                                                             glut);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gauss_nll_grad(const TrackParams &P, const uint8_t *pixels, int pitch, int64_t roi_stride, int count,
+                                  const float *params, float *nll, float *grad, cudaStream_t stream)
+{
+    if (count <= 0) return cudaSuccess;
+    const int W = P.width, H = P.height;
+    const int smem = (int)((((size_t)((W * H + 3) & ~3) + 3 * (W + H)) * 4 + 15) / 16 * 16) + 6 * 32 * 8;
+    cudaError_t e = cudaFuncSetAttribute(gauss_nll_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    gauss_nll_grad_kernel<<<count, kAdjThreads, smem, stream>>>(P, pixels, pitch, roi_stride, count, params, nll, grad);
     return cudaGetLastError();
 }
 

@@ -576,6 +576,17 @@ QTRK_API void QTRK_CALLCONV QTrkB200RefineZLUT(QueuedTracker *q, const void *d_s
     });
 }
 
+QTRK_API int QTRK_CALLCONV QTrkB200GaussianNLLGradient(QueuedTracker *q, const void *d_pixels, int pitch,
+                                                       int64_t roi_stride_bytes, QTRK_PixelDataType_t pdt, int count,
+                                                       const float *d_params, float *d_nll, float *d_grad,
+                                                       void *stream)
+{
+    return guarded_ret<int>(q, "QTrkB200GaussianNLLGradient", -100, [&](Tracker *t) {
+        return t->GaussianNLLGradient(d_pixels, pitch, roi_stride_bytes, pdt, count, d_params, d_nll, d_grad,
+                                      static_cast<cudaStream_t>(stream));
+    });
+}
+
 QTRK_API int QTRK_CALLCONV QTrkB200LocalizeDevice(QueuedTracker *q, const void *d_pixels, int pitch,
                                                   int64_t roi_stride_bytes, QTRK_PixelDataType_t pdt, int count,
                                                   const LocalizationJob *d_jobs, LocalizationResult *d_results,

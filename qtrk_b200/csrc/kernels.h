@@ -40,6 +40,11 @@ cudaError_t launch_zcost_grad(const TrackParams &P, const uint8_t *pixels, int p
                               const float *xyz, const int *beads, float *cost, float *grad, float *glut,
                               cudaStream_t stream);
 
+// Poisson NLL of the 5-parameter integrated-Gaussian model at params[5i..5i+4] = (x, y, I0, bg,
+// sigma) and its gradient, for `count` ROIs at pixels + i*roi_stride. One kernel launch.
+cudaError_t launch_gauss_nll_grad(const TrackParams &P, const uint8_t *pixels, int pitch, int64_t roi_stride, int count,
+                                  const float *params, float *nll, float *grad, cudaStream_t stream);
+
 // Joint Gauss-Newton (x, y, z) refinement of localized ROIs, in place on results (same ROI
 // addressing as launch_localize). One kernel launch.
 cudaError_t launch_joint_refine(const TrackParams &P, const uint8_t *pixels, int pitch, int64_t roi_stride,

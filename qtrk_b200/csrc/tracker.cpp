@@ -599,6 +599,31 @@ void Tracker::RefineZLUT(const void *d_stack, int pitch, int64_t roi_stride, int
         for (int k = 0; k < planes; k++) plane_z[k] = (float)(k + d[k]);
 }
 
+// The adjoint of the 5-parameter Gaussian MLE (see adjoint.cu), on the caller's stream.
+int Tracker::GaussianNLLGradient(const void *d_pixels, int pitch, int64_t roi_stride, int pdt, int count,
+                                 const float *d_params, float *d_nll, float *d_grad, cudaStream_t stream)
+{
+    if (!d_pixels || !d_params || !d_nll || !d_grad || count < 0 || pdt < 0 || pdt > 2) {
+        Warn("QTrkB200GaussianNLLGradient: invalid argument");
+        return -1;
+    }
+    if (pitch < cfg.base.width * pdt_bytes(pdt)) {
+        Warn("QTrkB200GaussianNLLGradient: pitch smaller than a row");
+        return -2;
+    }
+    DeviceGuard dg(device_);
+    TrackParams P;
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        P = Params(pdt);
+    }
+    CheckCuda(launch_gauss_nll_grad(P, static_cast<const uint8_t *>(d_pixels), pitch, roi_stride, count, d_params,
+                                    d_nll, d_grad, stream),
+              "Gaussian NLL gradient launch");
+    launches_++;
+    return 0;
+}
+
 // LT_B200_JointRefine: a joint Gauss-Newton pass follows the Z fit when the mode has one.
 bool Tracker::RefineAfterZ(const TrackParams &P)
 {

@@ -82,6 +82,8 @@ class Tracker : public QueuedTracker {
                               void *scratch, size_t scratch_bytes);
     void RefineZLUT(const void *d_stack, int pitch, int64_t roi_stride, int pdt, int beads, int planes, const float *d_xy,
                     int iterations, float smoothness, float *plane_z, float *cost_history);
+    int GaussianNLLGradient(const void *d_pixels, int pitch, int64_t roi_stride, int pdt, int count,
+                            const float *d_params, float *d_nll, float *d_grad, cudaStream_t stream);
     int ZLUTCostGradient(const void *d_pixels, int pitch, int64_t roi_stride, int pdt, int count, const float *d_xyz,
                          const int *d_beads, float *d_cost, float *d_grad, float *d_glut, cudaStream_t stream);
     int64_t LaunchCount() const { return launches_.load(); }

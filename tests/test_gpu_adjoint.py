@@ -223,3 +223,40 @@ def test_joint_refine_accuracy_vs_plain_fit():
     exy_ref = np.median(np.hypot(*(refined["pos"][ok, :2] - truth[ok, :2]).T))
     print(f"median |dz| plain {ez_plain:.4f} refined {ez_ref:.4f}; |dxy| plain {exy_plain:.4f} refined {exy_ref:.4f}")
     assert ez_ref <= 1.05 * ez_plain and exy_ref <= 1.2 * exy_plain
+
+
+def test_gaussian_nll_gradient_matches_oracle_and_differences(port):
+    """QTrkB200GaussianNLLGradient against the FP64 oracle (oracle_gauss_nll_grad) and central
+    differences of its own NLL."""
+    torch = _torch()
+    wl = synth.gauss16_f32(64, seed=91)
+    rng = np.random.default_rng(4)
+    params = np.stack([wl.true_xyz[:, 0] + rng.uniform(-0.3, 0.3, 64), wl.true_xyz[:, 1] + rng.uniform(-0.3, 0.3, 64),
+                       wl.extra["photons"] * rng.uniform(0.8, 1.2, 64), np.full(64, 10.0) * rng.uniform(0.8, 1.2, 64),
+                       rng.uniform(1.3, 1.7, 64)], 1).astype(np.float32)
+    d = _device_rois(wl.rois)
+
+    def run(p):
+        dp = torch.as_tensor(np.ascontiguousarray(p, np.float32)).cuda()
+        nll = torch.empty(len(p), device="cuda")
+        grad = torch.empty(len(p), 5, device="cuda")
+        rc = t.lib.QTrkB200GaussianNLLGradient(t.handle, d.data_ptr(), 64, 1024, abi.QTrkFloat, len(p), dp.data_ptr(),
+                                               nll.data_ptr(), grad.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        assert rc == 0
+        torch.cuda.synchronize()
+        return nll.cpu().numpy().astype(np.float64), grad.cpu().numpy().astype(np.float64)
+
+    with QTrkInstance(wl.settings) as t:
+        nll, grad = run(params)
+        want = [port.gauss_nll_grad(img.astype(np.float64), params[i].astype(np.float64)) for i, img in enumerate(wl.rois)]
+        want_n = np.array([w[0] for w in want])
+        want_g = np.array([w[1] for w in want])
+        np.testing.assert_allclose(nll, want_n, rtol=2e-5, atol=1e-2)
+        scale = np.abs(want_g).max(1, keepdims=True)
+        assert (np.abs(grad - want_g) <= 2e-3 * scale + 1e-3).all(), np.abs(grad - want_g).max()
+        for k, h in enumerate((1e-3, 1e-3, 1.0, 0.05, 1e-3)):
+            e = np.zeros(5, np.float32)
+            e[k] = h
+            fd = (run(params + e)[0] - run(params - e)[0]) / (2 * h)
+            tol = 0.02 * np.abs(grad[:, k]) + 0.01 * np.abs(grad).max(1) * (1 if k != 2 else 0.01) + 0.05
+            assert (np.abs(fd - grad[:, k]) <= tol).mean() >= 0.9, (k, np.abs(fd - grad[:, k]).max())
