@@ -723,6 +723,24 @@ def main(argv=None) -> int:
                 "median_z_err_planes_vs_truth": float(np.median(np.abs(res_dev["pos"][:, 2] - wl.true_xyz[:, 2]))),
                 "pixel_nm": PIXEL_NM}
 
+    # ---- error against the FP64 restatement of the algorithm, same LUT (rank 0) ----
+    if rank == 0 and not args.ncu:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        from oracle import PortOracle, port_available
+
+        if port_available():
+            port = PortOracle()
+            m = min(2000, N_ROIS)
+            fp64 = port.localize(port.computed_config(wl.settings), wl.mode, wl.rois[:m], lut)
+            d = res_dev[:m]
+            conv = np.hypot(fp64[:, 0] - fp64[:, 3], fp64[:, 1] - fp64[:, 4]) <= 5  # QI kept the bead
+            dxy = np.abs(d["pos"][:, :2] - fp64[:, :2]).max(1) * PIXEL_NM
+            dz = np.abs(d["pos"][:, 2] - fp64[:, 2])
+            accuracy["vs_fp64_oracle"] = {
+                "rois": m, "max_dxy_nm": float(dxy[conv].max()), "p99_dxy_nm": float(np.percentile(dxy[conv], 99)),
+                "max_dz_planes": float(dz[conv].max()), "p99_dz_planes": float(np.percentile(dz[conv], 99)),
+                "rois_where_qi_lost_the_bead": int((~conv).sum())}
+
     # ---- CPU baseline: the reference tracker on the host cores (rank 0, N=1) ----
     cpu_baseline = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and not args.ncu:
