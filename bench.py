@@ -476,6 +476,65 @@ def serving_bench(dev, main_trk, main_rois, seconds: float, fps: float) -> dict:
     return out
 
 
+def profile_workload(args) -> int:
+    """Small device workloads for ncu captures (a few launches, a few hundred MB at most):
+    tensorcore  2,048 ROIs 100x100 u16, COM + QI + Z with the tcgen05 Z match (LUT 200 x 64);
+    gauss5      100,000 ROIs 16x16 f32, 5-parameter Gaussian MLE;
+    adjoint     2,048 ROIs 100x100 u16, QTrkB200ZLUTCostGradient with the LUT gradient;
+    beadconv    QTrkFindBeads on a 2048 x 2048 frame with a 100 px sample."""
+    import torch
+
+    from qtrk_b200 import abi, synth
+    from qtrk_b200.tracker import QTrkInstance, load_library
+
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    total = args.warmup + args.steps
+    if args.profile_workload in ("tensorcore", "adjoint"):
+        n = 2048
+        wl = make_workload(n, seed=2)
+        lut = build_lut_on_gpu(wl)
+        d = torch.from_numpy(wl.rois.view(np.int16)).to(dev)
+        with QTrkInstance(wl.settings) as t:
+            t.SetRadialZLUT(lut)
+            if args.profile_workload == "tensorcore":
+                t.SetLocalizationMode(wl.mode | abi.LT_B200_ZMatchBF16)
+                res = torch.empty(n * 52, dtype=torch.uint8, device=dev)
+                f = lambda: t.LocalizeDevice(d.data_ptr(), 200, 20000, abi.QTrkU16, n, res.data_ptr(),
+                                             stream=stream.cuda_stream)
+            else:
+                t.SetLocalizationMode(wl.mode)
+                xyz = torch.from_numpy(wl.true_xyz.astype(np.float32)).to(dev)
+                cost, grad = torch.empty(n, device=dev), torch.empty(n, 3, device=dev)
+                glut = torch.zeros(lut.size, device=dev)
+                f = lambda: t.lib.QTrkB200ZLUTCostGradient(t.handle, d.data_ptr(), 200, 20000, abi.QTrkU16, n,
+                                                           xyz.data_ptr(), None, cost.data_ptr(), grad.data_ptr(),
+                                                           glut.data_ptr(), stream.cuda_stream)
+            ms = _timed(stream, f, args.steps, args.warmup)
+    elif args.profile_workload == "gauss5":
+        n = 100000
+        wl = synth.gauss16_f32(n, seed=3)
+        d = torch.from_numpy(wl.rois).to(dev)
+        res = torch.empty(n * 52, dtype=torch.uint8, device=dev)
+        with QTrkInstance(wl.settings) as t:
+            t.SetLocalizationMode(abi.LT_Gaussian2D | abi.LT_B200_Gaussian5P)
+            ms = _timed(stream, lambda: t.LocalizeDevice(d.data_ptr(), 64, 1024, abi.QTrkFloat, n, res.data_ptr(),
+                                                         stream=stream.cuda_stream), args.steps, args.warmup)
+    else:
+        lib = load_library()
+        frame, centres = synth.bead_frame(2048, 2048, 120, 100, seed=9, noise=2.0)
+        img = abi.ImageData(frame.ctypes.data_as(C.POINTER(C.c_float)), 2048, 2048)
+        corner = (int(centres[0][0] - 50), int(centres[0][1] - 50))
+        t0 = time.perf_counter()
+        for _ in range(total):
+            cnt = C.c_int()
+            p = lib.QTrkFindBeads(C.byref(img), corner[0], corner[1], 100, 1.0, 0.5, C.byref(cnt), None)
+            lib.QTrkFreeROIPositions(p)
+        ms = (time.perf_counter() - t0) * 1e3 / total
+    print(json.dumps({"profile_workload": args.profile_workload, "ms_per_call": ms, "launches": total}), flush=True)
+    return 0
+
+
 def run_reference_arm(args) -> int:
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -534,10 +593,14 @@ def main(argv=None) -> int:
     ap.add_argument("--fps", type=float, default=500.0, help="frame rate per instance in the serving runs")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-workloads", action="store_true", help="skip the Gaussian / BuildLUT / adjoint workloads")
+    ap.add_argument("--profile-workload", choices=["tensorcore", "gauss5", "adjoint", "beadconv"],
+                    help="run one small device workload --steps times for a profiler and exit")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.profile_workload:
+        return profile_workload(args)
 
     import torch
 
