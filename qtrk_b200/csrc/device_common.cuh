@@ -763,26 +763,29 @@ __device__ inline void gauss4_mle(const G &g, const float *img, int W, int H, fl
 }
 
 // Solve the symmetric 5x5 system A d = b (Gaussian elimination, partial pivoting, FP64).
+// Gaussian elimination with partial pivoting. The pivot row is found by swapping, row by row, any
+// row whose entry is larger in magnitude into the pivot position: every index is a compile-time
+// constant after unrolling, so the matrix stays in registers (a dynamically indexed row swap
+// would put it in local memory). The pivot chosen and every operation on a row are those of
+// the classic search-then-swap form.
 __device__ __forceinline__ bool solve5(double (&A)[5][5], double (&b)[5], double (&d)[5])
 {
 #pragma unroll
     for (int c = 0; c < 5; c++) {
-        int piv = c;
 #pragma unroll
-        for (int r = c + 1; r < 5; r++)
-            if (fabs(A[r][c]) > fabs(A[piv][c])) piv = r;
-        if (!(fabs(A[piv][c]) > 1e-300)) return false;
-        if (piv != c) {
+        for (int r = c + 1; r < 5; r++) {
+            const bool sw = fabs(A[r][c]) > fabs(A[c][c]);
 #pragma unroll
             for (int j = 0; j < 5; j++) {
                 const double t = A[c][j];
-                A[c][j] = A[piv][j];
-                A[piv][j] = t;
+                A[c][j] = sw ? A[r][j] : t;
+                A[r][j] = sw ? t : A[r][j];
             }
             const double t = b[c];
-            b[c] = b[piv];
-            b[piv] = t;
+            b[c] = sw ? b[r] : t;
+            b[r] = sw ? t : b[r];
         }
+        if (!(fabs(A[c][c]) > 1e-300)) return false;
 #pragma unroll
         for (int r = c + 1; r < 5; r++) {
             const double f = A[r][c] / A[c][c];
