@@ -48,6 +48,14 @@ BYTES_PER_ROI = 100 * 100 * 2 + 52 + 24 + (200 * 64 * 4) / N_ROIS  # algorithmic
 PIXEL_NM = 100.0  # stated pixel size for nm error reporting
 
 
+def workload_config(ws: int) -> dict:
+    """The `config` of the bench line, the same for this library's arm and the reference arm."""
+    return {"workload": "10,000 ROIs/step of 100x100 u16; COM + QI (4 it, 64 radial x 51 angular per quadrant) + "
+                        "Z-LUT 200 planes x 64 bins (206 angles); Z match form = methods.chosen",
+            "rois_per_step": N_ROIS, "lut_planes": 200, "l2": "inputs larger than L2 (200 MB per step)",
+            "parallelism": f"replicas x{ws}"}
+
+
 def dist_env():
     from qtrk_b200 import replicas
 
@@ -568,8 +576,7 @@ def run_reference_arm(args) -> int:
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * args.sample / value, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "100x100 u16 ROIs, COM + QI(4 it, 64x51/quadrant) + Z-LUT 200x64 (206 angles)",
-                   "rois_per_step": args.sample},
+        "config": workload_config(ws),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                          "sample": f"{args.sample} ROIs per step of the same seeded workload, QueuedCPUTracker "
                                    f"with numThreads=-1"},
@@ -826,10 +833,7 @@ def main(argv=None) -> int:
         "metric": METRIC, "value": methods[chosen]["rois_per_s"], "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": methods[chosen]["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded Poisson bead images, 100x100 u16 bead ROIs)",
-        "config": {"workload": "10,000 ROIs/step of 100x100 u16; COM + QI (4 it, 64 radial x 51 angular "
-                               "per quadrant) + Z-LUT 200 planes x 64 bins (206 angles); Z match form = methods.chosen",
-                   "rois_per_step": N_ROIS, "lut_planes": 200, "l2": "inputs larger than L2 (200 MB per step)",
-                   "parallelism": f"replicas x{ws}"},
+        "config": workload_config(ws),
         "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu_baseline,
         "gpu_launches": int(launches_value + launches_tc + launches_e2e +
                             (serving["gpu_launches"] if serving else 0) +
