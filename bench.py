@@ -48,6 +48,28 @@ BYTES_PER_ROI = 100 * 100 * 2 + 52 + 24 + (200 * 64 * 4) / N_ROIS  # algorithmic
 PIXEL_NM = 100.0  # stated pixel size for nm error reporting
 
 
+_STDOUT_FD = None
+
+
+def claim_stdout() -> None:
+    """Send everything the process writes to stdout (the reference's C++ tracker prints its thread
+    count there) to stderr, keeping the original stdout for the one bench line."""
+    global _STDOUT_FD
+    if _STDOUT_FD is None:
+        sys.stdout.flush()
+        _STDOUT_FD = os.dup(1)
+        os.dup2(2, 1)
+
+
+def emit(line: dict) -> None:
+    data = (json.dumps(line) + "\n").encode()
+    if _STDOUT_FD is None:
+        sys.stdout.write(data.decode())
+        sys.stdout.flush()
+    else:
+        os.write(_STDOUT_FD, data)
+
+
 def workload_config(ws: int) -> dict:
     """The `config` of the bench line, the same for this library's arm and the reference arm."""
     return {"workload": "10,000 ROIs/step of 100x100 u16; COM + QI (4 it, 64 radial x 51 angular per quadrant) + "
@@ -539,7 +561,7 @@ def profile_workload(args) -> int:
             p = lib.QTrkFindBeads(C.byref(img), corner[0], corner[1], 100, 1.0, 0.5, C.byref(cnt), None)
             lib.QTrkFreeROIPositions(p)
         ms = (time.perf_counter() - t0) * 1e3 / total
-    print(json.dumps({"profile_workload": args.profile_workload, "ms_per_call": ms, "launches": total}), flush=True)
+    emit({"profile_workload": args.profile_workload, "ms_per_call": ms, "launches": total})
     return 0
 
 
@@ -582,7 +604,7 @@ def run_reference_arm(args) -> int:
                                    f"with numThreads=-1"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line), flush=True)
+    emit(line)
     return 0
 
 
@@ -604,6 +626,7 @@ def main(argv=None) -> int:
                     help="run one small device workload --steps times for a profiler and exit")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
+    claim_stdout()
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.profile_workload:
@@ -846,7 +869,7 @@ def main(argv=None) -> int:
     if ws > 1:
         replicas.finalize()
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        emit(line)
     return 0
 
 
