@@ -1004,7 +1004,11 @@ int Tracker::ScheduleFrame(const void *img, int pitch, int width, int height, co
     if (skipped) Warn("ScheduleFrame: skipped " + std::to_string(skipped) + " ROI(s) outside the frame");
     if (idx.empty()) return 0;
 
-    // Group ROIs into row bands that fit a slot; one band keeps the caller's order.
+    // Group ROIs into row bands of at most 16 MiB (or one slot, if smaller); one band keeps the
+    // caller's order. The bands' copies run one after another (each waits for the previous one),
+    // so every band's kernel overlaps the next band's copy and only the last, small band's kernel
+    // is left after the frame has crossed PCIe.
+    const size_t band_cap = std::min(slot_bytes_, (size_t)16 << 20);
     int minx = width, maxx = 0;
     for (int i : idx) {
         minx = std::min(minx, pos[i].x);
@@ -1019,7 +1023,7 @@ int Tracker::ScheduleFrame(const void *img, int pitch, int width, int height, co
             y0 = std::min(y0, pos[i].y);
             y1 = std::max(y1, pos[i].y + H);
         }
-        if (span_bytes(y0, y1) <= slot_bytes_ && (int)idx.size() <= batch_) {
+        if (span_bytes(y0, y1) <= band_cap && (int)idx.size() <= batch_) {
             bands.push_back(idx);
         } else {
             std::vector<int> sorted = idx;
@@ -1034,7 +1038,7 @@ int Tracker::ScheduleFrame(const void *img, int pitch, int width, int height, co
                     continue;
                 }
                 const int ny1 = std::max(by1, pos[i].y + H);
-                if (span_bytes(by0, ny1) <= slot_bytes_ && (int)cur.size() < batch_) {
+                if (span_bytes(by0, ny1) <= band_cap && (int)cur.size() < batch_) {
                     by1 = ny1;
                     cur.push_back(i);
                 } else {
@@ -1061,7 +1065,7 @@ int Tracker::ScheduleFrame(const void *img, int pitch, int width, int height, co
     }
 
     const bool pinned = IsPinned(img);
-    std::vector<cudaEvent_t> copies;
+    std::vector<cudaEvent_t> copies;  // one per band, in order: the copy chain
     std::unique_lock<std::mutex> lk(mu_);
     if (filling_ >= 0) {  // keep FIFO order with earlier single-ROI jobs
         if (slots_[filling_].count > 0)
@@ -1094,16 +1098,15 @@ int Tracker::ScheduleFrame(const void *img, int pitch, int width, int height, co
             s.h_jobs[k].zlutIndex = i + job->zlutIndex;
         }
         CheckCuda(cudaEventRecord(s.ev_start, s.stream), "cudaEventRecord");
+        if (!copies.empty()) CheckCuda(cudaStreamWaitEvent(s.stream, copies.back(), 0), "cudaStreamWaitEvent");
         const uint8_t *src = static_cast<const uint8_t *>(img) + (size_t)y0 * pitch + (size_t)minx * bpp;
         CheckCuda(cudaMemcpy2DAsync(s.d_pix, dpitch, src, (size_t)pitch, (size_t)(maxx - minx) * bpp, (size_t)(y1 - y0),
                                     cudaMemcpyHostToDevice, s.stream),
                   "H2D frame rows");
-        if (pinned) {
-            cudaEvent_t ev;
-            CheckCuda(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
-            CheckCuda(cudaEventRecord(ev, s.stream), "cudaEventRecord");
-            copies.push_back(ev);
-        }
+        cudaEvent_t ev;
+        CheckCuda(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+        CheckCuda(cudaEventRecord(ev, s.stream), "cudaEventRecord");
+        copies.push_back(ev);
         SubmitLocked(si);
         count += s.count;
     }
@@ -1111,8 +1114,8 @@ int Tracker::ScheduleFrame(const void *img, int pitch, int width, int height, co
     // A pinned source is read by DMA after cudaMemcpy2DAsync returns: wait until it has been
     // read so the caller may reuse the frame buffer (pageable sources are staged before return).
     for (cudaEvent_t ev : copies) {
-        cudaEventSynchronize(ev);
-        cudaEventDestroy(ev);
+        if (pinned) cudaEventSynchronize(ev);
+        cudaEventDestroy(ev);  // a pending event is released once it completes
     }
     return count;
 }
