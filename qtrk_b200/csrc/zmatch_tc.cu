@@ -16,8 +16,10 @@
 // + O(2^-16 x)) and the cross term is p_hi.L_hi + p_hi.L_lo + p_lo.L_hi (three MMAs per K
 // slice, all accumulated in the same FP32 tensor-memory tile), which brings the error bound
 // down to d_k = 2^-9 |p'| |L'_k| (a generous cover of the ~3 2^-16 split error plus the FP32
-// accumulation of 3 K products), so only a few planes per ROI need the exact re-score. The 7-point fit (LsqQuadraticFit.h:132-176) then runs on exact scores,
-// so z equals the plain path's up to the summation order of the exact scores.
+// accumulation of 3 K products), so only a few planes per ROI need the exact re-score. Threads
+// record those candidate planes from their TMEM rows; warps then compute the exact scores with
+// the plain path's lane mapping and reduction order, take the argmax and run the 7-point fit
+// (LsqQuadraticFit.h:132-176) with the plain path's warp code, so z is the plain path's bit for bit.
 //
 // Launch: one CTA of 128 threads per tile. Shared memory is sized so that at most two CTAs
 // share an SM, so the two 256-column TMEM allocations always fit the SM's 512 columns and
@@ -40,6 +42,13 @@ constexpr int kMaxN = 256;   // N per tcgen05.mma (M = 128 allows N <= 256 in st
 constexpr float kBoundScale = 0.001953125f;  // 2^-9 (see above)
 constexpr int kTmemCols = 256;
 constexpr uint32_t kWaitLimit = 1u << 20;  // try_wait polls before the kernel gives up
+constexpr int kMaxCand = 16;  // candidate planes kept per ROI; more fall back to scoring every plane
+constexpr int kWarps = kTileM / 32;
+
+// Bytes after the A/B tiles: mbarrier (8) + TMEM slot (8), then |p'| per row (kTileM floats),
+// candidate counts (kTileM ints), candidate planes (kTileM x kMaxCand shorts) and one 8-double
+// score window per warp.
+constexpr int kTailBytes = 16 + kTileM * 4 + kTileM * 4 + kTileM * kMaxCand * 2 + kWarps * 8 * 8;
 
 __device__ const float kZLUTWeightsTC[7] = {0.15f, 0.5f, 0.85f, 1.0f, 0.85f, 0.5f, 0.15f};
 
@@ -118,14 +127,20 @@ __device__ __forceinline__ void store_chunk(uint8_t *base, int r, int c, int sbo
     *reinterpret_cast<uint4 *>(base + (r >> 3) * sbo + c * 128 + (r & 7) * 16) = v;
 }
 
-__device__ double exact_score(const float *prof, const float *lutrow, const float *w, int nb)
+// Exact score of one plane by one warp, in the plain path's order (zlut_scores_plain: lanes over
+// bins r = lane + 32 j, FP32 difference, FP64 square sums, xor-shuffle reduction): the tensor-core
+// path's scores, and so its argmax and fit, are the plain path's bit for bit. Every lane returns it.
+__device__ double warp_exact_score(const float *prof, const float *lutrow, const float *w, int nb)
 {
+    const int lane = threadIdx.x & 31;
     double acc = 0.0;
-    for (int r = 0; r < nb; r++) {
-        double d = (double)(prof[r] - lutrow[r]);
-        if (w) d *= (double)w[r];
+    for (int r = lane; r < nb; r += 32) {
+        double d = (double)(prof[r] - __ldg(lutrow + r));
+        if (w) d *= (double)__ldg(w + r);
         acc += d * d;
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     return -acc;
 }
 
@@ -147,6 +162,10 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
     uint8_t *sBl = sB + kMaxN * nbp * 2;
     uint64_t *mbar = reinterpret_cast<uint64_t *>(sBl + kMaxN * nbp * 2);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
+    float *s_pnorm = reinterpret_cast<float *>(mbar + 2);
+    int *s_ncand = reinterpret_cast<int *>(s_pnorm + kTileM);
+    short *s_cand = reinterpret_cast<short *>(s_ncand + kTileM);
+    double *s_win = reinterpret_cast<double *>(s_cand + kTileM * kMaxCand);
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
@@ -176,25 +195,31 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
         store_chunk(sAl, r, c, sbo, vl);
     }
 
-    // |p'| of this thread's ROI (FP32 profile times the radial weights)
+    // |p'| of each row's ROI (FP32 profile times the radial weights), one warp per row, lanes over
+    // bins; FP64 sums rounded up by 2^-20 so that the bound below stays a bound
     const int nb = Q.nb;
     const float *prof = (my_roi >= 0) ? Q.prof_f32 + (size_t)my_roi * nb : nullptr;
-    float pnorm = 0.0f;
-    if (prof) {
-        float s2 = 0.0f;
-        for (int r = 0; r < nb; r++) {
-            const float v = Q.weights ? prof[r] * Q.weights[r] : prof[r];
-            s2 += v * v;
+    for (int r = warp; r < kTileM; r += kWarps) {
+        double s2 = 0.0;
+        if (r < m) {
+            const int roi = Q.perm ? Q.perm[start + r] : start + r;
+            const float *pr = Q.prof_f32 + (size_t)roi * nb;
+            for (int b = tid & 31; b < nb; b += 32) {
+                const double v = Q.weights ? (double)pr[b] * Q.weights[b] : (double)pr[b];
+                s2 += v * v;
+            }
         }
-        pnorm = sqrtf(s2);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+        if ((tid & 31) == 0) s_pnorm[r] = (float)(sqrt(s2) * (1.0 + 0x1p-20));
     }
+    float pnorm = 0.0f;  // read after the first barrier of the chunk loop
+    int nc = 0;          // candidate planes of this thread's row (may exceed kMaxCand)
     const int gb = valid_bead ? bead : 0;
     const float *lut = Q.lut + (size_t)gb * Q.planes * nb;
     const float *lnorm = Q.lut_norm + (size_t)gb * Q.planes_pad;
 
     float smax = -INFINITY, dmax = 0.0f;  // BF16 maximum so far and its error bound
-    double best_e = -INFINITY;            // best exact score among the candidates
-    int best_k = -1;
     bool failed = false;
     uint32_t parity = 0;
     const int planes_pad = Q.planes_pad;
@@ -210,6 +235,7 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
+        pnorm = s_pnorm[tid];
         const uint32_t tmem = *tslot;
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -255,9 +281,9 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
                 }
             }
         }
-        // pass 2: exact re-score of every plane that can still be the best. The TMEM load is
-        // warp-collective (.sync.aligned), so every lane executes it; lanes without a ROI
-        // just skip the scoring.
+        // pass 2: record every plane that can still be the best (its exact score is computed by
+        // the warps afterwards). The TMEM load is warp-collective (.sync.aligned), so every lane
+        // executes it; lanes without a ROI record nothing.
         for (int c0 = 0; c0 < n; c0 += 16) {
             float v[16];
             tmem_ld16(trow + (uint32_t)c0, v);
@@ -270,11 +296,8 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
                     const float dk = kBoundScale * pnorm * sqrtf(lnorm[k]);
                     const float thr = smax - dmax - dk - 1e-5f * (1.0f + fabsf(smax));
                     if (sk >= thr) {
-                        const double e = exact_score(prof, lut + (size_t)k * nb, Q.weights, nb);
-                        if (e > best_e || (e == best_e && k < best_k)) {
-                            best_e = e;
-                            best_k = k;
-                        }
+                        if (nc < kMaxCand) s_cand[tid * kMaxCand + nc] = (short)k;
+                        nc++;
                     }
                 }
             }
@@ -283,38 +306,46 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
         __syncthreads();  // accumulators read before the next chunk overwrites sB / TMEM
     }
 
-    // the 7-point fit (LsqQuadraticFit.h:148-171) on exact scores around the exact argmax
-    if (my_roi >= 0) {
+    // Exact scores of the candidates, argmax (the first of equal maxima, NaN skipped: warp_argmax
+    // of the plain path), and the 7-point fit (LsqQuadraticFit.h:148-171) on exact scores around it:
+    // one warp per ROI row, lanes over bins. A row with more than kMaxCand candidates is scored
+    // over every plane.
+    s_ncand[tid] = nc;
+    __syncthreads();
+    double *win = s_win + warp * 8;
+    for (int r = warp; r < m; r += kWarps) {
+        const int roi = Q.perm ? Q.perm[start + r] : start + r;
         float z = 0.0f;
         if (failed) {
             z = __int_as_float(0x7fc00000);
-        } else if (valid_bead && best_k >= 0) {
-            const int bk = best_k;
-            const int s0 = max(bk - 3, 0), s1 = min(bk + 4, Q.planes), np = s1 - s0;
-            double zz = bk;
-            if (np >= 3) {
-                double Sx = 0, Sy = 0, Sx2 = 0, Sx3 = 0, Sx4 = 0, Sxy = 0, Sx2y = 0, Sw = 0;
-                for (int i = 0; i < np; i++) {
-                    const int k = s0 + i;
-                    const double y = (k == bk) ? best_e : exact_score(prof, lut + (size_t)k * nb, Q.weights, nb);
-                    const double x = k - bk, wt = kZLUTWeightsTC[i], sq = x * x;
-                    Sx += x * wt;
-                    Sy += y * wt;
-                    Sx2 += sq * wt;
-                    Sx3 += sq * x * wt;
-                    Sx4 += sq * sq * wt;
-                    Sxy += x * y * wt;
-                    Sx2y += sq * y * wt;
-                    Sw += wt;
+        } else if (valid_bead) {
+            const float *pr = Q.prof_f32 + (size_t)roi * nb;
+            const int cnt = s_ncand[r];
+            const bool all = cnt > kMaxCand;
+            const int ncheck = all ? Q.planes : cnt;
+            double best = 0.0;
+            int bk = -1;
+            for (int i = 0; i < ncheck; i++) {
+                const int k = all ? i : s_cand[r * kMaxCand + i];
+                const double e = warp_exact_score(pr, lut + (size_t)k * nb, Q.weights, nb);
+                if (e == e && (bk < 0 || e > best || (e == best && k < bk))) {
+                    best = e;
+                    bk = k;
                 }
-                const double d = Sx4 * (Sx2 * Sw - Sx * Sx) - Sx3 * (Sx3 * Sw - Sx * Sx2) + Sx2 * (Sx3 * Sx - Sx2 * Sx2);
-                const double A = Sx2y * (Sx2 * Sw - Sx * Sx) - Sxy * (Sx3 * Sw - Sx * Sx2) + Sy * (Sx3 * Sx - Sx2 * Sx2);
-                const double B = Sx4 * (Sxy * Sw - Sy * Sx) - Sx3 * (Sx2y * Sw - Sy * Sx2) + Sx2 * (Sx2y * Sx - Sxy * Sx2);
-                if (!(fabs(A) < 1e-9 * fabs(d))) zz = bk - B / (2 * A);
             }
+            if (bk < 0) bk = 0;
+            const int s0 = max(bk - 3, 0), s1 = min(bk + 4, Q.planes);
+            for (int k = s0; k < s1; k++) {
+                const double e = warp_exact_score(pr, lut + (size_t)k * nb, Q.weights, nb);
+                if ((tid & 31) == 0) win[k - s0] = e;
+            }
+            __syncwarp();
+            auto at = [&](int k) { return win[k - s0]; };
+            const double zz = max_interp7_warp(at, Q.planes, bk, kZLUTWeightsTC);
             z = zlut_bias_correct((float)zz, Q.planes, Q.zbias, Q.zbias_w, Q.zbias_count, bead);
+            __syncwarp();
         }
-        reinterpret_cast<float *>(Q.results)[(size_t)my_roi * 13 + 8] = z;
+        if ((tid & 31) == 0) reinterpret_cast<float *>(Q.results)[(size_t)roi * 13 + 8] = z;
     }
     if (failed && tid == 0 && Q.error_flag) atomicOr(Q.error_flag, 1u);
 
@@ -358,7 +389,7 @@ __global__ void zmatch_prepare_lut_kernel(const float *__restrict__ lut, const f
 
 int zmatch_smem_bytes(int nbp)
 {
-    const int need = 2 * (kTileM * nbp * 2 + kMaxN * nbp * 2) + 16;
+    const int need = 2 * (kTileM * nbp * 2 + kMaxN * nbp * 2) + kTailBytes;
     // at least 80 KB so that no more than two CTAs (2 x 256 TMEM columns) share an SM
     return need > 80 * 1024 ? need : 80 * 1024;
 }
