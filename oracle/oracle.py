@@ -79,8 +79,10 @@ class RefOracle:
     # ---- whole pipeline through the reference's QueuedCPUTracker ----
     def track(self, s: abi.QTrkSettings, mode: int, rois: np.ndarray, lut: np.ndarray | None = None,
               zlut_index: np.ndarray | None = None, weights: np.ndarray | None = None,
-              timeout_s: float = 600.0, return_seconds: bool = False):
-        """Localize a stack of ROIs (N,H,W; u8/u16/f32). Returns results sorted by job.frame."""
+              calib: tuple | None = None, timeout_s: float = 600.0, return_seconds: bool = False):
+        """Localize a stack of ROIs (N,H,W; u8/u16/f32). Returns results sorted by job.frame.
+        calib = (offset, gain): per-bead pixel calibration images ([beads][H][W] float32 or None),
+        installed after the Z-LUT as QueuedCPUTracker::SetPixelCalibrationImages requires."""
         L = self.lib
         rois = np.ascontiguousarray(rois)
         n, h, w = rois.shape
@@ -93,6 +95,11 @@ class RefOracle:
             if weights is not None:
                 weights = np.ascontiguousarray(weights, dtype=np.float32)
                 L.QTrkSetRadialWeights(trk, _ptr(weights))
+            if calib is not None:
+                off, gain = (None if a is None else np.ascontiguousarray(a, dtype=np.float32) for a in calib)
+                L.ref_set_pixel_calibration.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+                L.ref_set_pixel_calibration(trk, None if off is None else off.ctypes.data,
+                                            None if gain is None else gain.ctypes.data)
             L.QTrkSetLocalizationMode(trk, mode)
             job = abi.LocalizationJob()
             pitch = w * rois.itemsize

@@ -156,3 +156,12 @@ REF_EXPORT void ref_average_fisher(const float *lut, int lw, int lh, float minr,
                                             });
     for (int i = 0; i < 9; i++) out9[i] = mat[i];
 }
+
+/* QueuedTracker::SetPixelCalibrationImages (QueuedTracker.h:32, defined for the CPU tracker at
+ * QueuedCPUTracker.cpp:165-196). The reference's C ABI declares QTrkSetPixelCalibrationImages
+ * (qtrk_c_api.h) but defines no body for it, so the tests reach the method through this export.
+ * The tracker must already hold its Z-LUT (the bead count sizes the images). */
+REF_EXPORT void ref_set_pixel_calibration(QueuedTracker *qtrk, float *offset, float *gain)
+{
+    qtrk->SetPixelCalibrationImages(offset, gain);
+}

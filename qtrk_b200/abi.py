@@ -223,6 +223,7 @@ B200_PROTOTYPES = {
                                   _P, _P]),
     "QTrkB200LocalizeDeviceNoAlloc": (C.c_int, [_TRK, _P, C.c_int, C.c_int64, C.c_int, C.c_int, _P, _P, _P]),
     "QTrkB200RMStoreResults": (None, [_P, _P, C.c_int, C.c_int, C.c_int]),
+    "QTrkB200SetPixelCalibrationFactors": (None, [_TRK, C.c_float, C.c_float]),
     "QTrkB200ReadRadialZLUTFile": (C.c_int, [C.c_char_p, _P, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                              C.POINTER(C.c_int)]),
     "QTrkB200WriteRadialZLUTFile": (C.c_int, [C.c_char_p, _P, C.c_int, C.c_int, C.c_int]),

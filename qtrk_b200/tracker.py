@@ -118,6 +118,10 @@ class QTrkInstance:
         self.lib.QTrkSetPixelCalibrationImages(self.handle, None if o is None else o.ctypes.data_as(C.c_void_p),
                                                None if g is None else g.ctypes.data_as(C.c_void_p))
 
+    def SetPixelCalibrationFactors(self, offset_factor: float, gain_factor: float) -> None:
+        """Scale factors of this instance's calibration images (1, 1 by default)."""
+        self.lib.QTrkB200SetPixelCalibrationFactors(self.handle, float(offset_factor), float(gain_factor))
+
     # -- LUT building (QTrkInstance.cs:51-60, 95-98) --
     def BeginLUT(self, flags: int | bool = abi.BUILDLUT_NORMALIZE) -> None:
         if isinstance(flags, bool):

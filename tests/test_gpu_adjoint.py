@@ -166,7 +166,7 @@ def test_autograd_function_and_lut_steps():
         total.backward()
         cost, grad = _cost_grad(t, d, xyz.detach().cpu().numpy())
         assert np.allclose(xyz.grad.cpu().numpy(), grad, rtol=1e-6, atol=1e-9)
-        history = [float(total)]
+        history = [float(total.detach())]
         Lv = L.detach().clone()
         for _ in range(5):
             Lr = Lv.clone().requires_grad_(True)
