@@ -1,0 +1,41 @@
+"""bench.py's accuracy helpers on the CPU: the Poisson CRLB against closed forms."""
+import numpy as np
+
+import bench
+from qtrk_b200 import synth
+
+
+def test_crlb_of_a_bright_gaussian_spot_is_the_pixelated_width_over_photons():
+    """Background-free spot: var(x) -> (sigma^2 + 1/12) / N for a pixelated Gaussian (Mortensen et al.,
+    Nat. Methods 7:377, 2010, with b -> 0); x, y, I0, bg all free."""
+    n, w, sig, ph = 4, 32, 1.5, 1e5
+    x = np.array([16.0, 16.3, 15.7, 16.5])
+    y = np.array([16.0, 15.8, 16.2, 16.5])
+    f = lambda dx, dy: synth.gaussian_spots(n, w, x + dx, y + dy, sig, np.full(n, ph), 1e-6)
+    h = 1e-4
+    mu = f(0, 0)
+    dmu = [(f(h, 0) - f(-h, 0)) / (2 * h), (f(0, h) - f(0, -h)) / (2 * h), (mu - 1e-6) / ph, np.ones_like(mu)]
+    var = bench._crlb(mu, dmu)
+    want = (sig ** 2 + 1 / 12) / ph
+    np.testing.assert_allclose(var[:, 0], want, rtol=0.03)
+    np.testing.assert_allclose(var[:, 1], want, rtol=0.03)
+
+
+def test_crlb_scales_inversely_with_intensity():
+    """Doubling background and amplitude halves the variance (Fisher information is linear in the scale)."""
+    x, y, z = np.array([50.2]), np.array([49.7]), np.array([30.0])
+    h = 1e-4
+    out = []
+    for k in (1.0, 2.0):
+        f = lambda dx, dy, dz: synth.render(100, 100, x + dx, y + dy, 0.25 * (z + dz), 200.0 * k, 2000.0 * k)
+        mu = f(0, 0, 0)
+        dmu = [(f(h, 0, 0) - f(-h, 0, 0)) / (2 * h), (f(0, h, 0) - f(0, -h, 0)) / (2 * h),
+               (f(0, 0, h) - f(0, 0, -h)) / (2 * h)]
+        out.append(bench._crlb(mu, dmu)[0])
+    np.testing.assert_allclose(out[1], out[0] / 2, rtol=1e-6)
+
+
+def test_robust_sigma_of_a_normal_sample():
+    e = np.random.Generator(np.random.PCG64(1)).normal(0, 0.3, 200000)
+    e[:100] = np.nan
+    assert abs(bench._robust_sigma(e) - 0.3) < 0.005
