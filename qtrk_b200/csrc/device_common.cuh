@@ -256,55 +256,100 @@ __device__ inline void load_roi(const G &g, float *img, const uint8_t *src, int 
         if (P.calib_offset) off = P.calib_offset + (size_t)bead * n;
         if (P.calib_gain) gain = P.calib_gain + (size_t)bead * n;
     }
-    const bool contiguous = pitch == W * bpp && ((reinterpret_cast<uintptr_t>(src) & 15) == 0) && ((n * bpp) & 15) == 0;
+    const bool contiguous = pitch == W * bpp && ((reinterpret_cast<uintptr_t>(src) & 15) == 0) &&
+                            ((n * bpp) & 15) == 0 && ((reinterpret_cast<uintptr_t>(img) & 15) == 0);
     if (contiguous) {
-        // 128-bit streaming loads over the whole ROI (rows are back to back). Each thread
-        // issues up to kLoadBatch independent loads before converting any of them, so the
-        // HBM latency is paid about once per ROI rather than once per load.
-        constexpr int kLoadBatch = 4;
-        const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
-        const int nv = (n * bpp) >> 4;
-        for (int v0 = g.rank(); v0 < nv; v0 += kLoadBatch * g.size()) {
-            uint4 q[kLoadBatch];
-#pragma unroll
-            for (int k = 0; k < kLoadBatch; k++) {
-                const int v = v0 + k * g.size();
-                if (v < nv) q[k] = __ldcs(s4 + v);
+        // Rows are back to back: the ROI is a run of n/4 chunks of four pixels (4, 8 or 16 input
+        // bytes), and chunk c becomes the float4 at img + 4c, so a warp's stores fill 512
+        // contiguous bytes of shared memory without bank conflicts. Each thread issues
+        // kBatch streaming loads (8-16 registers' worth) before converting any of them, so the
+        // HBM latency is paid about once per batch rather than once per load.
+        const int nc = n >> 2;
+        const bool plain = !off && !gain && !(P.mode & kLT_ClearFirstFourPixels);
+        float4 *dst = reinterpret_cast<float4 *>(img);
+        auto finish4 = [&](float4 f, int c) {
+            if (!plain) {
+                f.x = finish_pixel(f.x, 4 * c, P, off, gain);
+                f.y = finish_pixel(f.y, 4 * c + 1, P, off, gain);
+                f.z = finish_pixel(f.z, 4 * c + 2, P, off, gain);
+                f.w = finish_pixel(f.w, 4 * c + 3, P, off, gain);
             }
+            dst[c] = f;
+        };
+        if (P.pdt == 0) {
+            constexpr int kBatch = 8;
+            const uint32_t *s1 = reinterpret_cast<const uint32_t *>(src);
+            for (int c0 = g.rank(); c0 < nc; c0 += kBatch * g.size()) {
+                uint32_t q[kBatch];
 #pragma unroll
-            for (int k = 0; k < kLoadBatch; k++) {
-                const int v = v0 + k * g.size();
-                if (v >= nv) break;
-                const uint32_t w4[4] = {q[k].x, q[k].y, q[k].z, q[k].w};
-                if (P.pdt == 0) {
-                    const int base = v * 16;
+                for (int k = 0; k < kBatch; k++) {
+                    const int c = c0 + k * g.size();
+                    if (c < nc) q[k] = __ldcs(s1 + c);
+                }
 #pragma unroll
-                    for (int j = 0; j < 16; j++)
-                        img[base + j] = finish_pixel(u_to_float((w4[j >> 2] >> ((j & 3) * 8)) & 0xffu), base + j, P, off, gain);
-                } else if (P.pdt == 1) {
-                    const int base = v * 8;
+                for (int k = 0; k < kBatch; k++) {
+                    const int c = c0 + k * g.size();
+                    if (c >= nc) break;
+                    finish4(make_float4(u_to_float(q[k] & 0xffu), u_to_float((q[k] >> 8) & 0xffu),
+                                        u_to_float((q[k] >> 16) & 0xffu), u_to_float(q[k] >> 24)),
+                            c);
+                }
+            }
+        } else if (P.pdt == 1) {
+            constexpr int kBatch = 8;
+            const uint2 *s2 = reinterpret_cast<const uint2 *>(src);
+            for (int c0 = g.rank(); c0 < nc; c0 += kBatch * g.size()) {
+                uint2 q[kBatch];
 #pragma unroll
-                    for (int j = 0; j < 8; j++)
-                        img[base + j] = finish_pixel(u_to_float((w4[j >> 1] >> ((j & 1) * 16)) & 0xffffu), base + j, P, off, gain);
-                } else {
-                    const int base = v * 4;
+                for (int k = 0; k < kBatch; k++) {
+                    const int c = c0 + k * g.size();
+                    if (c < nc) q[k] = __ldcs(s2 + c);
+                }
 #pragma unroll
-                    for (int j = 0; j < 4; j++) img[base + j] = finish_pixel(__uint_as_float(w4[j]), base + j, P, off, gain);
+                for (int k = 0; k < kBatch; k++) {
+                    const int c = c0 + k * g.size();
+                    if (c >= nc) break;
+                    finish4(make_float4(u_to_float(q[k].x & 0xffffu), u_to_float(q[k].x >> 16),
+                                        u_to_float(q[k].y & 0xffffu), u_to_float(q[k].y >> 16)),
+                            c);
+                }
+            }
+        } else {
+            constexpr int kBatch = 4;
+            const float4 *s4 = reinterpret_cast<const float4 *>(src);
+            for (int c0 = g.rank(); c0 < nc; c0 += kBatch * g.size()) {
+                float4 q[kBatch];
+#pragma unroll
+                for (int k = 0; k < kBatch; k++) {
+                    const int c = c0 + k * g.size();
+                    if (c < nc) q[k] = __ldcs(s4 + c);
+                }
+#pragma unroll
+                for (int k = 0; k < kBatch; k++) {
+                    const int c = c0 + k * g.size();
+                    if (c >= nc) break;
+                    finish4(q[k], c);
                 }
             }
         }
     } else {
-        for (int i = g.rank(); i < n; i += g.size()) {
-            const int y = i / W, x = i - y * W;
-            const uint8_t *p = src + (size_t)y * pitch + (size_t)x * bpp;
-            float v;
-            if (P.pdt == 0)
-                v = (float)(*p);
-            else if (P.pdt == 1)
-                v = (float)(*reinterpret_cast<const uint16_t *>(p));
-            else
-                v = *reinterpret_cast<const float *>(p);
-            img[i] = finish_pixel(v, i, P, off, gain);
+        // Rows at a pitch (a ROI inside a frame): warps over rows, lanes along a row, so loads
+        // are coalesced along the row and the stores are conflict-free.
+        const int lane = g.rank() & 31, wg = g.rank() >> 5, nwg = g.size() >> 5;
+        for (int y = wg; y < H; y += nwg) {
+            const uint8_t *row = src + (size_t)y * pitch;
+#pragma unroll 4
+            for (int x = lane; x < W; x += 32) {
+                float v;
+                if (P.pdt == 0)
+                    v = u_to_float(row[x]);
+                else if (P.pdt == 1)
+                    v = u_to_float(reinterpret_cast<const uint16_t *>(row)[x]);
+                else
+                    v = reinterpret_cast<const float *>(row)[x];
+                const int i = y * W + x;
+                img[i] = finish_pixel(v, i, P, off, gain);
+            }
         }
     }
     g.sync();
@@ -621,25 +666,29 @@ __device__ inline void radial_profile(const float *img, int W, int H, float cx, 
     __syncthreads();
 }
 
-// CPUTracker::LUTProfileCompare, cpu_tracker.cpp:791-868 (plain form): one warp per plane
-// group, lanes over radial bins. scores[k] = -sum_r (w_r (p_r - L_kr))^2 with the difference
-// taken in FP32 and squared/accumulated in FP64, as the reference does.
-__device__ inline void zlut_scores_plain(const float *prof, const float *lut, int planes, int nb, const float *weights,
-                                  double *scores)
+// One plane's score of CPUTracker::LUTProfileCompare (cpu_tracker.cpp:820-830) in the reference's
+// arithmetic and order: d = (double)(p_r - L_kr) with the difference taken in FP32, d *= w_r,
+// then sum += -(d * d) over r = 0 .. nb-1 in FP64, every operation rounded on its own (no
+// contraction). Given the same profile, the score equals the reference's bit for bit.
+// lut_k[r * stride] is L_kr.
+__device__ __forceinline__ double zlut_score(const float *prof, const float *lut_k, int stride, const float *w, int nb)
 {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int k = warp; k < planes; k += nw) {
-        const float *row = lut + (size_t)k * nb;
-        double acc = 0.0;
-        for (int r = lane; r < nb; r += 32) {
-            double d = (double)(prof[r] - __ldg(row + r));
-            if (weights) d *= (double)__ldg(weights + r);
-            acc += d * d;
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) scores[k] = -acc;
+    double acc = 0.0;
+#pragma unroll 8
+    for (int r = 0; r < nb; r++) {
+        double d = (double)(prof[r] - __ldg(lut_k + (size_t)r * stride));
+        if (w) d = __dmul_rn(d, (double)__ldg(w + r));
+        acc = __dadd_rn(acc, -__dmul_rn(d, d));
     }
+    return acc;
+}
+
+// The plain Z match: one thread per plane, reading the transposed LUT ([bin][plane], `pitch`
+// planes per bin) so that a warp's 32 planes are one coalesced 128-byte load per bin.
+__device__ inline void zlut_scores_plain(const float *prof, const float *lut_t, int pitch, int planes, int nb,
+                                         const float *weights, double *scores)
+{
+    for (int k = threadIdx.x; k < planes; k += blockDim.x) scores[k] = zlut_score(prof, lut_t + k, pitch, weights, nb);
     __syncthreads();
 }
 

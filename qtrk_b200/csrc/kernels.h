@@ -58,6 +58,11 @@ cudaError_t launch_build_lut(const TrackParams &P, const uint8_t *pixels, int pi
 // NormalizeRadialProfile on `rows` rows of nb floats.
 cudaError_t launch_finalize_lut(float *lut, int rows, int nb, cudaStream_t stream);
 
+// The transposed copy of a Z-LUT that the plain match reads: [count][nb][pitch] from [count][planes][nb].
+cudaError_t launch_transpose_lut(const float *lut, int count, int planes, int nb, int pitch, float *lut_t,
+                                 cudaStream_t stream);
+inline int lut_t_pitch(int planes) { return (planes + 31) & ~31; }
+
 // Radial profile of one float image (P.width x P.height) around (cx, cy).
 cudaError_t launch_profile(const TrackParams &P, const float *img, float cx, float cy, float mean, bool normalize,
                            float *out, cudaStream_t stream);

@@ -9,6 +9,7 @@
 // build_lut_kernel / finalize_lut_kernel: QueuedCPUTracker::BuildLUT / FinalizeLUT
 //   (cputrack/QueuedCPUTracker.cpp:580-659) with the accumulation on the device.
 // profile_kernel: ComputeRadialProfile (cputrack/utils.cpp:275-320) for one image.
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <cuda_runtime.h>
@@ -142,8 +143,9 @@ __device__ float z_localize(const SmemView &s, const TrackParams &P, float mean,
         return 0.0f;
     }
     if (!P.lut || bead < 0 || bead >= P.lut_count) return 0.0f;
-    const float *lut = P.lut + (size_t)bead * P.lut_planes * nb;
-    zlut_scores_plain(prof, lut, P.lut_planes, nb, P.z_weights, scores);
+    if (!P.lut_t) return __int_as_float(0x7fc00000);  // the host launched without refreshing the transposed LUT
+    const float *lut_t = P.lut_t + (size_t)bead * nb * P.lut_t_pitch;
+    zlut_scores_plain(prof, lut_t, P.lut_t_pitch, P.lut_planes, nb, P.z_weights, scores);
     if (P.cmp_scores)
         for (int k = threadIdx.x; k < P.lut_planes; k += blockDim.x)
             P.cmp_scores[(size_t)bead * P.lut_planes + k] = (float)scores[k];
@@ -541,6 +543,31 @@ cudaError_t launch_finalize_lut(float *lut, int rows, int nb, cudaStream_t strea
 {
     if (rows <= 0) return cudaSuccess;
     finalize_lut_kernel<<<(rows + 7) / 8, 256, 0, stream>>>(lut, rows, nb);
+    return cudaGetLastError();
+}
+
+// lut [count][planes][nb] -> lut_t [count][nb][pitch], planes pitch..planes-1 of each bin zero.
+// Reads are strided, writes coalesced; it runs once per LUT change.
+__global__ void transpose_lut_kernel(const float *__restrict__ lut, int count, int planes, int nb, int pitch,
+                                     float *__restrict__ lut_t)
+{
+    const size_t total = (size_t)count * nb * pitch;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(i % pitch);
+        const size_t br = i / pitch;
+        const int r = (int)(br % nb);
+        const size_t b = br / nb;
+        lut_t[i] = k < planes ? lut[(b * planes + k) * nb + r] : 0.0f;
+    }
+}
+
+cudaError_t launch_transpose_lut(const float *lut, int count, int planes, int nb, int pitch, float *lut_t,
+                                 cudaStream_t stream)
+{
+    const size_t total = (size_t)count * nb * pitch;
+    if (total == 0) return cudaSuccess;
+    const int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
+    transpose_lut_kernel<<<blocks, 256, 0, stream>>>(lut, count, planes, nb, pitch, lut_t);
     return cudaGetLastError();
 }
 

@@ -52,6 +52,10 @@ struct TrackParams {
     const void *z_dirs;       // float2[z_angsteps]
     const float *lut;         // [lut_count][lut_planes][z_nbins]
     int lut_count, lut_planes;
+    // The same LUT transposed, [lut_count][z_nbins][lut_t_pitch] (planes padded to a multiple of
+    // 32 with zeros), for the plain match's one-thread-per-plane scoring; nullptr while stale
+    const float *lut_t;
+    int lut_t_pitch;
     const float *z_weights;   // float[z_nbins] or nullptr
     float *cmp_scores;        // [lut_count][lut_planes] or nullptr (compare-profile output)
     // Tensor-core match: when zprof_f32 is set the localization kernel writes each ROI's

@@ -326,6 +326,7 @@ Tracker::~Tracker()
     cudaFree(d_zbias_);
     cudaFree(d_lut_bf16_);
     cudaFree(d_lut_norm_);
+    cudaFree(d_lut_t_);
     cudaFree(d_dev_zprof_);
     cudaFree(d_dev_zprof_bf16_);
     cudaFreeHost(h_err_);
@@ -342,6 +343,8 @@ TrackParams Tracker::Params(int pdt) const
     P.lut = d_lut_;
     P.lut_count = lut_count_;
     P.lut_planes = lut_planes_;
+    P.lut_t = lut_t_stale_ ? nullptr : d_lut_t_;
+    P.lut_t_pitch = lut_t_pitch(lut_planes_);
     P.z_weights = have_zw_ ? d_zw_ : nullptr;
     P.cmp_scores = cmp_enabled_ ? d_cmp_ : nullptr;
     P.zbias = d_zbias_;
@@ -354,6 +357,19 @@ TrackParams Tracker::Params(int pdt) const
     P.gain_factor = gain_factor_;
     plan_smem(P);
     return P;
+}
+
+TrackParams Tracker::LaunchParams(int pdt)
+{
+    if (d_lut_ && d_lut_t_ && lut_t_stale_) {
+        CheckCuda(launch_transpose_lut(d_lut_, lut_count_, lut_planes_, cfg.zlut_radialsteps, lut_t_pitch(lut_planes_),
+                                       d_lut_t_, lut_stream_),
+                  "LUT transpose");
+        launches_++;
+        CheckCuda(cudaEventRecord(lut_ready_, lut_stream_), "cudaEventRecord");
+        lut_t_stale_ = false;
+    }
+    return Params(pdt);
 }
 
 // The adjoint of the Z match (see adjoint.cu): cost and gradients of `count` device-resident ROIs
@@ -585,7 +601,7 @@ void Tracker::RefineZLUT(const void *d_stack, int pitch, int64_t roi_stride, int
                 std::lock_guard<std::mutex> lk(mu_);
                 CheckCuda(cudaMemcpyAsync(d_lut_, L.data(), sizeof(float) * lsz, cudaMemcpyHostToDevice, lut_stream_),
                           "upload Z-LUT");
-                tc_lut_stale_ = true;
+                tc_lut_stale_ = lut_t_stale_ = true;
                 CheckCuda(cudaEventRecord(lut_ready_, lut_stream_), "cudaEventRecord");
             }
             CheckCuda(cudaStreamSynchronize(lut_stream_), "upload Z-LUT");
@@ -633,9 +649,10 @@ bool Tracker::RefineAfterZ(const TrackParams &P)
 TrackParams Tracker::AcquireLaunch(int pdt, cudaStream_t stream)
 {
     std::lock_guard<std::mutex> lk(mu_);
+    TrackParams P = LaunchParams(pdt);
     CheckCuda(cudaStreamWaitEvent(stream, lut_ready_, 0), "cudaStreamWaitEvent");
     launches_++;
-    return Params(pdt);
+    return P;
 }
 
 void Tracker::AllocateSlots()
@@ -726,7 +743,7 @@ int Tracker::AcquireSlotLocked(std::unique_lock<std::mutex> &lk)
 void Tracker::SubmitLocked(int idx)
 {
     Slot &s = slots_[idx];
-    TrackParams P = Params(s.pdt);
+    TrackParams P = LaunchParams(s.pdt);
     const size_t roib = (size_t)cfg.base.width * cfg.base.height * pdt_bytes(s.pdt);
     const bool tc = UseTensorCoreMatch();
     int ntiles = 0;
@@ -1144,8 +1161,10 @@ void Tracker::SetRadialZLUT(const float *data, int count, int planes)
     WaitIdleForReconfigure();
     std::lock_guard<std::mutex> lk(mu_);
     cudaFree(d_lut_);
+    cudaFree(d_lut_t_);
     cudaFree(d_cmp_);
     d_lut_ = nullptr;
+    d_lut_t_ = nullptr;
     d_cmp_ = nullptr;
     cudaFree(d_zbias_);  // a new LUT drops the bias table, as QueuedCPUTracker.cpp:368-369
     d_zbias_ = nullptr;
@@ -1158,15 +1177,18 @@ void Tracker::SetRadialZLUT(const float *data, int count, int planes)
             CheckCuda(cudaMemcpy(d_lut_, data, total * 4, cudaMemcpyHostToDevice), "upload Z-LUT");
         else
             CheckCuda(cudaMemset(d_lut_, 0, total * 4), "clear Z-LUT");
+        CheckCuda(cudaMalloc(&d_lut_t_, (size_t)count * res * lut_t_pitch(planes) * 4), "cudaMalloc(Z-LUT copy)");
         CheckCuda(cudaMalloc(&d_cmp_, (size_t)count * planes * 4), "cudaMalloc(compare profiles)");
         CheckCuda(cudaMemset(d_cmp_, 0, (size_t)count * planes * 4), "clear compare profiles");
         lut_count_ = count;
         lut_planes_ = planes;
-        tc_lut_stale_ = true;
+        tc_lut_stale_ = lut_t_stale_ = true;
         if (Params(2).smem_bytes > 227 * 1024) {
             cudaFree(d_lut_);
+            cudaFree(d_lut_t_);
             cudaFree(d_cmp_);
             d_lut_ = nullptr;
+            d_lut_t_ = nullptr;
             d_cmp_ = nullptr;
             lut_count_ = lut_planes_ = 0;
             throw std::invalid_argument("Z-LUT with " + std::to_string(planes) +
@@ -1207,7 +1229,7 @@ void Tracker::SetRadialWeights(const float *w)
     } else {
         have_zw_ = false;
     }
-    tc_lut_stale_ = true;
+    tc_lut_stale_ = true;  // the BF16 copy holds weighted rows; the transposed one does not
 }
 
 // QueuedTracker::SetZLUTBiasCorrection (cputrack/QueuedTracker.cpp:178-182): table[bead][bias_plane],
@@ -1248,7 +1270,7 @@ void Tracker::ComputeZBiasTable(int bias_planes, int smp_per_pixel, bool spline,
         if (!d_lut_ || lut_count_ <= 0 || lut_planes_ < 2) throw std::runtime_error("ComputeZBiasTable: no Z-LUT set");
         count = lut_count_;
         planes = lut_planes_;
-        P = Params(2);
+        P = LaunchParams(2);
     }
     const int W = cfg.base.width, H = cfg.base.height, nb = P.z_nbins;
     P.mode = kLT_QI | kLT_LocalizeZ | kLT_NormalizeProfile;
@@ -1411,7 +1433,7 @@ void Tracker::BuildLUT(const void *data, int pitch, int pdt, int plane, const ve
     launches_++;
     CheckCuda(cudaEventRecord(lut_stage_free_[b], lut_stream_), "cudaEventRecord");
     CheckCuda(cudaEventRecord(lut_ready_, lut_stream_), "cudaEventRecord");
-    tc_lut_stale_ = true;
+    tc_lut_stale_ = lut_t_stale_ = true;
     if (pinned) CheckCuda(cudaEventSynchronize(lut_copy_done_[b]), "cudaEventSynchronize(LUT copy)");
 }
 
@@ -1427,7 +1449,7 @@ void Tracker::FinalizeLUT()
     }
     CheckCuda(cudaEventRecord(lut_ready_, lut_stream_), "cudaEventRecord");
     CheckCuda(cudaStreamSynchronize(lut_stream_), "cudaStreamSynchronize(lut)");
-    tc_lut_stale_ = true;
+    tc_lut_stale_ = lut_t_stale_ = true;
 }
 
 int Tracker::GetResultCount()
@@ -1513,7 +1535,7 @@ int Tracker::LocalizeDevice(const void *d_pixels, int pitch, int64_t roi_stride,
     bool tc;
     {
         std::lock_guard<std::mutex> lk(mu_);
-        P = Params(pdt);
+        P = LaunchParams(pdt);
         tc = UseTensorCoreMatch();
         if (tc && d_jobs) {
             // the bead of each ROI is only known on the device here: score with the plain path
@@ -1590,7 +1612,7 @@ int Tracker::LocalizeDeviceNoAlloc(const void *d_pixels, int pitch, int64_t roi_
     bool tc;
     {
         std::lock_guard<std::mutex> lk(mu_);
-        P = Params(pdt);
+        P = LaunchParams(pdt);
         tc = UseTensorCoreMatch() && !d_jobs;  // device-side jobs: plain match, as LocalizeDevice
         if (tc) {
             if (!d_lut_bf16_ || !d_lut_norm_) {

@@ -89,7 +89,7 @@ class Tracker : public QueuedTracker {
     int64_t LaunchCount() const { return launches_.load(); }
     void Warn(const std::string &msg);
     int device() const { return device_; }
-    TrackParams Params(int pdt) const;  // current parameters for a launch
+    TrackParams Params(int pdt) const;  // current parameters (the transposed LUT only if fresh)
     // Parameters for one launch that another component (the request server) puts on `stream`:
     // the stream is ordered after pending LUT work and the launch is counted.
     TrackParams AcquireLaunch(int pdt, cudaStream_t stream);
@@ -125,6 +125,9 @@ class Tracker : public QueuedTracker {
     bool UseTensorCoreMatch() const;     // mode asks for it and the LUT shape allows it
     static bool RefineAfterZ(const TrackParams &P);
     void PrepareTensorCoreLUT();         // BF16 weighted LUT + norms when stale (LUT stream)
+    // Params for a localization launch: refreshes the transposed LUT first when stale (a kernel on
+    // the LUT stream, no allocation); the caller's stream must wait on lut_ready_ afterwards.
+    TrackParams LaunchParams(int pdt);
     ZMatchParams TensorCoreParams() const;
     int BuildTiles(const LocalizationJob *jobs, int count, int *perm, int4 *tiles) const;
 
@@ -144,6 +147,8 @@ class Tracker : public QueuedTracker {
     // Z-LUT state
     float *d_lut_ = nullptr;
     int lut_count_ = 0, lut_planes_ = 0;
+    float *d_lut_t_ = nullptr;   // transposed copy, allocated with d_lut_
+    bool lut_t_stale_ = true;
     float *d_zw_ = nullptr;
     bool have_zw_ = false;
     float *d_cmp_ = nullptr;

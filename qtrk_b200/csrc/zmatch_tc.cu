@@ -18,8 +18,9 @@
 // down to d_k = 2^-9 |p'| |L'_k| (a generous cover of the ~3 2^-16 split error plus the FP32
 // accumulation of 3 K products), so only a few planes per ROI need the exact re-score. Threads
 // record those candidate planes from their TMEM rows; warps then compute the exact scores with
-// the plain path's lane mapping and reduction order, take the argmax and run the 7-point fit
-// (LsqQuadraticFit.h:132-176) with the plain path's warp code, so z is the plain path's bit for bit.
+// the plain path's per-plane function (zlut_score: one lane per plane, bins in order), take the
+// argmax and run the 7-point fit (LsqQuadraticFit.h:132-176) with the plain path's warp code, so z
+// is the plain path's bit for bit.
 //
 // Launch: one CTA of 128 threads per tile. Shared memory is sized so that at most two CTAs
 // share an SM, so the two 256-column TMEM allocations always fit the SM's 512 columns and
@@ -125,23 +126,6 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
 __device__ __forceinline__ void store_chunk(uint8_t *base, int r, int c, int sbo, uint4 v)
 {
     *reinterpret_cast<uint4 *>(base + (r >> 3) * sbo + c * 128 + (r & 7) * 16) = v;
-}
-
-// Exact score of one plane by one warp, in the plain path's order (zlut_scores_plain: lanes over
-// bins r = lane + 32 j, FP32 difference, FP64 square sums, xor-shuffle reduction): the tensor-core
-// path's scores, and so its argmax and fit, are the plain path's bit for bit. Every lane returns it.
-__device__ double warp_exact_score(const float *prof, const float *lutrow, const float *w, int nb)
-{
-    const int lane = threadIdx.x & 31;
-    double acc = 0.0;
-    for (int r = lane; r < nb; r += 32) {
-        double d = (double)(prof[r] - __ldg(lutrow + r));
-        if (w) d *= (double)__ldg(w + r);
-        acc += d * d;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    return -acc;
 }
 
 }  // namespace
@@ -306,12 +290,14 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
         __syncthreads();  // accumulators read before the next chunk overwrites sB / TMEM
     }
 
-    // Exact scores of the candidates, argmax (the first of equal maxima, NaN skipped: warp_argmax
-    // of the plain path), and the 7-point fit (LsqQuadraticFit.h:148-171) on exact scores around it:
-    // one warp per ROI row, lanes over bins. A row with more than kMaxCand candidates is scored
-    // over every plane.
+    // Exact scores of the candidates (zlut_score: the plain path's arithmetic and order, so the
+    // scores, argmax and fit are the plain path's bit for bit), argmax (the first of equal maxima,
+    // NaN skipped: warp_argmax of the plain path), and the 7-point fit (LsqQuadraticFit.h:148-171)
+    // on exact scores around it: one warp per ROI row, one lane per candidate plane. A row with more
+    // than kMaxCand candidates is scored over every plane.
     s_ncand[tid] = nc;
     __syncthreads();
+    const int lane = tid & 31;
     double *win = s_win + warp * 8;
     for (int r = warp; r < m; r += kWarps) {
         const int roi = Q.perm ? Q.perm[start + r] : start + r;
@@ -325,20 +311,26 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
             const int ncheck = all ? Q.planes : cnt;
             double best = 0.0;
             int bk = -1;
-            for (int i = 0; i < ncheck; i++) {
+            for (int i = lane; i < ncheck; i += 32) {
                 const int k = all ? i : s_cand[r * kMaxCand + i];
-                const double e = warp_exact_score(pr, lut + (size_t)k * nb, Q.weights, nb);
+                const double e = zlut_score(pr, lut + (size_t)k * nb, 1, Q.weights, nb);
                 if (e == e && (bk < 0 || e > best || (e == best && k < bk))) {
                     best = e;
                     bk = k;
                 }
             }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int ok = __shfl_xor_sync(0xffffffffu, bk, o);
+                if (ok >= 0 && (bk < 0 || ob > best || (ob == best && ok < bk))) {
+                    best = ob;
+                    bk = ok;
+                }
+            }
             if (bk < 0) bk = 0;
             const int s0 = max(bk - 3, 0), s1 = min(bk + 4, Q.planes);
-            for (int k = s0; k < s1; k++) {
-                const double e = warp_exact_score(pr, lut + (size_t)k * nb, Q.weights, nb);
-                if ((tid & 31) == 0) win[k - s0] = e;
-            }
+            if (lane < s1 - s0) win[lane] = zlut_score(pr, lut + (size_t)(s0 + lane) * nb, 1, Q.weights, nb);
             __syncwarp();
             auto at = [&](int k) { return win[k - s0]; };
             const double zz = max_interp7_warp(at, Q.planes, bk, kZLUTWeightsTC);
