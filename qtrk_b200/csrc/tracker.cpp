@@ -1021,11 +1021,11 @@ int Tracker::ScheduleFrame(const void *img, int pitch, int width, int height, co
     if (skipped) Warn("ScheduleFrame: skipped " + std::to_string(skipped) + " ROI(s) outside the frame");
     if (idx.empty()) return 0;
 
-    // Group ROIs into row bands of at most 16 MiB (or one slot, if smaller); one band keeps the
+    // Group ROIs into row bands of at most 32 MiB (or one slot, if smaller); one band keeps the
     // caller's order. The bands' copies run one after another (each waits for the previous one),
     // so every band's kernel overlaps the next band's copy and only the last, small band's kernel
     // is left after the frame has crossed PCIe.
-    const size_t band_cap = std::min(slot_bytes_, (size_t)16 << 20);
+    const size_t band_cap = std::min(slot_bytes_, (size_t)32 << 20);
     int minx = width, maxx = 0;
     for (int i : idx) {
         minx = std::min(minx, pos[i].x);
@@ -1044,7 +1044,9 @@ int Tracker::ScheduleFrame(const void *img, int pitch, int width, int height, co
             bands.push_back(idx);
         } else {
             std::vector<int> sorted = idx;
-            std::stable_sort(sorted.begin(), sorted.end(), [&](int a, int b) { return pos[a].y < pos[b].y; });
+            auto by_row = [&](int a, int b) { return pos[a].y < pos[b].y; };
+            if (!std::is_sorted(sorted.begin(), sorted.end(), by_row))  // frames are usually listed in scan order
+                std::stable_sort(sorted.begin(), sorted.end(), by_row);
             std::vector<int> cur;
             int by0 = 0, by1 = 0;
             for (int i : sorted) {
