@@ -130,39 +130,11 @@ __device__ __forceinline__ bool check_boundaries(float cx, float cy, float radiu
     return cx + radius >= w || cx - radius < 0 || cy + radius >= h || cy - radius < 0;
 }
 
-// LsqSqQuadFit + ComputeMaxInterp<T,7>::Compute, LsqQuadraticFit.h:8-176, evaluated in FP64.
-// `at(i)` returns element i of the length-`len` array; iMax is the first index of the maximum.
-// The weights are indexed from 0 even when the window is clipped at the array start, as in
-// the reference.
-template <typename Get>
-__device__ inline double max_interp7(Get at, int len, int iMax, const float (&wts)[7])
-{
-    const int startPos = max(iMax - 3, 0);
-    const int endPos = min(iMax + 4, len);
-    const int np = endPos - startPos;
-    if (np < 3) return (double)iMax;
-    double Sx = 0, Sy = 0, Sx2 = 0, Sx3 = 0, Sx4 = 0, Sxy = 0, Sx2y = 0, Sw = 0;
-    for (int i = 0; i < np; i++) {
-        const double x = (double)(startPos + i - iMax), y = (double)at(startPos + i), wt = (double)wts[i];
-        const double sq = x * x;
-        Sx += x * wt;
-        Sy += y * wt;
-        Sx2 += sq * wt;
-        Sx3 += sq * x * wt;
-        Sx4 += sq * sq * wt;
-        Sxy += x * y * wt;
-        Sx2y += sq * y * wt;
-        Sw += wt;
-    }
-    const double d = Sx4 * (Sx2 * Sw - Sx * Sx) - Sx3 * (Sx3 * Sw - Sx * Sx2) + Sx2 * (Sx3 * Sx - Sx2 * Sx2);
-    const double a = (Sx2y * (Sx2 * Sw - Sx * Sx) - Sxy * (Sx3 * Sw - Sx * Sx2) + Sy * (Sx3 * Sx - Sx2 * Sx2)) / d;
-    const double b = (Sx4 * (Sxy * Sw - Sy * Sx) - Sx3 * (Sx2y * Sw - Sy * Sx2) + Sx2 * (Sx2y * Sx - Sxy * Sx2)) / d;
-    if (fabs(a) < 1e-9) return (double)iMax;
-    return (double)iMax - b / (2 * a);
-}
-
-// The same fit with the eight weighted sums formed by lanes 0..6 of one warp (all 32 lanes
-// call; every lane returns the result). maxPos = iMax - b/(2a) with a = A/d, b = B/d, so the
+// LsqSqQuadFit + ComputeMaxInterp<T,7>::Compute (LsqQuadraticFit.h:8-176) in FP64, with the eight
+// weighted sums formed by lanes 0..6 of one warp (all 32 lanes call; every lane returns the result).
+// `at(i)` returns element i of the length-`len` array; iMax is the first index of the maximum;
+// the weights are indexed from 0 even when the window is clipped at the array start, as in the
+// reference. maxPos = iMax - b/(2a) with a = A/d, b = B/d, so the
 // determinant d cancels and one division remains; |a| < 1e-9 is tested as |A| < 1e-9 |d|.
 template <typename Get>
 __device__ inline double max_interp7_warp(Get at, int len, int iMax, const float (&wts)[7])
@@ -197,6 +169,42 @@ __device__ inline double max_interp7_warp(Get at, int len, int iMax, const float
     const double B = Sx4 * (Sxy * Sw - Sy * Sx) - Sx3 * (Sx2y * Sw - Sy * Sx2) + Sx2 * (Sx2y * Sx - Sxy * Sx2);
     if (fabs(A) < 1e-9 * fabs(d)) return (double)iMax;
     return (double)iMax - B / (2 * A);
+}
+
+// The same fit for the common case, a window iMax-3 .. iMax+3 inside the array with weights
+// symmetric about its centre (the reference's QIWeights and ZLUTWeights). Then S_x = S_x3 = 0
+// and the cofactor expansion of LsqSqQuadFit::Coeff::abc reduces to
+//   maxPos = iMax - (p0 / (2 Sx2)) N / D,  N = sum w x y,  D = sum w (x^2 Sw - Sx2) y,
+//   p0 = Sx4 Sw - Sx2^2,  S_x^k = sum w x^k,  Sw = sum w,
+// and a = D / p0 (the |a| < 1e-9 test). Both stencils sum to zero, so y is taken relative to
+// y[iMax]: the two 7-term sums run in FP32 on small differences, which keeps the offset to ~1e-7
+// of itself, with no FP64 and no cross-lane traffic. Clipped windows take max_interp7_warp.
+// All 32 lanes of a warp call (with the same arguments); every lane returns the result.
+template <typename Get>
+__device__ __forceinline__ float max_interp7_sym(Get at, int len, int iMax, const float (&wts)[7])
+{
+    if (iMax < 3 || iMax + 4 > len) return (float)max_interp7_warp(at, len, iMax, wts);
+    float Sw = 0.0f, Sx2 = 0.0f, Sx4 = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 7; i++) {
+        const float x2 = (float)((i - 3) * (i - 3)), w = wts[i];
+        Sw += w;
+        Sx2 += w * x2;
+        Sx4 += w * x2 * x2;
+    }
+    const auto yc = at(iMax);
+    float N = 0.0f, D = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 7; i++) {
+        if (i == 3) continue;  // y - y[iMax] = 0
+        const float x = (float)(i - 3), w = wts[i];
+        const float d = (float)(at(iMax - 3 + i) - yc);
+        N += w * x * d;
+        D += w * (x * x * Sw - Sx2) * d;
+    }
+    const float p0 = Sx4 * Sw - Sx2 * Sx2;
+    if (fabsf(D) < 1e-9f * p0) return (float)iMax;
+    return (float)iMax - (p0 / (2.0f * Sx2)) * (N / D);
 }
 
 // First index of the maximum of at(0..len), reduced over one warp (all 32 lanes call).

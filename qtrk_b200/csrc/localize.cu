@@ -101,7 +101,7 @@ __device__ void qi_localize(const SmemView &s, const TrackParams &P, float mean,
                 return yaxis ? ac[n].y : ac[n].x;
             };
             const int im = warp_argmax(at, L);
-            const float m = (float)max_interp7_warp(at, L, im, kQIWeights);
+            const float m = max_interp7_sym(at, L, im, kQIWeights);
             if ((threadIdx.x & 31) == 0) {
                 const float off = (m - (float)nr) * (3.14159265359f / 4);
                 s.misc[yaxis ? 1 : 0] = (yaxis ? cy : cx) + off * rstep;
@@ -152,7 +152,7 @@ __device__ float z_localize(const SmemView &s, const TrackParams &P, float mean,
     if (threadIdx.x < 32) {
         auto at = [&](int i) { return scores[i]; };
         const int im = warp_argmax(at, P.lut_planes);
-        const float z = (float)max_interp7_warp(at, P.lut_planes, im, kZLUTWeights);
+        const float z = max_interp7_sym(at, P.lut_planes, im, kZLUTWeights);
         if (threadIdx.x == 0) s.misc[2] = zlut_bias_correct(z, P.lut_planes, P.zbias, P.zbias_w, P.zbias_count, bead);
     }
     __syncthreads();

@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
             if (lane < s1 - s0) win[lane] = zlut_score(pr, lut + (size_t)(s0 + lane) * nb, 1, Q.weights, nb);
             __syncwarp();
             auto at = [&](int k) { return win[k - s0]; };
-            const double zz = max_interp7_warp(at, Q.planes, bk, kZLUTWeightsTC);
+            const float zz = max_interp7_sym(at, Q.planes, bk, kZLUTWeightsTC);
             z = zlut_bias_correct((float)zz, Q.planes, Q.zbias, Q.zbias_w, Q.zbias_count, bead);
             __syncwarp();
         }
