@@ -158,7 +158,6 @@ class Tracker : public QueuedTracker {
     cudaEvent_t lut_ready_ = nullptr;
     uint8_t *h_lut_stage_[2] = {nullptr, nullptr};
     uint8_t *d_lut_stage_[2] = {nullptr, nullptr};
-    float2 *d_known_[2] = {nullptr, nullptr};
     cudaEvent_t lut_stage_free_[2] = {nullptr, nullptr};
     cudaStream_t lut_copy_stream_ = nullptr;          // H2D of pinned BuildLUT stacks
     cudaEvent_t lut_copy_done_[2] = {nullptr, nullptr};
