@@ -47,6 +47,8 @@ Server::Server(int device, int64_t memory_budget) : device_(device)
         for (Lane &l : lanes_) {
             ck(cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking), "cudaStreamCreate");
             ck(cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming), "cudaEventCreate");
+            ck(cudaStreamCreateWithFlags(&l.copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+            for (cudaEvent_t &e : l.band_done) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
             ck(cudaMalloc(&l.d_pix, kLaneBytes), "cudaMalloc(lane pixels)");
             ck(cudaMalloc(&l.d_off, sizeof(int64_t) * kMaxLaneRois), "cudaMalloc");
             ck(cudaMalloc(&l.d_jobs, sizeof(LocalizationJob) * kMaxLaneRois), "cudaMalloc");
@@ -88,6 +90,7 @@ void Server::Release()
     cudaSetDevice(device_);
     for (Lane &l : lanes_) {
         if (l.stream) cudaStreamSynchronize(l.stream);
+        if (l.copy_stream) cudaStreamSynchronize(l.copy_stream);
         for (auto &kv : l.graphs) {
             cudaGraphExecDestroy(kv.second.exec);
             cudaGraphDestroy(kv.second.graph);
@@ -101,6 +104,9 @@ void Server::Release()
         cudaFreeHost(l.h_jobs);
         cudaFreeHost(l.h_res);
         if (l.done) cudaEventDestroy(l.done);
+        for (cudaEvent_t e : l.band_done)
+            if (e) cudaEventDestroy(e);
+        if (l.copy_stream) cudaStreamDestroy(l.copy_stream);
         if (l.stream) cudaStreamDestroy(l.stream);
         l = Lane();
     }
@@ -289,48 +295,108 @@ Server::Graph &Server::GraphFor(Lane &lane, int inst, int bucket, const TrackPar
 }
 
 // Runs without the server lock: touches only the lane (dispatcher-owned) and the requests'
-// immutable submission fields.
+// immutable submission fields. The requests' row bands are stacked in the lane at one pitch. A
+// batch of a few MiB or less is one copy plus a graph replay (kernel + result copy). A larger one
+// is split by rows into up to kMaxBands bands of about kBandBytes, copied in order on the lane's
+// copy stream; the kernel of band b runs on the lane stream as soon as band b has arrived, over a
+// prefix of the ROIs (in submission order) that lies inside the rows copied so far, so the
+// kernels overlap the later copies and only the last band's kernel is left after the batch has
+// crossed PCIe. Every ROI is computed the same way in either form.
 void Server::LaunchBatch(Lane &lane, Tracker *t, const std::vector<Request *> &batch)
 {
     const int pdt = batch[0]->pdt, bpp = pdt_bytes(pdt);
+    const int H = t->cfg.base.height;
     int maxw = 0;
     for (Request *r : batch) maxw = std::max(maxw, r->w);
     const size_t pitch = ((size_t)maxw * bpp + 15) & ~(size_t)15;
-    size_t base = 0;
-    int k = 0;
-    for (Request *r : batch) {
-        ck(cudaMemcpy2DAsync(lane.d_pix + base, pitch, r->frame + (size_t)r->y0 * r->pitch + (size_t)r->x0 * bpp,
-                             (size_t)r->pitch, (size_t)r->w * bpp, (size_t)r->h, cudaMemcpyHostToDevice, lane.stream),
-           "H2D frame band");
+    // stacked rows: request r at rows [row0[r], row0[r] + h); ROI i ends at row yend[i]
+    std::vector<int> row0(batch.size()), yend;
+    int rows = 0, k = 0;
+    for (size_t q = 0; q < batch.size(); q++) {
+        const Request *r = batch[q];
+        row0[q] = rows;
         for (size_t i = 0; i < r->offs.size(); i++) {
             const int64_t ry = r->offs[i] >> 32, rx = r->offs[i] & 0xffffffff;
-            lane.h_off[k] = (int64_t)base + ry * (int64_t)pitch + rx * bpp;
+            lane.h_off[k] = (int64_t)rows * (int64_t)pitch + ry * (int64_t)pitch + rx * bpp;
             lane.h_jobs[k] = r->jobs[i];
+            yend.push_back(rows + (int)ry + H);
             k++;
         }
-        base += (size_t)r->h * pitch;
+        rows += r->h;
     }
-    ck(cudaMemcpyAsync(lane.d_off, lane.h_off, sizeof(int64_t) * k, cudaMemcpyHostToDevice, lane.stream), "H2D offsets");
-    ck(cudaMemcpyAsync(lane.d_jobs, lane.h_jobs, sizeof(LocalizationJob) * k, cudaMemcpyHostToDevice, lane.stream),
-       "H2D jobs");
+    // bands: [m[b], m[b+1]) of the ROIs, rows [R[b], R[b+1]) of the stack
+    int nb = (int)std::min<size_t>(kMaxBands, std::max<size_t>(1, (size_t)rows * pitch / kBandBytes));
+    std::vector<int> m(1, 0), R(1, 0);
+    for (int b = 1; b < nb && m.back() < k; b++) {
+        const int target = std::max((int)((int64_t)k * b / nb), m.back() + 1);
+        int rb = R.back();
+        for (int i = m.back(); i < target; i++) rb = std::max(rb, yend[i]);
+        int mb = target;
+        while (mb < k && yend[mb] <= rb) mb++;
+        if (mb >= k || rb >= rows) break;  // what is left is the last band
+        m.push_back(mb);
+        R.push_back(rb);
+    }
+    m.push_back(k);
+    R.push_back(rows);
+    nb = (int)m.size() - 1;
+    cudaStream_t cs = nb > 1 ? lane.copy_stream : lane.stream;
+    for (int b = 0; b < nb; b++) {
+        // the rows [R[b], R[b+1]) of every request that has some
+        for (size_t q = 0; q < batch.size(); q++) {
+            const Request *r = batch[q];
+            const int lo = std::max(R[b], row0[q]), hi = std::min(R[b + 1], row0[q] + r->h);
+            if (lo >= hi) continue;
+            ck(cudaMemcpy2DAsync(lane.d_pix + (size_t)lo * pitch, pitch,
+                                 r->frame + (size_t)(r->y0 + lo - row0[q]) * r->pitch + (size_t)r->x0 * bpp,
+                                 (size_t)r->pitch, (size_t)r->w * bpp, (size_t)(hi - lo), cudaMemcpyHostToDevice, cs),
+               "H2D frame band");
+        }
+        if (b == 0) {
+            ck(cudaMemcpyAsync(lane.d_off, lane.h_off, sizeof(int64_t) * k, cudaMemcpyHostToDevice, cs), "H2D offsets");
+            ck(cudaMemcpyAsync(lane.d_jobs, lane.h_jobs, sizeof(LocalizationJob) * k, cudaMemcpyHostToDevice, cs),
+               "H2D jobs");
+        }
+        if (nb > 1) ck(cudaEventRecord(lane.band_done[b], cs), "cudaEventRecord");
+    }
     TrackParams P = t->AcquireLaunch(pdt, lane.stream);
     P.mode &= ~(kLT_ZMatchBF16 | kLT_JointRefine);  // the graph holds the localization kernel alone
-    int bucket = 32;
-    while (bucket < k) bucket <<= 1;
-    Graph &g = GraphFor(lane, batch[0]->inst, bucket, P);
     lane.P = P;
     lane.a_pix = lane.d_pix;
     lane.a_pitch = (int)pitch;
     lane.a_stride = 0;
-    lane.a_off = lane.d_off;
-    lane.a_jobs = lane.d_jobs;
-    lane.a_count = k;
-    lane.a_res = lane.d_res;
-    cudaKernelNodeParams kp;
-    localize_node(P, k, kp);  // grid for k ROIs; same function and shared memory as the graph's node
-    kp.kernelParams = lane.args;
-    ck(cudaGraphExecKernelNodeSetParams(g.exec, g.kernel, &kp), "cudaGraphExecKernelNodeSetParams");
-    ck(cudaGraphLaunch(g.exec, lane.stream), "cudaGraphLaunch");
+    if (nb > 1) {
+        for (int b = 0; b < nb; b++) {
+            ck(cudaStreamWaitEvent(lane.stream, lane.band_done[b], 0), "cudaStreamWaitEvent");
+            lane.a_off = lane.d_off + m[b];
+            lane.a_jobs = lane.d_jobs + m[b];
+            lane.a_count = m[b + 1] - m[b];
+            lane.a_res = lane.d_res + m[b];
+            cudaKernelNodeParams kp;
+            localize_node(P, lane.a_count, kp);
+            ck(cudaLaunchKernel(kp.func, kp.gridDim, kp.blockDim, lane.args, kp.sharedMemBytes, lane.stream),
+               "localize launch");
+        }
+        ck(cudaMemcpyAsync(lane.h_res, lane.d_res, sizeof(LocalizationResult) * k, cudaMemcpyDeviceToHost, lane.stream),
+           "D2H results");
+    } else {
+        int bucket = 32;
+        while (bucket < k) bucket <<= 1;
+        Graph &g = GraphFor(lane, batch[0]->inst, bucket, P);
+        lane.P = P;
+        lane.a_pix = lane.d_pix;
+        lane.a_pitch = (int)pitch;
+        lane.a_stride = 0;
+        lane.a_off = lane.d_off;
+        lane.a_jobs = lane.d_jobs;
+        lane.a_count = k;
+        lane.a_res = lane.d_res;
+        cudaKernelNodeParams kp;
+        localize_node(P, k, kp);  // grid for k ROIs; same function and shared memory as the graph's node
+        kp.kernelParams = lane.args;
+        ck(cudaGraphExecKernelNodeSetParams(g.exec, g.kernel, &kp), "cudaGraphExecKernelNodeSetParams");
+        ck(cudaGraphLaunch(g.exec, lane.stream), "cudaGraphLaunch");
+    }
     ck(cudaEventRecord(lane.done, lane.stream), "cudaEventRecord");
     lane.count = k;
 }
@@ -432,6 +498,14 @@ void Server::Run()
             progressed = true;
         }
         if (!any_busy && (pending_.empty() || hold_)) {
+            // idle: poll for the next frame for a short while before sleeping, so that frames
+            // arriving at camera rates do not each pay a thread wake-up
+            const double until = now_s() + kIdleSpinSeconds;
+            while (!stop_ && (pending_.empty() || hold_) && now_s() < until) {
+                lk.unlock();
+                std::this_thread::yield();
+                lk.lock();
+            }
             cv_.wait(lk, [&] { return stop_ || (!pending_.empty() && !hold_); });
         } else if (!progressed) {
             lk.unlock();

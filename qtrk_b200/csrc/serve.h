@@ -41,6 +41,8 @@ class Server {
 
     static constexpr int kMaxLaneRois = 8192;
     static constexpr size_t kLaneBytes = 48u << 20;
+    static constexpr double kIdleSpinSeconds = 0.005;  // dispatcher polls this long before it sleeps
+    static constexpr size_t kBandBytes = 6u << 20;  // a batch is copied in bands of about this size (<= 4)
 
   private:
     struct Request {
@@ -61,9 +63,13 @@ class Server {
         cudaGraphNode_t kernel = nullptr;
         int bucket = 0;
     };
+    static constexpr int kMaxBands = 4;
     struct Lane {
         cudaStream_t stream = nullptr;
         cudaEvent_t done = nullptr;
+        // a large batch is copied in row bands on copy_stream; band b's kernel waits on band_done[b]
+        cudaStream_t copy_stream = nullptr;
+        cudaEvent_t band_done[kMaxBands] = {};
         uint8_t *d_pix = nullptr;
         int64_t *d_off = nullptr, *h_off = nullptr;
         LocalizationJob *d_jobs = nullptr, *h_jobs = nullptr;
