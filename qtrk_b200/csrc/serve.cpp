@@ -27,11 +27,12 @@ void ck(cudaError_t e, const char *what)
 
 int pdt_bytes(int pdt) { return pdt == 0 ? 1 : (pdt == 1 ? 2 : 4); }
 
-uint64_t graph_key(int inst, int bucket, int pdt, int mode, int smem)
+uint64_t graph_key(int inst, int bucket, int bands, int pdt, int mode, int smem)
 {
-    // instance (8 bits) | bucket (14) | pdt (2) | mode bits folded (22) | smem / 16 (18)
-    return ((uint64_t)(inst & 0xff) << 56) | ((uint64_t)(bucket & 0x3fff) << 42) | ((uint64_t)(pdt & 3) << 40) |
-           ((uint64_t)((mode ^ (mode >> 22)) & 0x3fffff) << 18) | (uint64_t)((smem >> 4) & 0x3ffff);
+    // instance (8 bits) | bucket (14) | bands - 1 (2) | pdt (2) | mode bits folded (20) | smem / 16 (18)
+    return ((uint64_t)(inst & 0xff) << 56) | ((uint64_t)(bucket & 0x3fff) << 42) | ((uint64_t)((bands - 1) & 3) << 40) |
+           ((uint64_t)(pdt & 3) << 38) | ((uint64_t)((mode ^ (mode >> 20)) & 0xfffff) << 18) |
+           (uint64_t)((smem >> 4) & 0x3ffff);
 }
 
 }  // namespace
@@ -258,15 +259,18 @@ QTrkB200ServeStats Server::Stats()
 // followed by the copy of their results to the lane's pinned buffer. Built node by node (not
 // captured) so that the kernel node's function and shared memory are the ones launch_localize
 // uses; each replay patches the node's arguments and grid.
-Server::Graph &Server::GraphFor(Lane &lane, int inst, int bucket, const TrackParams &P)
+// The graph of one launch: for each row band, a wait for that band's copy (banded batches only)
+// and the localization kernel over the band's ROIs, then the copy of all results to the host.
+// Grids and arguments are patched into the kernel nodes at each replay.
+Server::Graph &Server::GraphFor(Lane &lane, int inst, int bucket, int bands, const TrackParams &P)
 {
-    const uint64_t key = graph_key(inst, bucket, P.pdt, P.mode, P.smem_bytes);
+    const uint64_t key = graph_key(inst, bucket, bands, P.pdt, P.mode, P.smem_bytes);
     auto it = lane.graphs.find(key);
     if (it != lane.graphs.end()) return it->second;
     cudaGraph_t g = nullptr;
     ck(cudaGraphCreate(&g, 0), "cudaGraphCreate");
     Graph gr;
-    gr.bucket = bucket;
+    gr.bands = bands;
     try {
         cudaKernelNodeParams kp;
         localize_node(P, bucket, kp);
@@ -279,10 +283,21 @@ Server::Graph &Server::GraphFor(Lane &lane, int inst, int bucket, const TrackPar
         lane.a_count = bucket;
         lane.a_res = lane.d_res;
         kp.kernelParams = lane.args;
-        ck(cudaGraphAddKernelNode(&gr.kernel, g, nullptr, 0, &kp), "cudaGraphAddKernelNode");
+        cudaGraphNode_t prev = nullptr;
+        for (int b = 0; b < bands; b++) {
+            if (bands > 1) {
+                cudaGraphNode_t wait;
+                ck(cudaGraphAddEventWaitNode(&wait, g, prev ? &prev : nullptr, prev ? 1 : 0, lane.band_done[b]),
+                   "cudaGraphAddEventWaitNode");
+                prev = wait;
+            }
+            ck(cudaGraphAddKernelNode(&gr.kernel[b], g, prev ? &prev : nullptr, prev ? 1 : 0, &kp),
+               "cudaGraphAddKernelNode");
+            prev = gr.kernel[b];
+        }
         cudaGraphNode_t copy;
-        ck(cudaGraphAddMemcpyNode1D(&copy, g, &gr.kernel, 1, lane.h_res, lane.d_res,
-                                    sizeof(LocalizationResult) * bucket, cudaMemcpyDeviceToHost),
+        ck(cudaGraphAddMemcpyNode1D(&copy, g, &prev, 1, lane.h_res, lane.d_res, sizeof(LocalizationResult) * bucket,
+                                    cudaMemcpyDeviceToHost),
            "cudaGraphAddMemcpyNode1D");
         ck(cudaGraphInstantiate(&gr.exec, g, 0), "cudaGraphInstantiate");
     } catch (...) {
@@ -298,7 +313,7 @@ Server::Graph &Server::GraphFor(Lane &lane, int inst, int bucket, const TrackPar
 // immutable submission fields. The requests' row bands are stacked in the lane at one pitch. A
 // batch of a few MiB or less is one copy plus a graph replay (kernel + result copy). A larger one
 // is split by rows into up to kMaxBands bands of about kBandBytes, copied in order on the lane's
-// copy stream; the kernel of band b runs on the lane stream as soon as band b has arrived, over a
+// copy stream, and its graph runs the kernel of band b as soon as band b has arrived, over a
 // prefix of the ROIs (in submission order) that lies inside the rows copied so far, so the
 // kernels overlap the later copies and only the last band's kernel is left after the batch has
 // crossed PCIe. Every ROI is computed the same way in either form.
@@ -361,42 +376,24 @@ void Server::LaunchBatch(Lane &lane, Tracker *t, const std::vector<Request *> &b
     }
     TrackParams P = t->AcquireLaunch(pdt, lane.stream);
     P.mode &= ~(kLT_ZMatchBF16 | kLT_JointRefine);  // the graph holds the localization kernel alone
+    int bucket = 32;
+    while (bucket < k) bucket <<= 1;
+    Graph &g = GraphFor(lane, batch[0]->inst, bucket, nb, P);
     lane.P = P;
     lane.a_pix = lane.d_pix;
     lane.a_pitch = (int)pitch;
     lane.a_stride = 0;
-    if (nb > 1) {
-        for (int b = 0; b < nb; b++) {
-            ck(cudaStreamWaitEvent(lane.stream, lane.band_done[b], 0), "cudaStreamWaitEvent");
-            lane.a_off = lane.d_off + m[b];
-            lane.a_jobs = lane.d_jobs + m[b];
-            lane.a_count = m[b + 1] - m[b];
-            lane.a_res = lane.d_res + m[b];
-            cudaKernelNodeParams kp;
-            localize_node(P, lane.a_count, kp);
-            ck(cudaLaunchKernel(kp.func, kp.gridDim, kp.blockDim, lane.args, kp.sharedMemBytes, lane.stream),
-               "localize launch");
-        }
-        ck(cudaMemcpyAsync(lane.h_res, lane.d_res, sizeof(LocalizationResult) * k, cudaMemcpyDeviceToHost, lane.stream),
-           "D2H results");
-    } else {
-        int bucket = 32;
-        while (bucket < k) bucket <<= 1;
-        Graph &g = GraphFor(lane, batch[0]->inst, bucket, P);
-        lane.P = P;
-        lane.a_pix = lane.d_pix;
-        lane.a_pitch = (int)pitch;
-        lane.a_stride = 0;
-        lane.a_off = lane.d_off;
-        lane.a_jobs = lane.d_jobs;
-        lane.a_count = k;
-        lane.a_res = lane.d_res;
+    for (int b = 0; b < nb; b++) {
+        lane.a_off = lane.d_off + m[b];
+        lane.a_jobs = lane.d_jobs + m[b];
+        lane.a_count = m[b + 1] - m[b];
+        lane.a_res = lane.d_res + m[b];
         cudaKernelNodeParams kp;
-        localize_node(P, k, kp);  // grid for k ROIs; same function and shared memory as the graph's node
-        kp.kernelParams = lane.args;
-        ck(cudaGraphExecKernelNodeSetParams(g.exec, g.kernel, &kp), "cudaGraphExecKernelNodeSetParams");
-        ck(cudaGraphLaunch(g.exec, lane.stream), "cudaGraphLaunch");
+        localize_node(P, lane.a_count, kp);  // same function and shared memory as the graph's node
+        kp.kernelParams = lane.args;          // the argument values are copied here
+        ck(cudaGraphExecKernelNodeSetParams(g.exec, g.kernel[b], &kp), "cudaGraphExecKernelNodeSetParams");
     }
+    ck(cudaGraphLaunch(g.exec, lane.stream), "cudaGraphLaunch");
     ck(cudaEventRecord(lane.done, lane.stream), "cudaEventRecord");
     lane.count = k;
 }

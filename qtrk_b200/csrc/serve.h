@@ -57,13 +57,14 @@ class Server {
         bool done = false, failed = false;
         std::vector<LocalizationResult> results;
     };
+    static constexpr int kMaxBands = 4;
     struct Graph {
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
-        cudaGraphNode_t kernel = nullptr;
+        cudaGraphNode_t kernel[kMaxBands] = {};  // one localization kernel per row band
+        int bands = 1;
         int bucket = 0;
     };
-    static constexpr int kMaxBands = 4;
     struct Lane {
         cudaStream_t stream = nullptr;
         cudaEvent_t done = nullptr;
@@ -93,7 +94,7 @@ class Server {
     void Run();                                   // dispatcher thread
     void LaunchBatch(Lane &lane, Tracker *t, const std::vector<Request *> &batch);
     void Fail(const std::vector<int64_t> &ids);  // mark requests done without results
-    Graph &GraphFor(Lane &lane, int inst, int bucket, const TrackParams &P);
+    Graph &GraphFor(Lane &lane, int inst, int bucket, int bands, const TrackParams &P);
     void Complete(Lane &lane);
     void Release();  // free every lane (destructor, failed constructor)
 
