@@ -761,38 +761,39 @@ def main(argv=None) -> int:
 
     res_dev = np.frombuffer(d_res.cpu().numpy().tobytes(), dtype=abi.RESULT_DTYPE)
 
-    # ---- the same steps with the tensor-core Z match (BF16 cross term, exact re-score) ----
+    # ---- the same steps with the tensor-core Z match (BF16 or TF32 cross term, exact re-score) ----
     methods = {"plain_fp32": {"rois_per_s": value, "ms_per_step": dev_ms_max / args.steps,
                               "max_dxy_nm_vs_plain": 0.0, "max_dz_planes_vs_plain": 0.0}}
     launches_tc = 0
     if not args.ncu:
-        trk.SetLocalizationMode(wl.mode | abi.LT_B200_ZMatchBF16)
         d_res_tc = torch.empty_like(d_res)
-        l0 = trk.KernelLaunchCount()
+        for name, bit in (("tensor_core_bf16", abi.LT_B200_ZMatchBF16), ("tensor_core_tf32", abi.LT_B200_ZMatchTF32)):
+            trk.SetLocalizationMode(wl.mode | bit)
+            l0 = trk.KernelLaunchCount()
 
-        def tc_step():
-            trk.LocalizeDevice(d_rois.data_ptr(), 200, 20000, abi.QTrkU16, N_ROIS, d_res_tc.data_ptr(),
-                               stream=stream.cuda_stream)
+            def tc_step():
+                trk.LocalizeDevice(d_rois.data_ptr(), 200, 20000, abi.QTrkU16, N_ROIS, d_res_tc.data_ptr(),
+                                   stream=stream.cuda_stream)
 
-        for _ in range(args.warmup):
-            tc_step()
-        steps_tc = max(1, min(args.steps, 50))
-        barrier()
-        torch.cuda.synchronize(dev)
-        ev0.record(stream)
-        for _ in range(steps_tc):
-            tc_step()
-        ev1.record(stream)
-        torch.cuda.synchronize(dev)
-        barrier()
-        tc_ms = max_over_ranks(ev0.elapsed_time(ev1))
-        launches_tc = trk.KernelLaunchCount() - l0
-        res_tc = np.frombuffer(d_res_tc.cpu().numpy().tobytes(), dtype=abi.RESULT_DTYPE)
-        methods["tensor_core_bf16"] = {
-            "rois_per_s": replicas.aggregate_rate(N_ROIS * steps_tc, ws, tc_ms / 1e3),
-            "ms_per_step": tc_ms / steps_tc,
-            "max_dxy_nm_vs_plain": float(np.abs(res_tc["pos"][:, :2] - res_dev["pos"][:, :2]).max() * PIXEL_NM),
-            "max_dz_planes_vs_plain": float(np.abs(res_tc["pos"][:, 2] - res_dev["pos"][:, 2]).max())}
+            for _ in range(args.warmup):
+                tc_step()
+            steps_tc = max(1, min(args.steps, 50))
+            barrier()
+            torch.cuda.synchronize(dev)
+            ev0.record(stream)
+            for _ in range(steps_tc):
+                tc_step()
+            ev1.record(stream)
+            torch.cuda.synchronize(dev)
+            barrier()
+            tc_ms = max_over_ranks(ev0.elapsed_time(ev1))
+            launches_tc += trk.KernelLaunchCount() - l0
+            res_tc = np.frombuffer(d_res_tc.cpu().numpy().tobytes(), dtype=abi.RESULT_DTYPE)
+            methods[name] = {
+                "rois_per_s": replicas.aggregate_rate(N_ROIS * steps_tc, ws, tc_ms / 1e3),
+                "ms_per_step": tc_ms / steps_tc,
+                "max_dxy_nm_vs_plain": float(np.abs(res_tc["pos"][:, :2] - res_dev["pos"][:, :2]).max() * PIXEL_NM),
+                "max_dz_planes_vs_plain": float(np.abs(res_tc["pos"][:, 2] - res_dev["pos"][:, 2]).max())}
         trk.SetLocalizationMode(wl.mode)
     ok = {k: m for k, m in methods.items() if m["max_dxy_nm_vs_plain"] <= 1.0}
     chosen = max(ok, key=lambda k: ok[k]["rois_per_s"])

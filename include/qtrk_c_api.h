@@ -61,6 +61,7 @@ enum LocalizeModeEnum {
     LT_B200_ZMatchBF16 = 1 << 20,    /* Z cross term on the tensor cores (BF16, FP32 accumulate) */
     LT_B200_JointRefine = 1 << 21,   /* joint Gauss-Newton (x,y,z) refinement after the Z fit */
     LT_B200_Gaussian5P = 1 << 22,    /* 5-parameter (x,y,I0,bg,sigma) full-Newton Gaussian MLE */
+    LT_B200_ZMatchTF32 = 1 << 23,    /* Z cross term on the tensor cores with TF32 operands (FP32 accumulate) */
     LT_Force32Bit = (int)0xffffffff
 };
 typedef int LocMode_t;
@@ -332,7 +333,7 @@ QTRK_API void QTRK_CALLCONV QTrkB200RefineZLUT(struct QueuedTracker *qtrk, const
  * cudaMalloc/cudaFree take the driver's allocation lock and can synchronize the device, and
  * processes whose device-memory budget is fixed at start-up. Same arguments, results and
  * kernels as QTrkB200LocalizeDevice; the intermediate profiles of the tensor-core Z match
- * (LT_B200_ZMatchBF16) go to one fixed 16 MiB array inside the library, which every GPU that
+ * (LT_B200_ZMatchBF16 / LT_B200_ZMatchTF32) go to one fixed 16 MiB array inside the library, which every GPU that
  * loads the library holds until the process exits.
  * Limit: count * (4 * zlut_radialsteps + 4 * zlut_radialsteps rounded up to 16) bytes (plus up
  * to 255 bytes of alignment) must fit in 16 MiB: 32,768 ROIs of 64 radial bins. Larger counts
@@ -419,10 +420,12 @@ QTRK_API struct ResultManager *QTRK_CALLCONV QTrkB200RMCreateNamed(const char *f
  * admits waiting frames to free lanes in arrival order, merges waiting frames of the same
  * instance and pixel type into one launch while they fit the lane (continuous batching), copies
  * each frame's ROI band to the lane and replays a CUDA graph holding the localization kernel and
- * the result copy (one graph per lane, instance and power-of-two ROI-count bucket). A frame's
+ * the result copy (one graph per lane, instance, power-of-two ROI-count bucket and band count: a
+ * batch above ~6 MiB is copied in up to four row bands, each band's kernel starting as its rows
+ * arrive). A frame's
  * results are the ones QTrkScheduleFrame gives for it: ROIs outside the frame are skipped and
  * result i carries zlutIndex = i + job->zlutIndex. The graphs hold the plain Z match: the tensor-core
- * match and the joint refinement (LT_B200_ZMatchBF16, LT_B200_JointRefine) are not applied here.
+ * match and the joint refinement (LT_B200_ZMatchBF16/TF32, LT_B200_JointRefine) are not applied here.
  */
 typedef struct QTrkB200ServeStats {
     int64_t frames;            /* frames completed */

@@ -26,6 +26,7 @@ LT_LocalizeZWeighted = 512
 LT_B200_ZMatchBF16 = 1 << 20
 LT_B200_JointRefine = 1 << 21
 LT_B200_Gaussian5P = 1 << 22
+LT_B200_ZMatchTF32 = 1 << 23
 
 # Pixel data types, cputrack/qtrk_c_api.h:24-29
 QTrkU8, QTrkU16, QTrkFloat = 0, 1, 2

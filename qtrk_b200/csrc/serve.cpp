@@ -375,7 +375,7 @@ void Server::LaunchBatch(Lane &lane, Tracker *t, const std::vector<Request *> &b
         if (nb > 1) ck(cudaEventRecord(lane.band_done[b], cs), "cudaEventRecord");
     }
     TrackParams P = t->AcquireLaunch(pdt, lane.stream);
-    P.mode &= ~(kLT_ZMatchBF16 | kLT_JointRefine);  // the graph holds the localization kernel alone
+    P.mode &= ~(kLT_ZMatchBF16 | kLT_ZMatchTF32 | kLT_JointRefine);  // the graph holds the localization kernel alone
     int bucket = 32;
     while (bucket < k) bucket <<= 1;
     Graph &g = GraphFor(lane, batch[0]->inst, bucket, nb, P);

@@ -29,6 +29,7 @@ enum : int {
     kLT_ZMatchBF16 = 1 << 20,
     kLT_JointRefine = 1 << 21,
     kLT_Gaussian5P = 1 << 22,
+    kLT_ZMatchTF32 = 1 << 23,
 };
 
 struct TrackParams {

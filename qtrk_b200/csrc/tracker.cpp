@@ -809,7 +809,7 @@ void Tracker::SubmitLocked(int idx)
 
 bool Tracker::UseTensorCoreMatch() const
 {
-    return (mode_ & LT_B200_ZMatchBF16) && (mode_ & LT_LocalizeZ) && d_lut_ && lut_count_ > 0 &&
+    return (mode_ & (LT_B200_ZMatchBF16 | LT_B200_ZMatchTF32)) && (mode_ & LT_LocalizeZ) && d_lut_ && lut_count_ > 0 &&
            lut_planes_ > 0 && zmatch_supported(cfg.zlut_radialsteps) && !cmp_enabled_;
 }
 
@@ -847,6 +847,7 @@ ZMatchParams Tracker::TensorCoreParams() const
     Q.lut = d_lut_;
     Q.weights = have_zw_ ? d_zw_ : nullptr;
     Q.error_flag = d_err_;
+    Q.tf32 = (mode_ & LT_B200_ZMatchTF32) ? 1 : 0;
     Q.zbias = d_zbias_;
     Q.zbias_w = zbias_w_;
     Q.zbias_count = zbias_count_;

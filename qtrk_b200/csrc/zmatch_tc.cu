@@ -16,7 +16,9 @@
 // + O(2^-16 x)) and the cross term is p_hi.L_hi + p_hi.L_lo + p_lo.L_hi (three MMAs per K
 // slice, all accumulated in the same FP32 tensor-memory tile), which brings the error bound
 // down to d_k = 2^-9 |p'| |L'_k| (a generous cover of the ~3 2^-16 split error plus the FP32
-// accumulation of 3 K products), so only a few planes per ROI need the exact re-score. Threads
+// accumulation of 3 K products), so only a few planes per ROI need the exact re-score. With
+// LT_B200_ZMatchTF32 the operands are w p and w L rounded to TF32 (kind::tf32, K = 8 per MMA,
+// one MMA per K step) and d_k = 2^-9 (1.02) |p'| |L'_k| (kBoundScaleTF32). Threads
 // record those candidate planes from their TMEM rows; warps then compute the exact scores with
 // the plain path's per-plane function (zlut_score: one lane per plane, bins in order), take the
 // argmax and run the 7-point fit (LsqQuadraticFit.h:132-176) with the plain path's warp code, so z
@@ -41,6 +43,11 @@ namespace {
 constexpr int kTileM = 128;
 constexpr int kMaxN = 256;   // N per tcgen05.mma (M = 128 allows N <= 256 in steps of 16)
 constexpr float kBoundScale = 0.001953125f;  // 2^-9 (see above)
+// TF32 operands, rounded to nearest (cvt.rna) when staged: 10 explicit mantissa bits, each factor
+// within 2^-11, so a product within 2^-10 + 2^-22; with the FP32 accumulation of <= 128 products
+// (2^-17) and the FP32 rounding of w p and w L, |d(p'.L'_k)| <= (2^-10 + 2^-16) |p'| |L'_k|, and
+// s_k = 2 p'.L'_k - |L'_k|^2 is within 2^-9 (1.016) |p'| |L'_k|; the scale below covers it.
+constexpr float kBoundScaleTF32 = 0.0020f;
 constexpr int kTmemCols = 256;
 constexpr uint32_t kWaitLimit = 1u << 20;  // try_wait polls before the kernel gives up
 constexpr int kMaxCand = 16;  // candidate planes kept per ROI; more fall back to scoring every plane
@@ -52,6 +59,14 @@ constexpr int kWarps = kTileM / 32;
 constexpr int kTailBytes = 16 + kTileM * 4 + kTileM * 4 + kTileM * kMaxCand * 2 + kWarps * 8 * 8;
 
 __device__ const float kZLUTWeightsTC[7] = {0.15f, 0.5f, 0.85f, 1.0f, 0.85f, 0.5f, 0.15f};
+
+// x rounded to TF32 (round to nearest, ties away from zero), as a 32-bit pattern
+__device__ __forceinline__ uint32_t to_tf32(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
@@ -71,11 +86,13 @@ __device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint
     return d;
 }
 
-// Instruction descriptor for kind::f16: FP32 accumulate (bits 4-5 = 1), A and B BF16 (bits
-// 7-9 = 1, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
-__device__ __forceinline__ uint32_t make_idesc(int M, int N)
+// Instruction descriptor for kind::f16 / kind::tf32: FP32 accumulate (bits 4-5 = 1), A and B
+// format in bits 7-9 and 10-12 (1 = BF16, 2 = TF32), both K-major, N >> 3 at bit 17, M >> 4 at
+// bit 24.
+__device__ __forceinline__ uint32_t make_idesc(int M, int N, bool tf32)
 {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+    const uint32_t fmt = tf32 ? 2u : 1u;
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -85,6 +102,17 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
         :
         : "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
@@ -139,6 +167,10 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
     const int start = tile.x, m = tile.y, bead = tile.z;
     const int tid = threadIdx.x, warp = tid >> 5;
     const int nbp = Q.nbp, kchunks = nbp >> 3, sbo = nbp * 16;
+    // TF32: 4 elements per 16-byte chunk; A spans the A_hi and A_lo space, B the B_hi and B_lo space
+    const bool tf32 = Q.tf32 != 0;
+    const int kch32 = nbp >> 2, sbo32 = nbp * 32;
+    const int nb = Q.nb;
     // [A_hi | A_lo | B_hi | B_lo], each in the no-swizzle K-major core-matrix layout
     uint8_t *sA = smem;
     uint8_t *sAl = sA + kTileM * nbp * 2;
@@ -162,11 +194,25 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
 
-    // A: this tile's BF16 weighted profiles (rows beyond m are zero)
+    // A: this tile's weighted profiles, BF16 hi/lo or FP32 (rows beyond m are zero)
     const bool valid_bead = bead >= 0 && bead < Q.lut_count;
     int my_roi = -1;
     if (tid < m) my_roi = Q.perm ? Q.perm[start + tid] : start + tid;
-    for (int idx = tid; idx < kTileM * kchunks; idx += kTileM) {
+    for (int idx = tid; tf32 && idx < kTileM * kch32; idx += kTileM) {
+        const int r = idx / kch32, c = idx - r * kch32;
+        float e[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        if (r < m) {
+            const int roi = Q.perm ? Q.perm[start + r] : start + r;
+            const float *pr = Q.prof_f32 + (size_t)roi * nb;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int b = 4 * c + j;
+                if (b < nb) e[j] = Q.weights ? pr[b] * Q.weights[b] : pr[b];
+            }
+        }
+        store_chunk(sA, r, c, sbo32, make_uint4(to_tf32(e[0]), to_tf32(e[1]), to_tf32(e[2]), to_tf32(e[3])));
+    }
+    for (int idx = tid; !tf32 && idx < kTileM * kchunks; idx += kTileM) {
         const int r = idx / kchunks, c = idx - r * kchunks;
         uint4 vh = make_uint4(0, 0, 0, 0), vl = vh;
         if (r < m) {
@@ -181,7 +227,6 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
 
     // |p'| of each row's ROI (FP32 profile times the radial weights), one warp per row, lanes over
     // bins; FP64 sums rounded up by 2^-20 so that the bound below stays a bound
-    const int nb = Q.nb;
     const float *prof = (my_roi >= 0) ? Q.prof_f32 + (size_t)my_roi * nb : nullptr;
     for (int r = warp; r < kTileM; r += kWarps) {
         double s2 = 0.0;
@@ -203,16 +248,30 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
     const float *lut = Q.lut + (size_t)gb * Q.planes * nb;
     const float *lnorm = Q.lut_norm + (size_t)gb * Q.planes_pad;
 
-    float smax = -INFINITY, dmax = 0.0f;  // BF16 maximum so far and its error bound
+    float smax = -INFINITY, dmax = 0.0f;  // tensor-core maximum so far and its error bound
+    const float bscale = tf32 ? kBoundScaleTF32 : kBoundScale;
     bool failed = false;
     uint32_t parity = 0;
     const int planes_pad = Q.planes_pad;
     for (int n0 = 0; n0 < planes_pad; n0 += kMaxN) {
         const int n = min(kMaxN, planes_pad - n0);
-        // LUT layout [bead][hi, lo][planes_pad][nbp]
+        // TF32: w L from the FP32 LUT (planes beyond the LUT and bins beyond nb are zero)
+        for (int idx = tid; tf32 && idx < n * kch32; idx += kTileM) {
+            const int r = idx / kch32, c = idx - r * kch32, k = n0 + r;
+            float e[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            if (k < Q.planes) {
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int b = 4 * c + j;
+                    if (b < nb) e[j] = Q.weights ? lut[(size_t)k * nb + b] * Q.weights[b] : lut[(size_t)k * nb + b];
+                }
+            }
+            store_chunk(sB, r, c, sbo32, make_uint4(to_tf32(e[0]), to_tf32(e[1]), to_tf32(e[2]), to_tf32(e[3])));
+        }
+        // BF16 LUT layout [bead][hi, lo][planes_pad][nbp]
         const __nv_bfloat16 *lutb = Q.lut_bf16 + ((size_t)gb * 2 * planes_pad + n0) * nbp;
         const __nv_bfloat16 *lutl = lutb + (size_t)planes_pad * nbp;
-        for (int idx = tid; idx < n * kchunks; idx += kTileM) {
+        for (int idx = tid; !tf32 && idx < n * kchunks; idx += kTileM) {
             const int r = idx / kchunks, c = idx - r * kchunks;
             store_chunk(sB, r, c, sbo, *reinterpret_cast<const uint4 *>(lutb + (size_t)r * nbp + c * 8));
             store_chunk(sBl, r, c, sbo, *reinterpret_cast<const uint4 *>(lutl + (size_t)r * nbp + c * 8));
@@ -223,9 +282,12 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
         const uint32_t tmem = *tslot;
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t idesc = make_idesc(kTileM, n);
+            const uint32_t idesc = make_idesc(kTileM, n, tf32);
             const uint32_t a0 = smem_u32(sA), al = smem_u32(sAl), b0 = smem_u32(sB), bl = smem_u32(sBl);
-            for (int k = 0; k < (nbp >> 4); k++) {
+            // TF32: K = 8 per MMA (32 bytes, two core matrices), one MMA per K step
+            for (int k = 0; tf32 && k < (nbp >> 3); k++)
+                mma_tf32(tmem, make_desc(a0 + k * 256, 128, sbo32), make_desc(b0 + k * 256, 128, sbo32), idesc, k > 0);
+            for (int k = 0; !tf32 && k < (nbp >> 4); k++) {
                 const uint64_t ah = make_desc(a0 + k * 256, 128, sbo), alo = make_desc(al + k * 256, 128, sbo);
                 const uint64_t bh = make_desc(b0 + k * 256, 128, sbo), blo = make_desc(bl + k * 256, 128, sbo);
                 mma_bf16(tmem, ah, bh, idesc, k > 0);
@@ -260,7 +322,7 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
                     const float sk = 2.0f * v[j] - lnorm[k];
                     if (sk > smax) {
                         smax = sk;
-                        dmax = kBoundScale * pnorm * sqrtf(lnorm[k]);
+                        dmax = bscale * pnorm * sqrtf(lnorm[k]);
                     }
                 }
             }
@@ -277,7 +339,7 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
                     const int k = n0 + c0 + j;
                     if (k >= Q.planes) continue;
                     const float sk = 2.0f * v[j] - lnorm[k];
-                    const float dk = kBoundScale * pnorm * sqrtf(lnorm[k]);
+                    const float dk = bscale * pnorm * sqrtf(lnorm[k]);
                     const float thr = smax - dmax - dk - 1e-5f * (1.0f + fabsf(smax));
                     if (sk >= thr) {
                         if (nc < kMaxCand) s_cand[tid * kMaxCand + nc] = (short)k;

@@ -1,4 +1,4 @@
-// Tensor-core (tcgen05, BF16 in / FP32 accumulate) Z-LUT match; see zmatch_tc.cu.
+// Tensor-core (tcgen05, BF16 or TF32 in / FP32 accumulate) Z-LUT match; see zmatch_tc.cu.
 #pragma once
 #include <cstdint>
 #include <cuda_bf16.h>
@@ -29,6 +29,7 @@ struct ZMatchParams {
     const float *zbias;              // Z-LUT bias table [zbias_count][zbias_w] or nullptr
     int zbias_w, zbias_count;
     unsigned *error_flag;            // set to 1 if an MMA completion wait gave up
+    int tf32;                        // 1: TF32 operands (w p and w L in FP32), one MMA per K step
 };
 
 int zmatch_padded_bins(int nb);
