@@ -460,17 +460,24 @@ def workloads_bench(dev, steps: int, warmup: int) -> dict:
         t.SetLocalizationMode(synth.MODE_QI_Z)
         t.SetRadialZLUTSize(nbeads, planes)
         l0 = t.KernelLaunchCount()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        t.BeginLUT(abi.BUILDLUT_NORMALIZE)
-        for k in range(planes):
-            t.BuildLUT(hs[k], k)
-        t.FinalizeLUT()
-        lut = t.GetRadialZLUT()  # waits for the LUT
-        build_s = time.perf_counter() - t0
+        times = []
+        for _ in range(2):  # the first build also allocates the instance's staging buffers
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            t.BeginLUT(abi.BUILDLUT_NORMALIZE)
+            for k in range(planes):
+                t.BuildLUT(hs[k], k)
+            t.FinalizeLUT()
+            lut = t.GetRadialZLUT()  # waits for the LUT
+            times.append(time.perf_counter() - t0)
+        d_plane = torch.empty_like(d_stack[0])
+        copy_ms = _timed(stream, lambda: d_plane.copy_(host[0], non_blocking=True), 20, 3)
         out["buildlut_256x200_80x80_u16"] = {
-            "workload": "BeginLUT / 200 x BuildLUT(256 ROIs 80x80 u16 from pinned host memory) / FinalizeLUT",
-            "rois_per_s": nbeads * planes / build_s, "seconds": build_s, "lut_shape": list(lut.shape)}
+            "workload": "BeginLUT / 200 x BuildLUT(256 ROIs 80x80 u16 from pinned host memory) / FinalizeLUT, "
+                        "second build on the instance",
+            "rois_per_s": nbeads * planes / times[1], "seconds": times[1], "first_build_seconds": times[0],
+            "copy_bound_rois_per_s": nbeads / (copy_ms / 1e3), "lut_shape": list(lut.shape)}
+        del d_plane
         flat = d_stack.view(-1, 80, 80)
         xyz = torch.zeros(nbeads * planes, 3, device=dev)
         xyz[:, 0] = 40.0
