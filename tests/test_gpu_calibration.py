@@ -106,3 +106,33 @@ def test_removing_calibration_restores_plain_results(roi60):
     assert not np.array_equal(cal["pos"], plain["pos"])
     for f in ("pos", "firstGuess", "error", "imageMean"):
         assert np.array_equal(again[f], plain[f]), f
+
+
+def test_calibration_through_schedule_frame_equals_per_roi(roi60):
+    """Frame path (ROIs cropped from frame rows at a pitch on the device) with calibration images
+    gives the same results as queuing the same ROIs one by one: ScheduleFrame gives ROI i the
+    images of bead i (zlutIndex = i, QueuedTracker.cpp:105)."""
+    wl, lut1, _ = roi60
+    n = 12
+    rois = wl.rois[:n]
+    off, gain = _calibration(rois.shape[1:], 47)
+    off = np.ascontiguousarray(np.concatenate([off] * 4))[:n]
+    gain = np.ascontiguousarray(np.concatenate([gain] * 4))[:n]
+    lut = np.ascontiguousarray(np.concatenate([lut1[:1]] * n))
+    gap, h, w = 3, rois.shape[1], rois.shape[2]
+    frame = np.zeros((3 * (h + gap) + gap, 4 * (w + gap) + gap), np.float32)
+    pos = []
+    for i in range(n):
+        y, x = gap + (i // 4) * (h + gap), gap + (i % 4) * (w + gap)
+        frame[y:y + h, x:x + w] = rois[i]
+        pos.append((x, y))
+    with QTrkInstance(wl.settings) as t:
+        t.SetRadialZLUT(lut)
+        t.SetLocalizationMode(wl.mode)
+        t.SetPixelCalibrationImages(off, gain)
+        assert t.ScheduleFrame(frame, np.array(pos, np.int32)) == n
+        fr = t.WaitForResults(n)
+        fr = fr[np.argsort(fr["zlutIndex"])]
+        single = t.Localize(rois, zlut_index=np.arange(n))
+    for f in ("pos", "firstGuess", "error", "imageMean"):
+        assert np.array_equal(fr[f], single[f]), f
