@@ -325,3 +325,26 @@ def test_full_size_roi100_properties(ref):
     check_results(r[sample], r_ref["pos"], r_ref["firstGuess"], r_ref["error"])
     assert np.median(np.abs(r["pos"][:, 0] - wl.true_xyz[:, 0])) < 0.1
     assert np.median(np.abs(r["pos"][:, 2] - wl.true_xyz[:, 2])) < 1.0
+
+
+@pytest.mark.parametrize("w,h", [(47, 33), (16, 16), (200, 200)])
+def test_ragged_and_extreme_roi_sizes_match_reference(ref, w, h):
+    """Non-square odd-sized, minimal and large ROIs (the largest here takes 166 KB of shared memory
+    per block and the shared-memory FFT of 256 points) with the reference's default radial and
+    angular coverage, COM + QI + Z, against the reference tracker."""
+    s = abi.settings(width=w, height=h, qi_iterations=4, qi_minradius=1.0, zlut_minradius=1.0)
+    rng = np.random.Generator(np.random.PCG64(w * 1000 + h))
+    n, planes = 40, 30
+    cx = w / 2 + rng.uniform(-1.5, 1.5, n)
+    cy = h / 2 + rng.uniform(-1.5, 1.5, n)
+    z = rng.uniform(4, planes - 4, n)
+    rois = rng.poisson(synth.render(w, h, cx, cy, z * (h / 60.0), 10.0, 100.0)).astype(np.float32)
+    kz = np.arange(planes, dtype=np.float64) * (h / 60.0)
+    stack = synth.render(w, h, np.full(planes, w / 2), np.full(planes, h / 2), kz, 10.0, 100.0).astype(np.float32)
+    known = np.array([[w / 2, h / 2]], np.float32)
+    mode = synth.MODE_QI_Z
+    lut = ref.build_lut(s, stack[:, None], abi.BUILDLUT_NORMALIZE, known_pos=known)
+    r_ref = ref.track(s, mode, rois, lut)
+    with make_tracker(s, mode, lut) as t:
+        r = t.Localize(rois)
+    check_results(r, r_ref["pos"], r_ref["firstGuess"], r_ref["error"], r_ref["imageMean"])
