@@ -329,9 +329,10 @@ def test_full_size_roi100_properties(ref):
 
 @pytest.mark.parametrize("w,h", [(47, 33), (16, 16), (200, 200)])
 def test_ragged_and_extreme_roi_sizes_match_reference(ref, w, h):
-    """Non-square odd-sized, minimal and large ROIs (the largest here takes 166 KB of shared memory
-    per block and the shared-memory FFT of 256 points) with the reference's default radial and
-    angular coverage, COM + QI + Z, against the reference tracker."""
+    """Non-square odd-sized, minimal and large ROIs with the reference's default radial and angular
+    coverage, COM + QI + Z, against the reference tracker. 47x33: QI and Z radii (23 px) beyond the
+    short side, so many samples fall outside; 16x16: a 32-point QI FFT; 200x200: 256 radial steps
+    (a 512-point QI FFT), 297 Z bins and ~173 KB of shared memory per block."""
     s = abi.settings(width=w, height=h, qi_iterations=4, qi_minradius=1.0, zlut_minradius=1.0)
     rng = np.random.Generator(np.random.PCG64(w * 1000 + h))
     n, planes = 40, 30
