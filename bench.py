@@ -132,6 +132,23 @@ def crlb_gauss_workload(wl, res: np.ndarray, m: int = 5000) -> dict:
             "x_error_over_crlb": ratio}
 
 
+def host_cpu() -> dict:
+    """The host CPU the baseline ran on: model name (from /proc/cpuinfo) and usable threads."""
+    model = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    try:
+        nproc = len(os.sched_getaffinity(0))
+    except AttributeError:
+        nproc = os.cpu_count() or 1
+    return {"model": model, "threads_available": nproc}
+
+
 def workload_config(ws: int) -> dict:
     """The `config` of the bench line, the same for this library's arm and the reference arm."""
     return {"workload": "10,000 ROIs/step of 100x100 u16; COM + QI (4 it, 64 radial x 51 angular per quadrant) + "
@@ -669,7 +686,7 @@ def run_reference_arm(args) -> int:
         "warmup": args.warmup, "ms_per_step": 1e3 * args.sample / value, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(ws),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "host": host_cpu(),
                          "sample": f"{args.sample} ROIs per step of the same seeded workload, QueuedCPUTracker "
                                    f"with numThreads=-1"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -943,7 +960,7 @@ def main(argv=None) -> int:
         r = cpu_reference_run(wl, lut, args.sample)
         if r is not None:
             rate, ref_res, cores = r
-            cpu_baseline = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
+            cpu_baseline = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference", "host": host_cpu(),
                             "sample": f"first {args.sample} ROIs of the same workload, reference QueuedCPUTracker "
                                       f"(oracle/_ref) with numThreads=-1"}
             one = cpu_reference_run(wl, lut, min(args.sample, 500), threads=1)
