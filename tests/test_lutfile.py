@@ -1,14 +1,17 @@
 """.radialzlut files: round trip through the C ABI, and ReadLUTFile's per-bead reading
 (cputrack/utils.cpp:680-710) of the reference's own fixture files."""
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
 import pytest
 
+from build import DEFAULT_REFERENCE  # oracle/build.py: where the reference tree is read from
 from qtrk_b200 import lutfile
 
-FIXTURES = [Path("/root/reference/cputrack-test/10x.radialzlut"), Path("/root/reference/cputrack-test/zrange/long.radialzlut")]
+_REF = Path(os.environ.get("QTRK_REFERENCE", DEFAULT_REFERENCE))
+FIXTURES = [_REF / "cputrack-test" / "10x.radialzlut", _REF / "cputrack-test" / "zrange" / "long.radialzlut"]
 
 
 def test_round_trip(tmp_path, qlib):
