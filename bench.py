@@ -11,13 +11,20 @@ FP32 profiles, FP64-accumulated scores) and the 7-point quadratic fit.
             The stack (200 MB) is larger than L2 (126 MB), so every step streams from HBM.
 * e2e     — ROIs/s through the public C ABI with host buffers: per step QTrkScheduleFrame
             of a pinned 10000x10000 u16 frame holding the 10,000 ROIs (host->device copy
-            inside the timed region), QTrkFlush, and QTrkFetchResults of all results
-            (device->host copy inside).
+            inside the timed region), QTrkFlush, and QTrkFetchResults of a frame's 10,000
+            results (device->host copy inside), with one frame in flight as an acquisition
+            loop runs it (frame k+1 is handed over before frame k's results are read; the
+            timed region ends after the last frame's results). The one-frame-at-a-time rate
+            and the box's plain pinned copy rate of the frame are reported beside it.
 * roofline — the localization kernel's algorithmic bytes (20,081 B per ROI: pixels +
             job + result + LUT share) per launch / its mean launch time, against the
             measured HBM copy bandwidth.
 * cpu_baseline — the reference's own CPU tracker (oracle/_ref, QueuedCPUTracker with
-            all host threads) on a bounded sample of the same workload.
+            all host threads, and with one) on a bounded sample of the same workload.
+* methods — the same device-resident steps with the tensor-core Z match (BF16 and TF32
+            operands); `chosen` is the fastest form within 1 nm of the plain one.
+* serving, workloads — the request server (paced and saturated) and the other workloads
+            (Gaussian MLE, BuildLUT, adjoint, LUT refinement), rank 0 at N=1 only.
 
 `--impl reference` times the reference CPU tracker alone and prints its line.
 Multi-GPU (torchrun): replicas; every rank localizes its own 10,000 ROIs, no collective
