@@ -39,3 +39,30 @@ def test_robust_sigma_of_a_normal_sample():
     e = np.random.Generator(np.random.PCG64(1)).normal(0, 0.3, 200000)
     e[:100] = np.nan
     assert abs(bench._robust_sigma(e) - 0.3) < 0.005
+
+
+def test_reference_arm_prints_one_contract_line():
+    """`bench.py --impl reference` runs on the host alone and prints exactly one JSON line with the
+    keys the bench contract names (its own e2e, no host-device bytes)."""
+    import json
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    import pytest
+
+    root = Path(__file__).resolve().parent.parent
+    if not (root / "oracle" / "_ref" / "libqtrk_ref.so").exists() and not (root / "oracle" / "liboracle_port.so").exists():
+        pytest.skip("oracle not built")
+    r = subprocess.run([sys.executable, str(root / "bench.py"), "--impl", "reference", "--steps", "1", "--warmup", "1",
+                        "--sample", "100"], capture_output=True, text=True, timeout=600, cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.strip()]
+    assert len(lines) == 1, r.stdout
+    d = json.loads(lines[0])
+    for k in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+              "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["value"] > 0 and d["warmup"] >= 3 and d["higher_is_better"] is True
+    assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["value"] == d["value"]
+    assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
