@@ -338,9 +338,13 @@ QTRK_API void QTRK_CALLCONV QTrkB200RefineZLUT(struct QueuedTracker *qtrk, const
  * Limit: count * (4 * zlut_radialsteps + 4 * zlut_radialsteps rounded up to 16) bytes (plus up
  * to 255 bytes of alignment) must fit in 16 MiB: 32,768 ROIs of 64 radial bins. Larger counts
  * return -3 and launch nothing. The instance's BF16 copy of the Z-LUT is made by its first
- * allocating call in this mode (QTrkB200LocalizeDevice or a queued batch); until then this call
- * returns -4 and launches nothing. With device-side jobs (d_jobs != NULL) Z uses the plain match,
- * which needs no scratch.
+ * allocating call in this mode (QTrkB200LocalizeDevice or a queued batch) and dropped whenever
+ * QTrkSetRadialZLUT installs a LUT; while there is none of the current LUT's shape this call
+ * returns -4 and launches nothing. New contents of a LUT of the same shape (BuildLUT,
+ * FinalizeLUT, new radial weights) are copied into the existing BF16 copy by one kernel, after
+ * the work already queued on `stream`; work of earlier calls on other streams must have finished
+ * before the LUT changes. With device-side jobs (d_jobs != NULL) Z uses the plain match, which
+ * needs no scratch.
  * The first call on each device looks up the array's device address; make that first call
  * before any stream capture. All calls share the array and each overwrites what it reads, so
  * nothing needs clearing; calls whose GPU work overlaps (other streams, other instances on the

@@ -21,9 +21,11 @@ Recipe (no reference build system is run):
    forced include, and link the reference's C ABI (``cputrack/qtrk_c_api.cpp``), its
    queued CPU tracker and ``oracle/ref_stage_exports.cpp`` into one shared library.
 
-Usage: ``python oracle/build.py [--reference DIR] [--force]``. When the reference
-tree is absent (e.g. on a machine that only runs the tests) the script does nothing
-and reports whether a prebuilt library is present.
+Usage: ``python oracle/build.py [--reference DIR] [--force]``. The reference checkout is
+``--reference DIR``, else the ``QTRK_REFERENCE`` environment variable, else a checkout named
+``reference`` beside this repository's root directory. When none of them holds the reference
+tree (e.g. on a machine that only runs the tests) the script does nothing and reports whether a
+prebuilt library is present.
 """
 from __future__ import annotations
 
@@ -39,7 +41,8 @@ HERE = Path(__file__).resolve().parent
 OUT_DIR = HERE / "_ref"
 LIB = OUT_DIR / "libqtrk_ref.so"
 PORT_LIB = HERE / "liboracle_port.so"
-DEFAULT_REFERENCE = "/root/reference"
+# a checkout of the reference placed beside this repository (used when no location is given)
+SIBLING_REFERENCE = HERE.parent.parent / "reference"
 
 SOURCES = [
     "cpu_tracker.cpp",
@@ -100,7 +103,7 @@ def build_port(force: bool = False, verbose: bool = True) -> Path:
 
 
 def build(reference: str | None = None, force: bool = False, verbose: bool = True) -> Path | None:
-    ref_root = Path(reference or os.environ.get("QTRK_REFERENCE", DEFAULT_REFERENCE))
+    ref_root = Path(reference or os.environ.get("QTRK_REFERENCE") or SIBLING_REFERENCE)
     cputrack = ref_root / "cputrack"
     if not cputrack.is_dir():
         if verbose:

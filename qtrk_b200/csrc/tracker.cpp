@@ -266,6 +266,7 @@ Tracker::Tracker(const QTrkSettings &settings)
     CheckCuda(cudaHostGetDevicePointer((void **)&d_err_, h_err_, 0), "cudaHostGetDevicePointer");
     CheckCuda(cudaStreamCreateWithFlags(&lut_stream_, cudaStreamNonBlocking), "cudaStreamCreate(lut)");
     CheckCuda(cudaEventCreateWithFlags(&lut_ready_, cudaEventDisableTiming), "cudaEventCreate");
+    CheckCuda(cudaEventCreateWithFlags(&noalloc_order_, cudaEventDisableTiming), "cudaEventCreate");
     CheckCuda(cudaStreamCreateWithFlags(&lut_copy_stream_, cudaStreamNonBlocking), "cudaStreamCreate(lut copy)");
     for (int b = 0; b < 2; b++) {
         CheckCuda(cudaEventCreateWithFlags(&lut_stage_free_[b], cudaEventDisableTiming), "cudaEventCreate");
@@ -331,6 +332,7 @@ Tracker::~Tracker()
     cudaFree(d_dev_zprof_bf16_);
     cudaFreeHost(h_err_);
     if (lut_ready_) cudaEventDestroy(lut_ready_);
+    if (noalloc_order_) cudaEventDestroy(noalloc_order_);
     if (lut_stream_) cudaStreamDestroy(lut_stream_);
     if (lut_copy_stream_) cudaStreamDestroy(lut_copy_stream_);
 }
@@ -694,8 +696,12 @@ bool Tracker::IsPinned(const void *p)
 void Tracker::CollectLocked()
 {
     if (h_err_ && *h_err_) {
+        const unsigned e = *h_err_;
         *h_err_ = 0;
         Warn("tensor-core Z match: an MMA completion wait timed out; z of the affected ROIs is NaN");
+        if (e & 2u)
+            Warn("tensor-core Z match: the timed-out MMAs had not finished when their tensor-memory columns were "
+                 "released; results of that launch are void");
     }
     while (!inflight_.empty()) {
         const int idx = inflight_.front();
@@ -822,9 +828,13 @@ void Tracker::PrepareTensorCoreLUT()
     cudaFree(d_lut_norm_);
     d_lut_bf16_ = nullptr;
     d_lut_norm_ = nullptr;
+    tc_lut_count_ = tc_lut_pp_ = tc_lut_nbp_ = 0;
     CheckCuda(cudaMalloc(&d_lut_bf16_, sizeof(__nv_bfloat16) * (size_t)lut_count_ * 2 * pp * nbp),
               "cudaMalloc(BF16 LUT)");
     CheckCuda(cudaMalloc(&d_lut_norm_, sizeof(float) * (size_t)lut_count_ * pp), "cudaMalloc(LUT norms)");
+    tc_lut_count_ = lut_count_;
+    tc_lut_pp_ = pp;
+    tc_lut_nbp_ = nbp;
     CheckCuda(zmatch_prepare_lut(d_lut_, have_zw_ ? d_zw_ : nullptr, lut_count_, lut_planes_, nb, d_lut_bf16_,
                                  d_lut_norm_, lut_stream_),
               "BF16 LUT preparation");
@@ -1169,6 +1179,13 @@ void Tracker::SetRadialZLUT(const float *data, int count, int planes)
     d_lut_ = nullptr;
     d_lut_t_ = nullptr;
     d_cmp_ = nullptr;
+    // the tensor-core copy was sized for the old LUT: drop it (the next allocating call in a
+    // tensor-core mode makes one of the new shape)
+    cudaFree(d_lut_bf16_);
+    cudaFree(d_lut_norm_);
+    d_lut_bf16_ = nullptr;
+    d_lut_norm_ = nullptr;
+    tc_lut_count_ = tc_lut_pp_ = tc_lut_nbp_ = 0;
     cudaFree(d_zbias_);  // a new LUT drops the bias table, as QueuedCPUTracker.cpp:368-369
     d_zbias_ = nullptr;
     zbias_w_ = zbias_count_ = 0;
@@ -1595,8 +1612,11 @@ int Tracker::LocalizeDevice(const void *d_pixels, int pitch, int64_t roi_stride,
 
 // The allocation-free variant of LocalizeDevice: the tensor-core match's profiles go to
 // `scratch` (a fixed device array owned by the caller of this method), and the instance's
-// BF16 LUT must already exist (it is created by the first allocating call in this mode);
-// refreshing a stale BF16 LUT is a kernel launch only. Nothing here calls cudaMalloc/cudaFree.
+// BF16 LUT must already exist with the current LUT's shape (it is created by the first
+// allocating call in this mode, and dropped when SetRadialZLUT installs a LUT); refreshing a
+// stale BF16 LUT of the same shape (new contents from BuildLUT, FinalizeLUT, new radial weights)
+// is a kernel launch only, ordered after the work already queued on the caller's stream, which
+// may still be reading the old copy. Nothing here calls cudaMalloc/cudaFree.
 int Tracker::LocalizeDeviceNoAlloc(const void *d_pixels, int pitch, int64_t roi_stride, int pdt, int count,
                                    const LocalizationJob *d_jobs, LocalizationResult *d_results, cudaStream_t stream,
                                    void *scratch, size_t scratch_bytes)
@@ -1618,12 +1638,15 @@ int Tracker::LocalizeDeviceNoAlloc(const void *d_pixels, int pitch, int64_t roi_
         P = LaunchParams(pdt);
         tc = UseTensorCoreMatch() && !d_jobs;  // device-side jobs: plain match, as LocalizeDevice
         if (tc) {
-            if (!d_lut_bf16_ || !d_lut_norm_) {
-                Warn("QTrkB200LocalizeDeviceNoAlloc: the instance has no tensor-core LUT yet; it is created by the "
-                     "first QTrkB200LocalizeDevice call or queued batch in this mode");
+            const int nb = cfg.zlut_radialsteps, nbp = zmatch_padded_bins(nb);
+            const bool shape_ok = tc_lut_count_ == lut_count_ && tc_lut_pp_ == zmatch_padded_planes(lut_planes_) &&
+                                  tc_lut_nbp_ == nbp;
+            if (!d_lut_bf16_ || !d_lut_norm_ || !shape_ok) {
+                Warn("QTrkB200LocalizeDeviceNoAlloc: the instance has no tensor-core LUT of the current LUT's shape; "
+                     "it is created by the first QTrkB200LocalizeDevice call or queued batch in this mode after "
+                     "the LUT is set");
                 return -4;
             }
-            const int nb = cfg.zlut_radialsteps, nbp = zmatch_padded_bins(nb);
             const size_t prof_bytes = ((sizeof(float) * (size_t)count * nb) + 255) & ~(size_t)255;
             const size_t need = prof_bytes + sizeof(__nv_bfloat16) * (size_t)count * 2 * nbp;
             if (need > scratch_bytes) {
@@ -1633,7 +1656,9 @@ int Tracker::LocalizeDeviceNoAlloc(const void *d_pixels, int pitch, int64_t roi_
             }
             float *zprof = static_cast<float *>(scratch);
             __nv_bfloat16 *zbf = reinterpret_cast<__nv_bfloat16 *>(static_cast<uint8_t *>(scratch) + prof_bytes);
-            if (tc_lut_stale_) {  // refresh in place: one kernel launch, the buffers keep their size
+            if (tc_lut_stale_) {  // refresh in place: one kernel launch into buffers of this shape
+                CheckCuda(cudaEventRecord(noalloc_order_, stream), "cudaEventRecord");
+                CheckCuda(cudaStreamWaitEvent(lut_stream_, noalloc_order_, 0), "cudaStreamWaitEvent");
                 CheckCuda(zmatch_prepare_lut(d_lut_, have_zw_ ? d_zw_ : nullptr, lut_count_, lut_planes_, nb,
                                              d_lut_bf16_, d_lut_norm_, lut_stream_),
                           "BF16 LUT preparation");

@@ -168,6 +168,10 @@ class Tracker : public QueuedTracker {
     __nv_bfloat16 *d_lut_bf16_ = nullptr;
     float *d_lut_norm_ = nullptr;
     bool tc_lut_stale_ = true;
+    // the (beads, padded planes, padded bins) shape d_lut_bf16_ / d_lut_norm_ were allocated for;
+    // an in-place refresh is only valid while it equals the current LUT's shape
+    int tc_lut_count_ = 0, tc_lut_pp_ = 0, tc_lut_nbp_ = 0;
+    cudaEvent_t noalloc_order_ = nullptr;  // orders an in-place BF16 refresh after the caller's earlier work
     unsigned *h_err_ = nullptr, *d_err_ = nullptr;  // mapped pinned word set by the Z-match kernel
     float *d_dev_zprof_ = nullptr;                  // scratch of the device-resident entry point
     __nv_bfloat16 *d_dev_zprof_bf16_ = nullptr;

@@ -27,7 +27,12 @@
 // Launch: one CTA of 128 threads per tile. Shared memory is sized so that at most two CTAs
 // share an SM, so the two 256-column TMEM allocations always fit the SM's 512 columns and
 // tcgen05.alloc never waits. Every wait on the MMA-completion mbarrier is bounded; on timeout
-// the kernel records an error flag, skips the tensor-memory read, frees its columns and exits.
+// the kernel records an error flag and skips the tensor-memory read. The MMAs it gave up on may
+// still be writing the accumulator columns, so before the columns are released thread 0 waits
+// again for that commit (a second, longer bound, kDrainLimit); only if that wait also gives up
+// are the columns released with the MMAs possibly still in flight (flag bit 2: the results of the
+// launch are void). Releasing is preferred to keeping the columns, since a CTA that exits holding
+// them could leave a later CTA on the same SM waiting in tcgen05.alloc.
 #include <cstdint>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -49,7 +54,8 @@ constexpr float kBoundScale = 0.001953125f;  // 2^-9 (see above)
 // s_k = 2 p'.L'_k - |L'_k|^2 is within 2^-9 (1.016) |p'| |L'_k|; the scale below covers it.
 constexpr float kBoundScaleTF32 = 0.0020f;
 constexpr int kTmemCols = 256;
-constexpr uint32_t kWaitLimit = 1u << 20;  // try_wait polls before the kernel gives up
+constexpr uint32_t kWaitLimit = 1u << 20;   // try_wait polls before the kernel gives up
+constexpr uint32_t kDrainLimit = 1u << 24;  // polls for the abandoned commit before the columns are released
 constexpr int kMaxCand = 16;  // candidate planes kept per ROI; more fall back to scoring every plane
 constexpr int kWarps = kTileM / 32;
 
@@ -252,6 +258,7 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
     const float bscale = tf32 ? kBoundScaleTF32 : kBoundScale;
     bool failed = false;
     uint32_t parity = 0;
+    uint32_t pending_parity = 0;  // phase of the commit a timed-out wait gave up on
     const int planes_pad = Q.planes_pad;
     for (int n0 = 0; n0 < planes_pad; n0 += kMaxN) {
         const int n = min(kMaxN, planes_pad - n0);
@@ -297,6 +304,7 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
             mma_commit(mbar);
         }
         uint32_t polls = 0;
+        pending_parity = parity;
         while (!mbar_try_wait(mbar, parity)) {
             if (++polls > kWaitLimit) {
                 failed = true;
@@ -401,7 +409,19 @@ __global__ void __launch_bounds__(kTileM, 1) zmatch_tc_kernel(ZMatchParams Q)
         }
         if ((tid & 31) == 0) reinterpret_cast<float *>(Q.results)[(size_t)roi * 13 + 8] = z;
     }
-    if (failed && tid == 0 && Q.error_flag) atomicOr(Q.error_flag, 1u);
+    if (failed && tid == 0) {
+        // Wait for the commit of the MMAs this CTA gave up on (they arrive on the mbarrier once
+        // they have finished writing TMEM) before the columns are released below.
+        uint32_t polls = 0;
+        bool drained = true;
+        while (!mbar_try_wait(mbar, pending_parity)) {
+            if (++polls > kDrainLimit) {
+                drained = false;
+                break;
+            }
+        }
+        if (Q.error_flag) atomicOr(Q.error_flag, drained ? 1u : 3u);
+    }
 
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();

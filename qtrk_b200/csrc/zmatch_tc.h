@@ -28,7 +28,8 @@ struct ZMatchParams {
     LocalizationResult *results;     // z (word 8 of each 13-word record) is written
     const float *zbias;              // Z-LUT bias table [zbias_count][zbias_w] or nullptr
     int zbias_w, zbias_count;
-    unsigned *error_flag;            // set to 1 if an MMA completion wait gave up
+    unsigned *error_flag;            // |= 1 if an MMA completion wait gave up, |= 2 if the abandoned MMAs
+                                     // had not committed when their columns were released
     int tf32;                        // 1: TF32 operands (w p and w L in FP32), one MMA per K step
 };
 

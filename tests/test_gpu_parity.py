@@ -349,3 +349,27 @@ def test_ragged_and_extreme_roi_sizes_match_reference(ref, w, h):
     with make_tracker(s, mode, lut) as t:
         r = t.Localize(rois)
     check_results(r, r_ref["pos"], r_ref["firstGuess"], r_ref["error"], r_ref["imageMean"])
+
+
+@pytest.mark.parametrize("factor", [1.5, 2.0])
+@pytest.mark.parametrize("shape", ["roi60_f32", "roi100_u16"])
+def test_qi_angstep_factor_matches_reference(ref, shape, factor):
+    """qi_angstep_factor != 1: ComputeQI starts at angularStepsPerQ / factor^iterations samples per
+    quadrant and multiplies by the factor each iteration, and ComputeQuadrantProfile reads the
+    direction table at the truncated stride (int)(table size / samples) (cpu_tracker.cpp:314,356,
+    655-657). Both BASELINE shapes (60x60 f32 with 64 directions per quadrant, 100x100 u16 with 51),
+    COM + QI + Z against the reference tracker with the same factor."""
+    if shape == "roi60_f32":
+        wl = synth.roi60_f32(120, seed=31)
+        s = synth.settings_roi60(qi_angstep_factor=factor)
+    else:
+        wl = synth.roi100_u16(120, seed=32)
+        s = synth.settings_roi100(qi_angstep_factor=factor)
+    lut = ref.build_lut(wl.settings, wl.lut_stack, abi.BUILDLUT_NORMALIZE, known_pos=wl.lut_known_pos)
+    r_ref = ref.track(s, wl.mode, wl.rois, lut)
+    with make_tracker(s, wl.mode, lut) as t:
+        r = t.Localize(wl.rois)
+    check_results(r, r_ref["pos"], r_ref["firstGuess"], r_ref["error"], r_ref["imageMean"])
+    # the factor changes the result: the same ROIs with factor 1 are localized differently
+    r1 = ref.track(wl.settings, wl.mode, wl.rois, lut)
+    assert np.abs(r1["pos"][:, :2] - r_ref["pos"][:, :2]).max() > 1e-6

@@ -7,10 +7,10 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from build import DEFAULT_REFERENCE  # oracle/build.py: where the reference tree is read from
+from build import SIBLING_REFERENCE  # oracle/build.py: where the reference tree is read from
 from qtrk_b200 import lutfile
 
-_REF = Path(os.environ.get("QTRK_REFERENCE", DEFAULT_REFERENCE))
+_REF = Path(os.environ.get("QTRK_REFERENCE") or SIBLING_REFERENCE)
 FIXTURES = [_REF / "cputrack-test" / "10x.radialzlut", _REF / "cputrack-test" / "zrange" / "long.radialzlut"]
 
 
