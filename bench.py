@@ -438,6 +438,44 @@ def gpu_calibration_stack(dev, nbeads: int, planes: int, w: int = 80, seed: int 
     return out, c.cpu().numpy()
 
 
+def _ref_rate(fn, n: int) -> float:
+    """ROIs/s of one timed call of fn() that processes n ROIs on the host (seconds measured inside)."""
+    return n / fn()
+
+
+def reference_cpu(kind: str, threads: int, **kw) -> dict | None:
+    """The reference's own CPU tracker (oracle/_ref, QueuedCPUTracker) timed on this host for one of the
+    BASELINE workloads: `kind` is "track" (kw: settings, mode, rois, lut) or "buildlut" (kw: settings,
+    stack (planes, beads, H, W)). threads = -1 uses every host thread."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from oracle import RefOracle, cpu_count, ref_available
+
+    from qtrk_b200 import abi
+
+    if not ref_available():
+        return None
+    ref = RefOracle()
+    st = kw["settings"]
+    old = st.numThreads
+    st.numThreads = threads
+    try:
+        if kind == "track":
+            rois = kw["rois"]
+            _, dt = ref.track(st, kw["mode"], rois, kw.get("lut"), return_seconds=True)
+            n = rois.shape[0]
+        else:
+            stack = kw["stack"]
+            t0 = time.perf_counter()
+            ref.build_lut(st, stack, abi.BUILDLUT_NORMALIZE)
+            dt = time.perf_counter() - t0
+            n = stack.shape[0] * stack.shape[1]
+    finally:
+        st.numThreads = old
+    cores = cpu_count() if threads < 0 else threads
+    return {"value": n / dt, "unit": UNIT, "cores": cores, "kind": "reference", "rois_timed": int(n),
+            "seconds": dt}
+
+
 def workloads_bench(dev, steps: int, warmup: int) -> dict:
     """The other workloads: the Gaussian MLE (100,000 16x16 f32 ROIs, 4- and 5-parameter forms), BuildLUT
     of a 256-bead x 200-plane 80x80 u16 calibration stack from host memory, the adjoint over that stack,
@@ -471,6 +509,15 @@ def workloads_bench(dev, steps: int, warmup: int) -> dict:
                      "median_xy_err_nm_vs_truth": float(np.nanmedian(err) * PIXEL_NM),
                      "non_finite_fraction": float(np.mean(~np.isfinite(err))),
                      "crlb": crlb_gauss_workload(wl, res)}
+        if mode == abi.LT_Gaussian2D:  # the reference has the 4-parameter form only (LT_Gaussian2D)
+            cb = reference_cpu("track", -1, settings=s, mode=mode, rois=wl.rois)
+            if cb is not None:
+                cb["host"] = host_cpu()
+                cb["sample"] = f"all {n:,} ROIs of the workload, QueuedCPUTracker numThreads=-1"
+                one = reference_cpu("track", 1, settings=s, mode=mode, rois=wl.rois[:5000])
+                one["sample"] = "first 5,000 ROIs, numThreads=1"
+                cb["single_thread"] = one
+            out[name]["cpu_baseline"] = cb
     del d_rois, d_res
     # ---- BuildLUT / adjoint / LUT refinement on a 256 x 200 calibration stack ----
     nbeads, planes = 256, 200
@@ -501,6 +548,14 @@ def workloads_bench(dev, steps: int, warmup: int) -> dict:
                         "second build on the instance",
             "rois_per_s": nbeads * planes / times[1], "seconds": times[1], "first_build_seconds": times[0],
             "copy_bound_rois_per_s": nbeads / (copy_ms / 1e3), "lut_shape": list(lut.shape)}
+        cb = reference_cpu("buildlut", -1, settings=cs, stack=hs[:40])
+        if cb is not None:
+            cb["host"] = host_cpu()
+            cb["sample"] = "BeginLUT / 40 x BuildLUT(256 ROIs) / FinalizeLUT (planes 0-39 of the stack), numThreads=-1"
+            one = reference_cpu("buildlut", 1, settings=cs, stack=hs[:4])
+            one["sample"] = "4 planes x 256 ROIs, numThreads=1"
+            cb["single_thread"] = one
+        out["buildlut_256x200_80x80_u16"]["cpu_baseline"] = cb
         del d_plane
         flat = d_stack.view(-1, 80, 80)
         xyz = torch.zeros(nbeads * planes, 3, device=dev)
@@ -531,8 +586,72 @@ def workloads_bench(dev, steps: int, warmup: int) -> dict:
                                      "seconds": ref_s, "seconds_per_iteration": ref_s / iters,
                                      "objective_first": float(hist[0]), "objective_last": float(hist[-1])}
         launches += t.KernelLaunchCount() - l0
+    # ---- config 1: 1,000 ROIs of 60x60 f32, COM + QI + Z-LUT 50 x 40 ----
+    wl1 = synth.roi60_f32(1000, seed=1)
+    s1 = wl1.settings
+    s1.cuda_device = dev.index
+    lut1 = build_lut_on_gpu(wl1)
+    d1 = torch.from_numpy(wl1.rois).to(dev)
+    r1 = torch.empty(1000 * 52, dtype=torch.uint8, device=dev)
+    with QTrkInstance(s1) as t:
+        t.SetRadialZLUT(lut1)
+        t.SetLocalizationMode(wl1.mode)
+        l0 = t.KernelLaunchCount()
+        ms = _timed(stream, lambda: t.LocalizeDevice(d1.data_ptr(), 240, 14400, abi.QTrkFloat, 1000, r1.data_ptr(),
+                                                     stream=stream.cuda_stream), steps, warmup)
+        launches += t.KernelLaunchCount() - l0
+    res1 = np.frombuffer(r1.cpu().numpy().tobytes(), dtype=abi.RESULT_DTYPE)
+    out["roi60_f32_1000"] = {"workload": "1,000 ROIs 60x60 f32, COM + QI (4 it, 32 radial x 64 angular per "
+                                         "quadrant) + Z-LUT 50 planes x 40 bins, device-resident, one launch",
+                             "rois_per_s": 1000 / (ms / 1e3), "ms_per_launch": ms}
+    cb = reference_cpu("track", -1, settings=s1, mode=wl1.mode, rois=wl1.rois, lut=lut1)
+    if cb is not None:
+        cb["host"] = host_cpu()
+        cb["sample"] = "all 1,000 ROIs, QueuedCPUTracker numThreads=-1"
+        one = reference_cpu("track", 1, settings=s1, mode=wl1.mode, rois=wl1.rois, lut=lut1)
+        one["sample"] = "all 1,000 ROIs, numThreads=1"
+        cb["single_thread"] = one
+        sys.path.insert(0, str(ROOT / "oracle"))
+        from oracle import RefOracle
+
+        rr = RefOracle().track(s1, wl1.mode, wl1.rois, lut1)
+        out["roi60_f32_1000"]["vs_reference_max_dxy_px"] = float(np.abs(res1["pos"][:, :2] - rr["pos"][:, :2]).max())
+        out["roi60_f32_1000"]["vs_reference_max_dz_planes"] = float(np.abs(res1["pos"][:, 2] - rr["pos"][:, 2]).max())
+    out["roi60_f32_1000"]["cpu_baseline"] = cb
     out["gpu_launches"] = int(launches)
     return out
+
+
+COM_BYTES_PER_ROI = 100 * 100 * 2 + 52  # pixels in, result out (no job records: jobs pointer is null)
+
+
+def com_only_bench(dev, settings, d_rois, n: int, steps: int, warmup: int) -> dict:
+    """LT_OnlyCOM on the headline stack (n ROIs of 100x100 u16 resident in HBM): the register-held
+    streaming COM kernel, one launch per step, with its roofline against the measured HBM copy rate."""
+    import torch
+
+    from qtrk_b200 import abi
+    from qtrk_b200.tracker import QTrkInstance
+
+    stream = torch.cuda.current_stream(dev)
+    d_res = torch.empty(n * 52, dtype=torch.uint8, device=dev)
+    with QTrkInstance(settings) as t:
+        t.SetLocalizationMode(abi.LT_OnlyCOM)
+        l0 = t.KernelLaunchCount()
+        ms = _timed(stream, lambda: t.LocalizeDevice(d_rois.data_ptr(), 200, 20000, abi.QTrkU16, n, d_res.data_ptr(),
+                                                     stream=stream.cuda_stream), steps, warmup)
+        launches = t.KernelLaunchCount() - l0
+    peaks, peak_kind = measured_peaks()
+    achieved = COM_BYTES_PER_ROI * n / (ms / 1e3) / 1e9
+    traffic = None
+    tfile = ROOT / "profiles" / "com_100x100_u16_traffic.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get("dram_bytes_per_launch")
+    return {"workload": f"LT_OnlyCOM, {n:,} ROIs of 100x100 u16 resident in HBM (200 MB > L2), one launch per step",
+            "rois_per_s": n / (ms / 1e3), "ms_per_launch": ms, "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "qtrk::com_kernel<1, 4>", "kernel_ms": ms, "bytes_per_roi": COM_BYTES_PER_ROI}}
 
 
 def serving_bench(dev, main_trk, main_rois, seconds: float, fps: float) -> dict:
@@ -920,6 +1039,10 @@ def main(argv=None) -> int:
     workloads = None
     if rank == 0 and ws == 1 and not args.ncu and not args.no_workloads:
         workloads = workloads_bench(dev, args.steps, args.warmup)
+    if rank == 0 and ws == 1 and not args.ncu:
+        workloads = workloads or {"gpu_launches": 0}
+        workloads["com_only_100x100_u16"] = com_only_bench(dev, s, d_rois, N_ROIS, args.steps, args.warmup)
+        workloads["gpu_launches"] += workloads["com_only_100x100_u16"]["gpu_launches"]
 
     # ---- roofline of the localization kernel ----
     peaks, peak_kind = measured_peaks()

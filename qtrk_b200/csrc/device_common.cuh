@@ -82,19 +82,20 @@ struct WarpGroup {
 };
 
 // Interpolate, utils.h:40-58: rx = (int)x (C truncation); the sample is outside when rx < 0,
-// ry < 0, rx+1 >= w or ry+1 >= h. Returns false when outside.
+// ry < 0, rx+1 >= w or ry+1 >= h. Returns false when outside. Row y of the tile starts at
+// img + y * ts (ts >= w: the tile's row pitch in floats).
 // Without float->int conversions: truncation keeps a sample inside exactly when -1 < x < w-1,
 // and for those x, (int)x == floor(max(x, 0)), which a round-toward-zero add of 2^23 puts in
 // the low mantissa bits. The fraction x - rx is formed from the same exact float as the
 // reference's x - (float)rx, so the interpolated value is unchanged.
-__device__ __forceinline__ bool bilinear(const float *img, int w, int h, float x, float y, float &v)
+__device__ __forceinline__ bool bilinear(const float *img, int w, int h, int ts, float x, float y, float &v)
 {
     if (!(x > -1.0f && x < (float)(w - 1) && y > -1.0f && y < (float)(h - 1))) return false;
     const float kMagic = 8388608.0f;  // 2^23
     const float tx = __fadd_rz(fmaxf(x, 0.0f), kMagic), ty = __fadd_rz(fmaxf(y, 0.0f), kMagic);
     const int rx = __float_as_int(tx) - 0x4B000000, ry = __float_as_int(ty) - 0x4B000000;
-    const float *p = img + ry * w + rx;
-    const float v00 = p[0], v10 = p[1], v01 = p[w], v11 = p[w + 1];
+    const float *p = img + ry * ts + rx;
+    const float v00 = p[0], v10 = p[1], v01 = p[ts], v11 = p[ts + 1];
     const float fx = x - (tx - kMagic), fy = y - (ty - kMagic);
     const float v0 = v00 + (v10 - v00) * fx;
     const float v1 = v01 + (v11 - v01) * fx;
@@ -104,12 +105,12 @@ __device__ __forceinline__ bool bilinear(const float *img, int w, int h, float x
 
 // bilinear() for a sample known to lie strictly inside (0 < x < w-1, 0 < y < h-1): the same
 // arithmetic without the range test. Callers prove the range for a whole bin at once.
-__device__ __forceinline__ float bilinear_inside(const float *img, int w, float x, float y)
+__device__ __forceinline__ float bilinear_inside(const float *img, int ts, float x, float y)
 {
     const float kMagic = 8388608.0f;
     const float tx = __fadd_rz(x, kMagic), ty = __fadd_rz(y, kMagic);
-    const float *p = img + ((__float_as_int(ty) - 0x4B000000) * w + (__float_as_int(tx) - 0x4B000000));
-    const float v00 = p[0], v10 = p[1], v01 = p[w], v11 = p[w + 1];
+    const float *p = img + ((__float_as_int(ty) - 0x4B000000) * ts + (__float_as_int(tx) - 0x4B000000));
+    const float v00 = p[0], v10 = p[1], v01 = p[ts], v11 = p[ts + 1];
     const float fx = x - (tx - kMagic), fy = y - (ty - kMagic);
     const float v0 = v00 + (v10 - v00) * fx;
     const float v1 = v01 + (v11 - v01) * fx;
@@ -420,6 +421,384 @@ __device__ ComResult compute_com(const G &g, const float *img, int W, int H, flo
     return r;
 }
 
+// -------------------------------------------------------------------------------------
+// Padded ROI tile for the sampling kernels. Row y of the float tile starts at img + y * ts,
+// with ts >= W even (8-byte aligned rows for float2 stores) and ts mod 32 in {6, 12, 20, 26}:
+// a warp's bilinear gathers cover a patch a few pixels wide and high around the sample points,
+// and with these pitches the rows of such a patch fall on different banks (simulated for the
+// QI and radial-profile lane layouts below on 60-200 px ROIs: ~1.3-1.4 shared-memory wavefronts
+// per gather, against 1.6 at W = 100 and up to 5 at W = 64 or 128 without padding).
+// -------------------------------------------------------------------------------------
+__host__ __device__ inline int tile_pitch(int W)
+{
+    for (int p = W + (W & 1);; p += 2) {
+        const int m = p & 31;
+        if (m == 6 || m == 12 || m == 20 || m == 26) return p;
+    }
+}
+
+// Load a ROI into the padded tile (pitch ts) with the per-pixel steps of load_roi (conversion,
+// ClearFirstFourPixels, offset/gain), and return this thread's FP32 partial sums of v and v^2
+// over the pixels it converted (the first pass of CPUTracker::ComputeMeanAndCOM,
+// cpu_tracker.cpp:687-693), so the tile is not read again for them. Warps take rows, lanes take
+// pixel pairs along a row (two rows per step, all of a step's loads issued before any is used);
+// each pair is one 2/4/8-byte streaming load and one conflict-free float2 store. Rows of odd
+// width or unaligned rows are read pixel by pixel. Every thread of the CTA calls; a barrier
+// must follow before the tile is read.
+__device__ inline float2 load_roi_tile(float *img, int ts, const uint8_t *src, int pitch, const TrackParams &P,
+                                       int bead)
+{
+    const int W = P.width, H = P.height, n = W * H;
+    const int bpp = P.pdt == 0 ? 1 : (P.pdt == 1 ? 2 : 4);
+    const float *off = nullptr, *gain = nullptr;
+    if (bead >= 0 && bead < P.calib_count) {
+        if (P.calib_offset) off = P.calib_offset + (size_t)bead * n;
+        if (P.calib_gain) gain = P.calib_gain + (size_t)bead * n;
+    }
+    const bool plain = !off && !gain && !(P.mode & kLT_ClearFirstFourPixels);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    float s = 0.0f, s2 = 0.0f;
+    constexpr int kMaxPairsPerLane = 4;  // rows up to 256 pixels (wider rows: pixel by pixel)
+    const bool pairs = !(W & 1) && W <= 64 * kMaxPairsPerLane && !(reinterpret_cast<uintptr_t>(src) & (2 * bpp - 1)) &&
+                       !(pitch & (2 * bpp - 1));
+    if (pairs) {
+        const int np = W >> 1, mp = (np + 31) >> 5;
+        for (int y0 = warp; y0 < H; y0 += 2 * nw) {
+            uint2 q[2][kMaxPairsPerLane];
+#pragma unroll
+            for (int r = 0; r < 2; r++) {
+                const int y = y0 + r * nw;
+                const uint8_t *row = src + (size_t)y * pitch;
+#pragma unroll
+                for (int m = 0; m < kMaxPairsPerLane; m++) {
+                    const int k = lane + 32 * m;
+                    if (m < mp && y < H && k < np) {
+                        if (P.pdt == 0)
+                            q[r][m].x = __ldcs(reinterpret_cast<const unsigned short *>(row) + k);
+                        else if (P.pdt == 1)
+                            q[r][m].x = __ldcs(reinterpret_cast<const unsigned int *>(row) + k);
+                        else
+                            q[r][m] = __ldcs(reinterpret_cast<const uint2 *>(row) + k);
+                    }
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < 2; r++) {
+                const int y = y0 + r * nw;
+#pragma unroll
+                for (int m = 0; m < kMaxPairsPerLane; m++) {
+                    const int k = lane + 32 * m;
+                    if (m < mp && y < H && k < np) {
+                        float a, b;
+                        if (P.pdt == 0) {
+                            a = u_to_float(q[r][m].x & 0xffu);
+                            b = u_to_float((q[r][m].x >> 8) & 0xffu);
+                        } else if (P.pdt == 1) {
+                            a = u_to_float(q[r][m].x & 0xffffu);
+                            b = u_to_float(q[r][m].x >> 16);
+                        } else {
+                            a = __uint_as_float(q[r][m].x);
+                            b = __uint_as_float(q[r][m].y);
+                        }
+                        if (!plain) {
+                            a = finish_pixel(a, y * W + 2 * k, P, off, gain);
+                            b = finish_pixel(b, y * W + 2 * k + 1, P, off, gain);
+                        }
+                        s += a;
+                        s2 = fmaf(a, a, s2);
+                        s += b;
+                        s2 = fmaf(b, b, s2);
+                        reinterpret_cast<float2 *>(img + y * ts)[k] = make_float2(a, b);
+                    }
+                }
+            }
+        }
+    } else {
+        for (int y = warp; y < H; y += nw) {
+            const uint8_t *row = src + (size_t)y * pitch;
+            for (int x = lane; x < W; x += 32) {
+                float v;
+                if (P.pdt == 0)
+                    v = u_to_float(row[x]);
+                else if (P.pdt == 1)
+                    v = u_to_float(reinterpret_cast<const uint16_t *>(row)[x]);
+                else
+                    v = reinterpret_cast<const float *>(row)[x];
+                v = finish_pixel(v, y * W + x, P, off, gain);
+                s += v;
+                s2 = fmaf(v, v, s2);
+                img[y * ts + x] = v;
+            }
+        }
+    }
+    return make_float2(s, s2);
+}
+
+// load_roi_tile for a ROI whose raw rows already sit in shared memory, back to back, at
+// `raw` inside the tile region (placed at the region's end, so that raw row y starts at or after
+// the end of float row y - 1: see plan_smem). Rows are converted in groups of 2 x warps rows:
+// each group's raw pixel pairs are read into registers, a barrier passes, then the group's float
+// rows are written (they may overlap the group's own raw rows but never a later group's). W must
+// be even. Every thread calls; the tile is complete at return (a barrier ends the last group).
+__device__ inline float2 convert_staged_tile(float *img, int ts, const uint8_t *raw, const TrackParams &P, int bead)
+{
+    const int W = P.width, H = P.height, n = W * H;
+    const int bpp = P.pdt == 0 ? 1 : (P.pdt == 1 ? 2 : 4);
+    const float *off = nullptr, *gain = nullptr;
+    if (bead >= 0 && bead < P.calib_count) {
+        if (P.calib_offset) off = P.calib_offset + (size_t)bead * n;
+        if (P.calib_gain) gain = P.calib_gain + (size_t)bead * n;
+    }
+    const bool plain = !off && !gain && !(P.mode & kLT_ClearFirstFourPixels);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    constexpr int kMaxPairsPerLane = 4;  // rows up to 256 pixels
+    const int np = W >> 1, mp = (np + 31) >> 5;
+    float s = 0.0f, s2 = 0.0f;
+    for (int y0 = 0; y0 < H; y0 += 2 * nw) {
+        uint2 q[2][kMaxPairsPerLane];
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const int y = y0 + warp + r * nw;
+            const uint8_t *row = raw + (size_t)y * W * bpp;
+#pragma unroll
+            for (int m = 0; m < kMaxPairsPerLane; m++) {
+                const int k = lane + 32 * m;
+                if (m < mp && y < H && k < np) {
+                    if (P.pdt == 0)
+                        q[r][m].x = reinterpret_cast<const unsigned short *>(row)[k];
+                    else if (P.pdt == 1)
+                        q[r][m].x = reinterpret_cast<const unsigned int *>(row)[k];
+                    else
+                        q[r][m] = reinterpret_cast<const uint2 *>(row)[k];
+                }
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const int y = y0 + warp + r * nw;
+#pragma unroll
+            for (int m = 0; m < kMaxPairsPerLane; m++) {
+                const int k = lane + 32 * m;
+                if (m < mp && y < H && k < np) {
+                    float a, b;
+                    if (P.pdt == 0) {
+                        a = u_to_float(q[r][m].x & 0xffu);
+                        b = u_to_float((q[r][m].x >> 8) & 0xffu);
+                    } else if (P.pdt == 1) {
+                        a = u_to_float(q[r][m].x & 0xffffu);
+                        b = u_to_float(q[r][m].x >> 16);
+                    } else {
+                        a = __uint_as_float(q[r][m].x);
+                        b = __uint_as_float(q[r][m].y);
+                    }
+                    if (!plain) {
+                        a = finish_pixel(a, y * W + 2 * k, P, off, gain);
+                        b = finish_pixel(b, y * W + 2 * k + 1, P, off, gain);
+                    }
+                    s += a;
+                    s2 = fmaf(a, a, s2);
+                    s += b;
+                    s2 = fmaf(b, b, s2);
+                    reinterpret_cast<float2 *>(img + y * ts)[k] = make_float2(a, b);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    return make_float2(s, s2);
+}
+
+// CPUTracker::ComputeMeanAndCOM (cpu_tracker.cpp:681-729) on a padded tile whose pass-1 partial
+// sums (v, v^2) come from load_roi_tile: mean and stdev as the reference rounds them, then the
+// background-corrected moments over the tile (rows by warps, pixel pairs by lanes), FP32 per
+// thread and FP64 across the CTA. All threads call; every thread gets the result.
+__device__ inline ComResult com_tile(const float *img, int ts, int W, int H, float2 part, float bgcorr, double *red)
+{
+    BlockGroup g{red};
+    double s[2] = {part.x, part.y};
+    g.sum(s);
+    const int n = W * H;
+    const float invN = 1.0f / (float)n;
+    ComResult r;
+    r.mean = (float)(s[0] * (double)invN);
+    r.stdev = sqrtf((float)(s[1] * (double)invN - (double)(r.mean * r.mean)));
+    const float thr = bgcorr * r.stdev;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    float q0 = 0.0f, qx = 0.0f, qy = 0.0f;
+    if (!(W & 1)) {
+        const int np = W >> 1;
+        for (int y = warp; y < H; y += nw) {
+            const float2 *row = reinterpret_cast<const float2 *>(img + y * ts);
+            float r0 = 0.0f, rx = 0.0f;
+            for (int k = lane; k < np; k += 32) {
+                const float2 v = row[k];
+                const float a = fmaxf(0.0f, fabsf(v.x - r.mean) - thr);
+                const float b = fmaxf(0.0f, fabsf(v.y - r.mean) - thr);
+                const float x = (float)(2 * k);
+                r0 += a + b;
+                rx = fmaf(x, a, rx);
+                rx = fmaf(x + 1.0f, b, rx);
+            }
+            q0 += r0;
+            qx += rx;
+            qy = fmaf((float)y, r0, qy);
+        }
+    } else {
+        for (int y = warp; y < H; y += nw) {
+            float r0 = 0.0f, rx = 0.0f;
+            for (int x = lane; x < W; x += 32) {
+                const float a = fmaxf(0.0f, fabsf(img[y * ts + x] - r.mean) - thr);
+                r0 += a;
+                rx = fmaf((float)x, a, rx);
+            }
+            q0 += r0;
+            qx += rx;
+            qy = fmaf((float)y, r0, qy);
+        }
+    }
+    double m[3] = {q0, qx, qy};
+    g.sum(m);
+    r.x = (float)(m[1] / m[0]);
+    r.y = (float)(m[2] / m[0]);
+    return r;
+}
+
+// Bilinear value at a sample whose truncated corner (ix, row) and fractions are known: row points
+// at the tile row of the upper corner pixels. Arithmetic of bilinear_inside.
+__device__ __forceinline__ float lerp_cell(const float *row, int ts, int ix, float fx, float fy)
+{
+    const float *p = row + ix;
+    const float v00 = p[0], v10 = p[1], v01 = p[ts], v11 = p[ts + 1];
+    const float v0 = v00 + (v10 - v00) * fx;
+    const float v1 = v01 + (v11 - v01) * fx;
+    return v0 + (v1 - v0) * fy;
+}
+
+// CPUTracker::ComputeQuadrantProfile (cpu_tracker.cpp:631-677) for all four quadrants at once,
+// written as the FFT input of the QI autoconvolution. The four quadrants sample the same
+// table direction d at radius r with mirrored signs (x = cx +- d.x r, y = cy +- d.y r), so one
+// thread takes one radius and a strided subset of the directions and produces all four samples
+// of each: the products d.x r, d.y r, the truncations and fractions of the two x and two y
+// coordinates are shared by four samples. Coordinates are formed as the reference forms them
+// (d.x r rounded, then added to the centre). Layout: S = blockDim/nr direction subsets
+// (directions sub, sub + S, ...); a warp holds R = 32/A radii x A = min(S, 4) adjacent subsets,
+// so its gathers fall into a small patch (see tile_pitch). Per quadrant and radius the bin value
+// is the mean of the in-bounds samples (the image mean when fewer than 4), times the radial
+// weight; the subsets' partial sums meet through warp shuffles (and `part`, 2 KB of shared
+// memory, when S > A). The thread of subset 0 writes the X and Y concatenations
+// (cpu_tracker.cpp:327-343; X = [(q1+q2) reversed | q0+q3], Y = [(q2+q3) reversed | q0+q1]) as
+// one complex value z = X + iY per position, in bit-reversed order (log2L = log2(2 nr)) or in
+// natural order when log2L < 0. All threads call; a barrier must follow before A is read.
+__device__ inline void qi_profiles_sym(const float *img, int W, int H, int ts, float cx, float cy, float mean, int nr,
+                                       int nang, int stride, float minr, float rstep, const float2 *dirs,
+                                       const float *rweights, float4 *part, float2 *A, int log2L)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int S = nr >= (int)blockDim.x ? 1 : (int)blockDim.x / nr;
+    const int Aw = S < 4 ? S : 4, R = 32 / Aw;
+    const int nwr = nr >= R ? nr / R : 1, nsb = S / Aw;
+    const float kMagic = 8388608.0f;
+    for (int wi = warp; wi < nwr * nsb; wi += nw) {
+        const int rb = wi % nwr, sb = wi / nwr;
+        const int i = rb * R + lane / Aw, sub = sb * Aw + lane % Aw;
+        float sm[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        int cnt[4] = {0, 0, 0, 0};
+        if (i < nr) {
+            const float r = __fadd_rn(minr, __fmul_rn(rstep, (float)i));
+            if (circle_inside(cx, cy, fabsf(r), W, H)) {
+                for (int a = sub; a < nang; a += S) {
+                    const float2 d = dirs[stride * a];
+                    const float dx = __fmul_rn(d.x, r), dy = __fmul_rn(d.y, r);
+                    const float xp = __fadd_rn(cx, dx), xm = __fadd_rn(cx, -dx);
+                    const float yp = __fadd_rn(cy, dy), ym = __fadd_rn(cy, -dy);
+                    const float txp = __fadd_rz(xp, kMagic), txm = __fadd_rz(xm, kMagic);
+                    const float typ = __fadd_rz(yp, kMagic), tym = __fadd_rz(ym, kMagic);
+                    const float fxp = xp - (txp - kMagic), fxm = xm - (txm - kMagic);
+                    const float fyp = yp - (typ - kMagic), fym = ym - (tym - kMagic);
+                    const int ixp = __float_as_int(txp) - 0x4B000000, ixm = __float_as_int(txm) - 0x4B000000;
+                    const float *rowp = img + (__float_as_int(typ) - 0x4B000000) * ts;
+                    const float *rowm = img + (__float_as_int(tym) - 0x4B000000) * ts;
+                    sm[0] += lerp_cell(rowp, ts, ixp, fxp, fyp);  // q0 (+, +)
+                    sm[1] += lerp_cell(rowp, ts, ixm, fxm, fyp);  // q1 (-, +)
+                    sm[2] += lerp_cell(rowm, ts, ixm, fxm, fym);  // q2 (-, -)
+                    sm[3] += lerp_cell(rowm, ts, ixp, fxp, fym);  // q3 (+, -)
+                }
+                const int c = sub < nang ? (nang - sub + S - 1) / S : 0;
+                cnt[0] = cnt[1] = cnt[2] = cnt[3] = c;
+            } else {
+                for (int a = sub; a < nang; a += S) {
+                    const float2 d = dirs[stride * a];
+                    const float dx = __fmul_rn(d.x, r), dy = __fmul_rn(d.y, r);
+                    const float xp = __fadd_rn(cx, dx), xm = __fadd_rn(cx, -dx);
+                    const float yp = __fadd_rn(cy, dy), ym = __fadd_rn(cy, -dy);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        float v;
+                        if (bilinear(img, W, H, ts, (q == 0 || q == 3) ? xp : xm, q < 2 ? yp : ym, v)) {
+                            sm[q] += v;
+                            cnt[q]++;
+                        }
+                    }
+                }
+            }
+        }
+        // subsets of one radius: lanes that differ in their low log2(Aw) bits
+        for (int o = 1; o < Aw; o <<= 1)
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                sm[q] += __shfl_xor_sync(0xffffffffu, sm[q], o);
+                cnt[q] += __shfl_xor_sync(0xffffffffu, cnt[q], o);
+            }
+        if (nsb > 1) {  // subsets spread over warps (nr < blockDim/4): meet in shared memory
+            if (lane % Aw == 0 && i < nr) {
+                part[2 * (sb * nr + i)] = make_float4(sm[0], sm[1], sm[2], sm[3]);
+                part[2 * (sb * nr + i) + 1] = make_float4(__int_as_float(cnt[0]), __int_as_float(cnt[1]),
+                                                          __int_as_float(cnt[2]), __int_as_float(cnt[3]));
+            }
+            continue;
+        }
+        if (lane % Aw == 0 && i < nr) {
+            float v[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                v[q] = cnt[q] >= 4 ? sm[q] / (float)cnt[q] : mean;
+                if (rweights) v[q] *= rweights[i];
+            }
+            const int n0 = nr - 1 - i, n1 = nr + i;
+            A[log2L >= 0 ? (int)bitrev(n0, log2L) : n0] = make_float2(v[1] + v[2], v[2] + v[3]);
+            A[log2L >= 0 ? (int)bitrev(n1, log2L) : n1] = make_float2(v[0] + v[3], v[0] + v[1]);
+        }
+    }
+    if (nsb > 1) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < nr; i += blockDim.x) {
+            float sm[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            int cnt[4] = {0, 0, 0, 0};
+            for (int b = 0; b < nsb; b++) {
+                const float4 p = part[2 * (b * nr + i)], c = part[2 * (b * nr + i) + 1];
+                sm[0] += p.x;
+                sm[1] += p.y;
+                sm[2] += p.z;
+                sm[3] += p.w;
+                cnt[0] += __float_as_int(c.x);
+                cnt[1] += __float_as_int(c.y);
+                cnt[2] += __float_as_int(c.z);
+                cnt[3] += __float_as_int(c.w);
+            }
+            float v[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                v[q] = cnt[q] >= 4 ? sm[q] / (float)cnt[q] : mean;
+                if (rweights) v[q] *= rweights[i];
+            }
+            const int n0 = nr - 1 - i, n1 = nr + i;
+            A[log2L >= 0 ? (int)bitrev(n0, log2L) : n0] = make_float2(v[1] + v[2], v[2] + v[3]);
+            A[log2L >= 0 ? (int)bitrev(n1, log2L) : n1] = make_float2(v[0] + v[3], v[0] + v[1]);
+        }
+    }
+}
+
 // Lanes per radial/quadrant bin: the largest power of two with nbins*lanes <= threads, <= 32.
 __device__ __forceinline__ int lanes_per_bin(int nbins)
 {
@@ -435,7 +814,7 @@ __device__ __forceinline__ int lanes_per_bin(int nbins)
 // radius minr + rstep*i (the image mean when fewer than 4 are in bounds), times the
 // radial weight. Directions come from the quadrant table at stride `stride`.
 // -------------------------------------------------------------------------------------
-__device__ inline void qi_quadrant_profiles(const float *img, int W, int H, float cx, float cy, float mean, int nr, int nang,
+__device__ inline void qi_quadrant_profiles(const float *img, int W, int H, int ts, float cx, float cy, float mean, int nr, int nang,
                                      int stride, float minr, float rstep, const float2 *dirs, const float *rweights,
                                      float *qprof)
 {
@@ -459,7 +838,7 @@ __device__ inline void qi_quadrant_profiles(const float *img, int W, int H, floa
 #pragma unroll kSampleUnroll
                 for (int a = sub; a < nang; a += tpb) {
                     const float2 d = dirs[stride * a];
-                    sum += bilinear_inside(img, W, cx + d.x * sx, cy + d.y * sy);
+                    sum += bilinear_inside(img, ts, cx + d.x * sx, cy + d.y * sy);
                 }
                 cnt = (nang - sub + tpb - 1) / tpb;
             } else {
@@ -467,7 +846,7 @@ __device__ inline void qi_quadrant_profiles(const float *img, int W, int H, floa
                 for (int a = sub; a < nang; a += tpb) {
                     const float2 d = dirs[stride * a];
                     float v;
-                    if (bilinear(img, W, H, cx + d.x * sx, cy + d.y * sy, v)) {
+                    if (bilinear(img, W, H, ts, cx + d.x * sx, cy + d.y * sy, v)) {
                         sum += v;
                         cnt++;
                     }
@@ -557,12 +936,12 @@ __device__ __forceinline__ float2 qi_concat(const float *qprof, int nr, int n)
 // FFT(reverse(p))* = e^{-2 pi i k/L} FFT(p) for real p, the product the reference forms
 // from two forward FFTs equals e^{-2 pi i k/L} P[k]^2, so one forward and one inverse
 // FFT per iteration give both axes. Result: ac[n] = (out_x[n], out_y[n]). Warp 0 only.
-__device__ inline void qi_autoconv_fft(const float *qprof, int nr, float2 *A, float2 *ac, const float2 *tw)
+// qi_autoconv_fft with A already holding the packed profile in bit-reversed order (as
+// qi_profiles_sym writes it). Warp 0 only.
+__device__ inline void qi_autoconv_fft_filled(int nr, float2 *A, float2 *ac, const float2 *tw)
 {
     const int lane = threadIdx.x & 31;
     const int L = 2 * nr, log2L = ilog2_pow2(L);
-    for (int n = lane; n < L; n += 32) A[bitrev(n, log2L)] = qi_concat(qprof, nr, n);
-    __syncwarp();
     warp_fft(A, L, log2L, tw, false);
     for (int k = lane; k < L; k += 32) {
         const float2 Zk = A[k];
@@ -580,12 +959,20 @@ __device__ inline void qi_autoconv_fft(const float *qprof, int nr, float2 *A, fl
     warp_fft(ac, L, log2L, tw, true);
 }
 
-// Same quantity by direct summation (any L; used when 2nr is not a power of two). All threads.
-__device__ inline void qi_autoconv_direct(const float *qprof, int nr, float2 *A, float2 *ac)
+__device__ inline void qi_autoconv_fft(const float *qprof, int nr, float2 *A, float2 *ac, const float2 *tw)
+{
+    const int lane = threadIdx.x & 31;
+    const int L = 2 * nr, log2L = ilog2_pow2(L);
+    for (int n = lane; n < L; n += 32) A[bitrev(n, log2L)] = qi_concat(qprof, nr, n);
+    __syncwarp();
+    qi_autoconv_fft_filled(nr, A, ac, tw);
+}
+
+// Same quantity by direct summation (any L; used when 2nr is not a power of two), A already
+// holding the packed profile in natural order and a barrier passed. All threads.
+__device__ inline void qi_autoconv_direct_filled(int nr, const float2 *A, float2 *ac)
 {
     const int L = 2 * nr;
-    for (int n = threadIdx.x; n < L; n += blockDim.x) A[n] = qi_concat(qprof, nr, n);
-    __syncthreads();
     for (int n = threadIdx.x; n < L; n += blockDim.x) {
         float sx = 0.0f, sy = 0.0f;
         for (int m = 0; m < L; m++) {
@@ -605,7 +992,7 @@ __device__ inline void qi_autoconv_direct(const float *qprof, int nr, float2 *A,
 // bilinear samples on the full circle (FP64 sum), or `mean` when no more than 4 samples
 // are in bounds; then NormalizeRadialProfile (utils.cpp:230-261) when asked.
 // -------------------------------------------------------------------------------------
-__device__ inline void radial_profile(const float *img, int W, int H, float cx, float cy, float mean, int nb, int nang,
+__device__ inline void radial_profile(const float *img, int W, int H, int ts, float cx, float cy, float mean, int nb, int nang,
                                float minr, float rstep, const float2 *dirs, float *prof, bool normalize,
                                double *red)
 {
@@ -629,7 +1016,7 @@ __device__ inline void radial_profile(const float *img, int W, int H, float cx, 
                         const int a = a0 + k * tpb;
                         if (a < nang) {
                             const float2 d = dirs[a];
-                            part += bilinear_inside(img, W, cx + d.x * r, cy + d.y * r);
+                            part += bilinear_inside(img, ts, cx + d.x * r, cy + d.y * r);
                             cnt++;
                         }
                     }
@@ -638,7 +1025,7 @@ __device__ inline void radial_profile(const float *img, int W, int H, float cx, 
                     for (int k = 0; k < 8; k++) {
                         const int a = a0 + k * tpb;
                         float v;
-                        if (a < nang && bilinear(img, W, H, cx + dirs[a].x * r, cy + dirs[a].y * r, v)) {
+                        if (a < nang && bilinear(img, W, H, ts, cx + dirs[a].x * r, cy + dirs[a].y * r, v)) {
                             part += v;
                             cnt++;
                         }

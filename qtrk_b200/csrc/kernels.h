@@ -21,9 +21,17 @@ cudaError_t launch_localize(const TrackParams &P, const uint8_t *pixels, int pit
                             const int64_t *roi_offsets, const LocalizationJob *jobs, int count,
                             LocalizationResult *results, cudaStream_t stream);
 
-// The kernel node that launch_localize would launch for `count` ROIs (function, grid, block,
-// shared memory); the caller sets kernelParams to the 8 arguments of launch_localize's kernel
-// (P, pixels, pitch, roi_stride, roi_offsets, jobs, count, results). For explicitly built graphs.
+// LT_OnlyCOM on ROIs stored back to back (no per-bead calibration): the register-held streaming
+// COM kernel (com.cu) serves them; launch_localize chooses it by itself.
+bool use_com_kernel(const TrackParams &P, const uint8_t *pixels, int pitch, int64_t roi_stride,
+                    const int64_t *roi_offsets);
+cudaError_t launch_com(const TrackParams &P, const uint8_t *pixels, int64_t roi_stride, const LocalizationJob *jobs,
+                       int count, LocalizationResult *results, cudaStream_t stream);
+
+// The kernel node that launch_localize would launch for `count` ROIs addressed through
+// roi_offsets (function, grid, block, shared memory); the caller sets kernelParams to the 8
+// arguments of launch_localize's kernel (P, pixels, pitch, roi_stride, roi_offsets, jobs, count,
+// results). For explicitly built graphs; never the COM kernel, which takes ROIs back to back.
 void localize_node(const TrackParams &P, int count, cudaKernelNodeParams &kp);
 
 // Bias-table images [first_image, first_image + n_images) of QueuedTracker::ComputeZBiasCorrection

@@ -1,10 +1,12 @@
 // Localization kernels for sm_100a.
 //
-// localize_kernel: one CTA per ROI runs the whole per-ROI pipeline of
-//   QueuedCPUTracker::ProcessJob (cputrack/QueuedCPUTracker.cpp:273-361) on a float tile
-//   of the ROI in shared memory: load + convert (+ calibration) -> mean/COM -> QI
-//   iterations (or the 2D Gaussian MLE) -> radial profile -> Z-LUT match -> result.
-//   Pixels are read from HBM exactly once; everything after the load works on-chip.
+// localize_qi_kernel: each CTA walks a queue of ROIs and runs the whole per-ROI pipeline of
+//   QueuedCPUTracker::ProcessJob (cputrack/QueuedCPUTracker.cpp:273-361) on a padded float tile
+//   of the ROI in shared memory: stage (bulk copy of the next ROI during the current one's Z
+//   stage) + convert (+ calibration) fused with the first COM pass -> COM -> QI iterations ->
+//   radial profile -> Z-LUT match -> result. Pixels are read from HBM exactly once; everything
+//   after the copy works on-chip.
+// localize_gauss_kernel: one CTA per ROI, COM -> 2D Gaussian MLE (-> Z) on a plain tile.
 // gauss_warp_kernel: one warp per small ROI (<= 32x32) for the Gaussian-only mode.
 // build_lut_kernel / finalize_lut_kernel: QueuedCPUTracker::BuildLUT / FinalizeLUT
 //   (cputrack/QueuedCPUTracker.cpp:580-659) with the accumulation on the device.
@@ -12,10 +14,12 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <cuda_runtime.h>
 
 #include <cuda_bf16.h>
 
+#include "bulk_copy.cuh"
 #include "device_common.cuh"
 #include "kernels.h"
 
@@ -67,28 +71,27 @@ __device__ __forceinline__ void load_z_tables(const SmemView &s, const TrackPara
         for (int i = threadIdx.x; i < P.z_angsteps; i += blockDim.x) s.zdirs[i] = zd[i];
 }
 
-// CPUTracker::ComputeQI, cpu_tracker.cpp:285-360. All threads call; returns the position
-// and the boundary flag of the last iteration.
+// CPUTracker::ComputeQI, cpu_tracker.cpp:285-360, on the padded tile (row pitch P.sm_pitch). All
+// threads call; returns the position and the boundary flag of the last iteration.
 __device__ void qi_localize(const SmemView &s, const TrackParams &P, float mean, float &cx, float &cy, bool &bhit,
                             const float *rweights)
 {
     const int W = P.width, H = P.height, nr = P.qi_nr, L = 2 * nr;
     const bool pow2 = (L & (L - 1)) == 0 && L >= 2;
-    // qprof (4 nr floats) is dead once the concatenated profile A is built, so the
-    // autoconvolution ac (L = 2 nr complex) reuses its space: [ qprof | ac ] [ A ].
-    float *qprof = reinterpret_cast<float *>(s.work);
+    // work: [ ac (L complex) ] [ A (L complex) ] [ subset partials (2 KB) ]
     float2 *ac = reinterpret_cast<float2 *>(s.work);
     float2 *A = reinterpret_cast<float2 *>(s.work + L * 8);
+    float4 *part = reinterpret_cast<float4 *>(s.work + 2 * L * 8);
     const float rstep = (P.qi_maxr - P.qi_minr) / (float)nr;  // also pixelsPerProfLen (cpu_tracker.cpp:311,649)
     for (int k = 0; k < P.qi_iterations; k++) {
         bhit = check_boundaries(cx, cy, P.qi_maxr, W, H);
-        qi_quadrant_profiles(s.img, W, H, cx, cy, mean, nr, P.qi_nang[k], P.qi_stride[k], P.qi_minr, rstep, s.qdirs,
-                             rweights, qprof);
+        qi_profiles_sym(s.img, W, H, P.sm_pitch, cx, cy, mean, nr, P.qi_nang[k], P.qi_stride[k], P.qi_minr, rstep,
+                        s.qdirs, rweights, part, A, pow2 ? ilog2_pow2(L) : -1);
         __syncthreads();
         if (pow2) {
-            if (threadIdx.x < 32) qi_autoconv_fft(qprof, nr, A, ac, s.tw);
+            if (threadIdx.x < 32) qi_autoconv_fft_filled(nr, A, ac, s.tw);
         } else {
-            qi_autoconv_direct(qprof, nr, A, ac);
+            qi_autoconv_direct_filled(nr, A, ac);
         }
         if (pow2) __syncthreads();  // the FFT ran on warp 0 only
         if (threadIdx.x < 64) {
@@ -114,9 +117,21 @@ __device__ void qi_localize(const SmemView &s, const TrackParams &P, float mean,
     }
 }
 
-// Radial profile + Z-LUT compare (QueuedCPUTracker.cpp:319-338). Returns z (0 without a LUT).
-// With P.zprof_f32 set, the profile is written out for the tensor-core match instead.
-__device__ float z_localize(const SmemView &s, const TrackParams &P, float mean, float x, float y, int bead, int roi)
+// Starts the bulk copy of the next ROI's raw bytes into the tile region (thread 0; the CTA's reads
+// of the tile must be complete and ordered by a barrier). No-op when next_src is null.
+__device__ __forceinline__ void stage_next(uint8_t *tile, const TrackParams &P, const uint8_t *next_src, uint64_t *mbar)
+{
+    if (next_src && threadIdx.x == 0)
+        bulk_load(tile + P.sm_raw, next_src, (uint32_t)(P.width * P.height * (P.pdt == 0 ? 1 : (P.pdt == 1 ? 2 : 4))),
+                  mbar);
+}
+
+// Radial profile + Z-LUT compare (QueuedCPUTracker.cpp:319-338) on a tile of row pitch ts. Returns z
+// (0 without a LUT). With P.zprof_f32 set, the profile is written out for the tensor-core match instead.
+// When next_src is set, the next ROI's bulk copy into the tile region starts as soon as the
+// profile's samples are taken (the compare and fit do not read the tile).
+__device__ float z_localize(const SmemView &s, const TrackParams &P, int ts, float mean, float x, float y, int bead,
+                            int roi, const uint8_t *next_src = nullptr, uint64_t *mbar = nullptr)
 {
     const int nb = P.z_nbins;
     float *prof = reinterpret_cast<float *>(s.work);
@@ -124,8 +139,9 @@ __device__ float z_localize(const SmemView &s, const TrackParams &P, float mean,
     const float rstep = (P.z_maxr - P.z_minr) / (float)nb;
     load_z_tables(s, P);
     __syncthreads();
-    radial_profile(s.img, P.width, P.height, x, y, mean, nb, P.z_angsteps, P.z_minr, rstep, s.zdirs, prof,
+    radial_profile(s.img, P.width, P.height, ts, x, y, mean, nb, P.z_angsteps, P.z_minr, rstep, s.zdirs, prof,
                    (P.mode & kLT_NormalizeProfile) != 0, s.red);
+    stage_next(reinterpret_cast<uint8_t *>(s.img), P, next_src, mbar);
     if (P.zprof_f32) {
         // [hi | lo] BF16 split of the weighted profile: v = hi + lo + O(2^-16 v)
         __nv_bfloat16 *pb = static_cast<__nv_bfloat16 *>(P.zprof_bf16) + (size_t)roi * 2 * P.zprof_nbp;
@@ -187,18 +203,81 @@ __device__ __forceinline__ void write_result(LocalizationResult *results, int i,
     o[12] = __float_as_uint(mean);
 }
 
-// kGauss selects the instantiation: false = COM / QI (+ Z), true = 2D Gaussian MLE (+ Z).
-// Separate instantiations keep the QI path's register budget free of the MLE's FP64 solve.
 #ifndef QTRK_MIN_BLOCKS
 #define QTRK_MIN_BLOCKS 4
 #endif
 
-template <bool kGauss>
-__global__ void __launch_bounds__(kBlockThreads, QTRK_MIN_BLOCKS) localize_kernel(TrackParams P, const uint8_t *__restrict__ pixels,
-                                                                    int pitch, int64_t roi_stride,
-                                                                    const int64_t *__restrict__ roi_offsets,
-                                                                    const LocalizationJob *__restrict__ jobs, int count,
-                                                                    LocalizationResult *__restrict__ results)
+constexpr uint32_t kStageWaitLimit = 1u << 22;  // mbarrier polls before a staged copy counts as lost
+
+// COM / QI (+ Z): QueuedCPUTracker::ProcessJob (QueuedCPUTracker.cpp:273-361) for ROIs r =
+// blockIdx.x, blockIdx.x + gridDim.x, ... (the launcher sizes the grid to the CTAs that fit on
+// the GPU at once, so each CTA walks a queue of ROIs). Each ROI becomes a padded float tile in
+// shared memory: with P.stage_raw its raw bytes arrive by one bulk copy (cp.async.bulk, mbarrier
+// completion) that the CTA started while it was finishing the previous ROI's Z compare and fit,
+// and are converted in place; otherwise threads load them from global memory (frame bands,
+// unaligned or odd-width ROIs). The COM's first pass is fused into that conversion. kStaged
+// selects the form (one instantiation each, so neither carries the other's registers).
+template <bool kStaged>
+__global__ void __launch_bounds__(kBlockThreads, QTRK_MIN_BLOCKS)
+    localize_qi_kernel(TrackParams P, const uint8_t *__restrict__ pixels, int pitch, int64_t roi_stride,
+                       const int64_t *__restrict__ roi_offsets, const LocalizationJob *__restrict__ jobs, int count,
+                       LocalizationResult *__restrict__ results)
+{
+    extern __shared__ __align__(16) uint8_t smem[];
+    if ((int)blockIdx.x >= count) return;
+    const SmemView s = smem_view(smem, P);
+    uint8_t *tile = reinterpret_cast<uint8_t *>(s.img);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(reinterpret_cast<uint8_t *>(s.misc) + 32);
+    const int W = P.width, H = P.height, ts = P.sm_pitch;
+    constexpr bool staged = kStaged;
+    uint32_t parity = 0;
+    if (staged) {
+        if (threadIdx.x == 0) mbar_init(mbar);
+        __syncthreads();
+        stage_next(tile, P, pixels + (int64_t)blockIdx.x * roi_stride, mbar);
+    }
+    for (int roi = blockIdx.x; roi < count; roi += gridDim.x) {
+        const int next = roi + (int)gridDim.x;
+        const uint8_t *next_src = (staged && next < count) ? pixels + (int64_t)next * roi_stride : nullptr;
+        uint32_t job[6];
+        read_job(jobs, roi, job);
+        const int bead = (int)job[2];
+        load_qi_tables(s, P);
+        float2 part;
+        if constexpr (staged) {
+            if (!mbar_wait(mbar, parity, kStageWaitLimit) && P.err_flag) atomicOr(P.err_flag, 4u);
+            parity ^= 1u;
+            part = convert_staged_tile(s.img, ts, tile + P.sm_raw, P, bead);
+        } else {
+            const int64_t off = roi_offsets ? roi_offsets[roi] : (int64_t)roi * roi_stride;
+            part = load_roi_tile(s.img, ts, pixels + off, pitch, P, bead);
+        }
+        const ComResult com = com_tile(s.img, ts, W, H, part, P.com_bgcorrection, s.red);
+        float comx = com.x, comy = com.y;
+        if (isnan(comx) || isnan(comy)) {  // QueuedCPUTracker.cpp:294-295
+            comx = (float)(W / 2);
+            comy = (float)(H / 2);
+        }
+        float x = comx, y = comy, z = 0.0f;
+        bool bhit = false;
+        if (P.mode & kLT_QI) qi_localize(s, P, com.mean, x, y, bhit, P.qi_rweights);
+        if (P.mode & kLT_LocalizeZ) {
+            bhit = check_boundaries(x, y, P.z_maxr, W, H);
+            z = z_localize(s, P, ts, com.mean, x, y, bead, roi, next_src, mbar);
+        } else {
+            stage_next(tile, P, next_src, mbar);  // the last tile reads ended at a barrier
+        }
+        if (threadIdx.x == 0) write_result(results, roi, job, x, y, z, comx, comy, bhit ? 1u : 0u, com.mean);
+        __syncthreads();  // tables, work and misc are rewritten by the next ROI
+    }
+}
+
+// 2D Gaussian MLE (+ Z) for ROIs above 32x32 or with QI/Z bits: one CTA per ROI on a plain tile.
+// Kept apart from the QI kernel so that its register budget is free of the MLE's FP64 solve.
+__global__ void __launch_bounds__(kBlockThreads, QTRK_MIN_BLOCKS)
+    localize_gauss_kernel(TrackParams P, const uint8_t *__restrict__ pixels, int pitch, int64_t roi_stride,
+                          const int64_t *__restrict__ roi_offsets, const LocalizationJob *__restrict__ jobs, int count,
+                          LocalizationResult *__restrict__ results)
 {
     extern __shared__ __align__(16) uint8_t smem[];
     const int roi = blockIdx.x;
@@ -208,12 +287,9 @@ __global__ void __launch_bounds__(kBlockThreads, QTRK_MIN_BLOCKS) localize_kerne
     read_job(jobs, roi, job);
     const int bead = (int)job[2];
     const int64_t off = roi_offsets ? roi_offsets[roi] : (int64_t)roi * roi_stride;
-
-    load_qi_tables(s, P);
     BlockGroup g{s.red};
-    load_roi(g, s.img, pixels + off, pitch, P, bead);
-
     const int W = P.width, H = P.height;
+    load_roi(g, s.img, pixels + off, pitch, P, bead);
     const ComResult com = compute_com(g, s.img, W, H, P.com_bgcorrection);
     float comx = com.x, comy = com.y;
     if (isnan(comx) || isnan(comy)) {  // QueuedCPUTracker.cpp:294-295
@@ -222,24 +298,20 @@ __global__ void __launch_bounds__(kBlockThreads, QTRK_MIN_BLOCKS) localize_kerne
     }
     float x = comx, y = comy, z = 0.0f;
     bool bhit = false;
-    if (!kGauss) {
-        if (P.mode & kLT_QI) qi_localize(s, P, com.mean, x, y, bhit, P.qi_rweights);
+    float *col = reinterpret_cast<float *>(s.work);
+    if (P.mode & kLT_Gaussian5P) {
+        float p[5] = {x, y, com.mean * 0.5f * (float)(W * H), com.mean * 0.5f, P.g_sigma};
+        gauss5_mle(g, s.img, W, H, p, P.g_iterations, col, col + 3 * W);
+        x = p[0];
+        y = p[1];
+        z = p[4];
     } else {
-        float *col = reinterpret_cast<float *>(s.work);
-        if (P.mode & kLT_Gaussian5P) {
-            float p[5] = {x, y, com.mean * 0.5f * (float)(W * H), com.mean * 0.5f, P.g_sigma};
-            gauss5_mle(g, s.img, W, H, p, P.g_iterations, col, col + 3 * W);
-            x = p[0];
-            y = p[1];
-            z = p[4];
-        } else {
-            gauss4_mle(g, s.img, W, H, com.mean, x, y, P.g_iterations, P.g_sigma, col, col + 3 * W);
-        }
-        __syncthreads();
+        gauss4_mle(g, s.img, W, H, com.mean, x, y, P.g_iterations, P.g_sigma, col, col + 3 * W);
     }
+    __syncthreads();
     if (P.mode & kLT_LocalizeZ) {
         bhit = check_boundaries(x, y, P.z_maxr, W, H);
-        z = z_localize(s, P, com.mean, x, y, bead, roi);
+        z = z_localize(s, P, W, com.mean, x, y, bead, roi);
     }
     if (threadIdx.x == 0) write_result(results, roi, job, x, y, z, comx, comy, bhit ? 1u : 0u, com.mean);
 }
@@ -298,14 +370,15 @@ __global__ void __launch_bounds__(kBlockThreads) build_lut_kernel(TrackParams P,
     if (bead >= nbeads) return;
     const SmemView s = smem_view(smem, P);
     load_qi_tables(s, P);
-    BlockGroup g{s.red};
-    load_roi(g, s.img, pixels + (size_t)pitch * P.height * bead, pitch, P, bead);
+    const int ts = P.sm_pitch;
+    const float2 part = load_roi_tile(s.img, ts, pixels + (size_t)pitch * P.height * bead, pitch, P, bead);
     float x, y, mean = 0.0f;
     if (known_pos) {
+        __syncthreads();
         x = known_pos[bead].x;
         y = known_pos[bead].y;
     } else {
-        const ComResult com = compute_com(g, s.img, P.width, P.height, 0.0f);
+        const ComResult com = com_tile(s.img, ts, P.width, P.height, part, 0.0f, s.red);
         mean = com.mean;
         x = com.x;
         y = com.y;
@@ -318,7 +391,7 @@ __global__ void __launch_bounds__(kBlockThreads) build_lut_kernel(TrackParams P,
     __syncthreads();
     load_z_tables(s, P);
     __syncthreads();
-    radial_profile(s.img, P.width, P.height, x, y, mean, nb, P.z_angsteps, P.z_minr, rstep, s.zdirs, prof,
+    radial_profile(s.img, P.width, P.height, ts, x, y, mean, nb, P.z_angsteps, P.z_minr, rstep, s.zdirs, prof,
                    normalize != 0, s.red);
     float *dst = lut + ((size_t)bead * P.lut_planes + plane) * nb;
     for (int r = threadIdx.x; r < nb; r += blockDim.x) dst[r] += prof[r];
@@ -361,8 +434,8 @@ __global__ void __launch_bounds__(kBlockThreads) profile_kernel(TrackParams P, c
     load_roi(g, s.img, reinterpret_cast<const uint8_t *>(img_in), P.width * 4, P, -1);
     float *prof = reinterpret_cast<float *>(s.work);
     const float rstep = (P.z_maxr - P.z_minr) / (float)P.z_nbins;
-    radial_profile(s.img, P.width, P.height, cx, cy, mean, P.z_nbins, P.z_angsteps, P.z_minr, rstep, s.zdirs, prof,
-                   normalize != 0, s.red);
+    radial_profile(s.img, P.width, P.height, P.width, cx, cy, mean, P.z_nbins, P.z_angsteps, P.z_minr, rstep, s.zdirs,
+                   prof, normalize != 0, s.red);
     for (int r = threadIdx.x; r < P.z_nbins; r += blockDim.x) out[r] = prof[r];
 }
 
@@ -375,11 +448,17 @@ void plan_smem(TrackParams &P)
 {
     const int W = P.width, H = P.height;
     const int nr = P.qi_nr > 0 ? P.qi_nr : 1, L = 2 * nr;
+    P.sm_pitch = tile_pitch(W);
     P.sm_img = 0;
-    P.sm_tables = align16(W * H * 4);
+    // padded tile (the plain tile of the other kernels fits in it) + 16 bytes of slack, so that a
+    // staged raw ROI placed at the region's end, 16-byte aligned, starts after the float tile's
+    // last row would require (convert_staged_tile)
+    P.sm_tile_bytes = align16(H * P.sm_pitch * 4) + 16;
+    P.sm_tables = P.sm_tile_bytes;
     const int qi_tables = (P.qi_angpq + nr) * 8, z_tables = P.z_angsteps * 8;
     P.sm_work = P.sm_tables + align16(qi_tables > z_tables ? qi_tables : z_tables);
-    const int qi_work = 2 * L * 8;  // [ qprof | ac ] [ A ], qprof (16 nr bytes) fits in ac (8 L bytes)
+    // [ ac | A ] (L complex each) + 2 KB of subset partials when the QI directions are split over warps
+    const int qi_work = 2 * L * 8 + (nr < kBlockThreads / 4 ? 2048 : 0);
     const int z_work = align16(P.z_nbins * 4) + P.lut_planes * 8;
     const int g_work = (P.mode & kLT_Gaussian2D) ? (3 * W + 3 * H) * 4 : 0;
     int work = qi_work;
@@ -405,15 +484,50 @@ cudaError_t prepare_kernels(int device)
     if (g_attrs_set[device]) return cudaSuccess;
     const int max_smem = 227 * 1024;
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(localize_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)))
+    if ((e = cudaFuncSetAttribute(localize_qi_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)))
         return e;
-    if ((e = cudaFuncSetAttribute(localize_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)))
+    if ((e = cudaFuncSetAttribute(localize_qi_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)))
+        return e;
+    if ((e = cudaFuncSetAttribute(localize_gauss_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)))
         return e;
     if ((e = cudaFuncSetAttribute(build_lut_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem))) return e;
     if ((e = cudaFuncSetAttribute(profile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem))) return e;
     if ((e = cudaFuncSetAttribute(gauss_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem))) return e;
     g_attrs_set[device] = true;
     return cudaSuccess;
+}
+
+// CTAs of the QI kernel for `count` ROIs: as many as fit on the GPU at once (its ROI loop takes
+// the rest), looked up once per device and shared-memory size.
+static int qi_grid(int smem_bytes, int count)
+{
+    struct Entry {
+        int device, smem, ctas;
+    };
+    static std::mutex mu;
+    static Entry cache[16];
+    static int ncache = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int ctas = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        for (int i = 0; i < ncache; i++)
+            if (cache[i].device == dev && cache[i].smem == smem_bytes) ctas = cache[i].ctas;
+    }
+    if (ctas == 0) {
+        int per_sm = 0, sms = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, localize_qi_kernel<true>, kBlockThreads, smem_bytes) !=
+                cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || per_sm <= 0) {
+            cudaGetLastError();
+            return count;  // one CTA per ROI
+        }
+        ctas = per_sm * sms;
+        std::lock_guard<std::mutex> lk(mu);
+        if (ncache < 16) cache[ncache++] = Entry{dev, smem_bytes, ctas};
+    }
+    return count < ctas ? count : ctas;
 }
 
 bool use_gauss_warp(const TrackParams &P)
@@ -426,15 +540,29 @@ cudaError_t launch_localize(const TrackParams &P, const uint8_t *pixels, int pit
                             LocalizationResult *results, cudaStream_t stream)
 {
     if (count <= 0) return cudaSuccess;
+    if (use_com_kernel(P, pixels, pitch, roi_stride, roi_offsets))
+        return launch_com(P, pixels, roi_stride, jobs, count, results, stream);
     if (use_gauss_warp(P)) {
         gauss_warp_kernel<<<(count + 7) / 8, 256, gauss_warp_smem(P), stream>>>(P, pixels, pitch, roi_stride,
                                                                               roi_offsets, jobs, count, results);
     } else if ((P.mode & kLT_Gaussian2D) && !(P.mode & kLT_QI)) {
-        localize_kernel<true><<<count, kBlockThreads, P.smem_bytes, stream>>>(P, pixels, pitch, roi_stride,
+        localize_gauss_kernel<<<count, kBlockThreads, P.smem_bytes, stream>>>(P, pixels, pitch, roi_stride,
                                                                               roi_offsets, jobs, count, results);
     } else {
-        localize_kernel<false><<<count, kBlockThreads, P.smem_bytes, stream>>>(P, pixels, pitch, roi_stride,
-                                                                               roi_offsets, jobs, count, results);
+        TrackParams Q = P;
+        const int bpp = P.pdt == 0 ? 1 : (P.pdt == 1 ? 2 : 4);
+        const int64_t raw = (int64_t)P.width * P.height * bpp;
+        Q.stage_raw = !roi_offsets && pitch == P.width * bpp && !(P.width & 1) && P.width <= 256 &&
+                      !(reinterpret_cast<uintptr_t>(pixels) & 15) && !(roi_stride & 15) && !(raw & 15) &&
+                      raw <= P.sm_tile_bytes;
+        Q.sm_raw = Q.stage_raw ? (int)((P.sm_tile_bytes - raw) & ~(int64_t)15) : 0;
+        const int grid = qi_grid(P.smem_bytes, count);
+        if (Q.stage_raw)
+            localize_qi_kernel<true><<<grid, kBlockThreads, P.smem_bytes, stream>>>(Q, pixels, pitch, roi_stride,
+                                                                                   roi_offsets, jobs, count, results);
+        else
+            localize_qi_kernel<false><<<grid, kBlockThreads, P.smem_bytes, stream>>>(Q, pixels, pitch, roi_stride,
+                                                                                    roi_offsets, jobs, count, results);
     }
     return cudaGetLastError();
 }
@@ -522,8 +650,8 @@ void localize_node(const TrackParams &P, int count, cudaKernelNodeParams &kp)
         kp.blockDim = dim3(256);
         kp.sharedMemBytes = gauss_warp_smem(P);
     } else {
-        kp.func = (P.mode & kLT_Gaussian2D) && !(P.mode & kLT_QI) ? reinterpret_cast<void *>(localize_kernel<true>)
-                                                                   : reinterpret_cast<void *>(localize_kernel<false>);
+        kp.func = (P.mode & kLT_Gaussian2D) && !(P.mode & kLT_QI) ? reinterpret_cast<void *>(localize_gauss_kernel)
+                                                                   : reinterpret_cast<void *>(localize_qi_kernel<false>);
         kp.gridDim = dim3(count);
         kp.blockDim = dim3(kBlockThreads);
         kp.sharedMemBytes = P.smem_bytes;

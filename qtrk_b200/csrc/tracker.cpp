@@ -357,6 +357,7 @@ TrackParams Tracker::Params(int pdt) const
     P.calib_count = (d_calib_off_ || d_calib_gain_) ? calib_count_ : 0;
     P.offset_factor = offset_factor_;
     P.gain_factor = gain_factor_;
+    P.err_flag = d_err_;
     plan_smem(P);
     return P;
 }
@@ -698,10 +699,13 @@ void Tracker::CollectLocked()
     if (h_err_ && *h_err_) {
         const unsigned e = *h_err_;
         *h_err_ = 0;
-        Warn("tensor-core Z match: an MMA completion wait timed out; z of the affected ROIs is NaN");
+        if (e & 3u) Warn("tensor-core Z match: an MMA completion wait timed out; z of the affected ROIs is NaN");
         if (e & 2u)
             Warn("tensor-core Z match: the timed-out MMAs had not finished when their tensor-memory columns were "
                  "released; results of that launch are void");
+        if (e & 4u)
+            Warn("localization kernel: a staged ROI copy did not arrive within the wait limit; results of that "
+                 "launch are void");
     }
     while (!inflight_.empty()) {
         const int idx = inflight_.front();

@@ -179,6 +179,65 @@ def test_autograd_function_and_lut_steps():
         t.Destroy()
 
 
+def _crossing_free(xyz, cc, s, h):
+    """Per ROI and axis: True when moving that coordinate by +-h moves no profile sample across a
+    pixel edge (x, y: every bin's samples; z: no plane boundary), so the cost is smooth there and a
+    central difference converges to the derivative."""
+    n = cc.zlut_angularsteps
+    ang = 2 * float(np.float32(3.141593)) * np.arange(n) / n  # the oracle's FP64 sample positions
+    d = np.stack([np.cos(ang), np.sin(ang)], 1)
+    nb = cc.zlut_radialsteps
+    minr, maxr = float(s.zlut_minradius), float(cc.zlut_maxradius)
+    r = minr + (maxr - minr) / nb * np.arange(nb)
+    out = np.zeros((len(xyz), 3), bool)
+    for i, (x, y, z) in enumerate(xyz):
+        for k, c in ((0, x), (1, y)):
+            v = c + d[None, :, k] * r[:, None]
+            out[i, k] = (np.floor(v - h) == np.floor(v + h)).all()
+        out[i, 2] = np.floor(z - h) == np.floor(z + h)
+    return out
+
+
+def test_cost_gradient_tight_central_differences(port):
+    """The GPU gradient against FP64 central differences of the FP64 oracle's cost with step 1e-5,
+    on every (ROI, axis) where the step moves no sample across a pixel edge (there the cost is
+    smooth and the quotient is the derivative to ~1e-9): within 2e-3 of the largest gradient
+    component, the tolerance of the oracle-gradient comparison, for all of them. The oracle's
+    analytic gradient meets the same differences to 1e-6 relative."""
+    g, s, lut, mode, rois, t, w = _setup()
+    try:
+        loc = t.Localize(rois)
+        xyz = np.stack([loc["pos"][:, 0] + 0.2, loc["pos"][:, 1] - 0.15, loc["pos"][:, 2] + 0.3], 1)
+        xyz = xyz.astype(np.float32).astype(np.float64)
+        _, grad = _cost_grad(t, _device_rois(rois), xyz)
+    finally:
+        t.Destroy()
+    cc = port.computed_config(s)
+    h = 1e-5
+    smooth = _crossing_free(xyz, cc, s, h)
+    assert smooth[:, :2].mean() > 0.5, smooth.mean(0)
+    checked = 0
+    for i, img in enumerate(rois.astype(np.float64)):
+        mean = img.mean()
+        _, g64, _ = port.zcost_grad(img, mean, xyz[i], lut[0], cc.zlut_angularsteps, s.zlut_minradius,
+                                    cc.zlut_maxradius, normalize=True)
+        scale = np.abs(g64).max()
+        for k in range(3):
+            if not smooth[i, k]:
+                continue
+            e = np.zeros(3)
+            e[k] = h
+            cp = port.zcost_grad(img, mean, xyz[i] + e, lut[0], cc.zlut_angularsteps, s.zlut_minradius,
+                                 cc.zlut_maxradius, normalize=True)[0]
+            cm = port.zcost_grad(img, mean, xyz[i] - e, lut[0], cc.zlut_angularsteps, s.zlut_minradius,
+                                 cc.zlut_maxradius, normalize=True)[0]
+            fd = (cp - cm) / (2 * h)
+            assert abs(g64[k] - fd) <= 1e-6 * scale + 1e-9, (i, k, g64[k], fd)
+            assert abs(grad[i, k] - fd) <= 2e-3 * scale + 1e-5, (i, k, grad[i, k], fd)
+            checked += 1
+    assert checked >= len(rois)
+
+
 def test_joint_refine_mode_matches_oracle(port):
     g, s, lut, mode, rois, t, w = _setup()
     try:

@@ -373,3 +373,100 @@ def test_qi_angstep_factor_matches_reference(ref, shape, factor):
     # the factor changes the result: the same ROIs with factor 1 are localized differently
     r1 = ref.track(wl.settings, wl.mode, wl.rois, lut)
     assert np.abs(r1["pos"][:, :2] - r_ref["pos"][:, :2]).max() > 1e-6
+
+
+@pytest.mark.parametrize("case", ["roi100_u16", "roi60_f32", "u8_64", "u16_bgcorr", "f32_clear4", "u16_128"])
+def test_com_only_streaming_kernel_matches_reference(ref, case):
+    """LT_OnlyCOM on ROIs stored back to back runs the register-held streaming COM kernel (com.cu):
+    ComputeMeanAndCOM (cpu_tracker.cpp:681-729) against the reference tracker for u8/u16/f32 pixels,
+    row ends inside 16-byte chunks (60x60 f32 and 100x100 u16 rows are not whole chunks), the
+    background correction and ClearFirstFourPixels. COM within 1e-4 px, imageMean to 1e-6."""
+    rng = np.random.Generator(np.random.PCG64(77))
+    if case == "roi100_u16":
+        wl = synth.roi100_u16(400, seed=33)
+        s, rois = wl.settings, wl.rois
+    elif case == "roi60_f32":
+        wl = synth.roi60_f32(400, seed=34)
+        s, rois = wl.settings, wl.rois
+    elif case == "u8_64":
+        s = abi.settings(width=64, height=64)
+        rois = np.clip(rng.poisson(synth.render(64, 64, 32 + rng.uniform(-4, 4, 200), 32 + rng.uniform(-4, 4, 200),
+                                                rng.uniform(0, 10, 200), 20.0, 150.0)), 0, 255).astype(np.uint8)
+    elif case == "u16_bgcorr":
+        wl = synth.roi100_u16(300, seed=35)
+        s, rois = synth.settings_roi100(com_bgcorrection=0.7), wl.rois
+    elif case == "f32_clear4":
+        wl = synth.roi60_f32(200, seed=36)
+        s, rois = wl.settings, wl.rois
+    else:
+        s = abi.settings(width=128, height=128, com_bgcorrection=0.3)
+        rois = np.minimum(rng.poisson(synth.render(128, 128, 64 + rng.uniform(-6, 6, 100), 64 + rng.uniform(-6, 6, 100),
+                                                   rng.uniform(0, 20, 100), 200.0, 2000.0)), 65535).astype(np.uint16)
+    mode = abi.LT_OnlyCOM | (abi.LT_ClearFirstFourPixels if case == "f32_clear4" else 0)
+    r_ref = ref.track(s, mode, rois)
+    with make_tracker(s, mode) as t:
+        l0 = t.KernelLaunchCount()
+        r = t.Localize(rois)
+        assert t.KernelLaunchCount() > l0
+    assert np.abs(r["pos"][:, :2] - r_ref["pos"][:, :2]).max() < TOL_COM
+    assert np.abs(r["firstGuess"] - r_ref["firstGuess"]).max() < TOL_COM
+    assert (r["pos"][:, 2] == 0).all()
+    assert (r["error"] == r_ref["error"]).all()
+    np.testing.assert_allclose(r["imageMean"], r_ref["imageMean"], rtol=1e-6)
+    assert np.array_equal(r["frame"], r_ref["frame"])
+
+
+def test_com_only_full_size_equals_fused_kernel_com():
+    """Full BASELINE config-2 size (10,000 ROIs of 100x100 u16, device-resident): the streaming COM
+    kernel's positions and image means equal the COM stage of the fused localization kernel (its
+    firstGuess and imageMean in QI mode) within the COM tolerance, and frame indices run in order.
+    The fused kernel's COM is checked against the reference in the parity tests above."""
+    import torch
+
+    wl = synth.roi100_u16(10000, seed=37)
+    n = wl.rois.shape[0]
+    d = torch.from_numpy(wl.rois.view(np.int16)).cuda()
+    stream = torch.cuda.current_stream().cuda_stream
+    outs = {}
+    for mode in (abi.LT_OnlyCOM, abi.LT_QI):
+        with make_tracker(wl.settings, mode) as t:
+            out = torch.zeros(n * 52, dtype=torch.uint8, device="cuda")
+            t.LocalizeDevice(d.data_ptr(), 200, 20000, abi.QTrkU16, n, out.data_ptr(), stream=stream)
+            torch.cuda.synchronize()
+            outs[mode] = np.frombuffer(out.cpu().numpy().tobytes(), dtype=abi.RESULT_DTYPE)
+    com, fused = outs[abi.LT_OnlyCOM], outs[abi.LT_QI]
+    assert np.abs(com["pos"][:, :2] - fused["firstGuess"]).max() < TOL_COM
+    assert np.abs(com["firstGuess"] - fused["firstGuess"]).max() < TOL_COM
+    np.testing.assert_allclose(com["imageMean"], fused["imageMean"], rtol=1e-6)
+    np.testing.assert_array_equal(com["frame"], np.arange(n))
+    assert np.median(np.abs(com["pos"][:, 0] - wl.true_xyz[:, 0])) < 0.5
+
+
+def test_staged_and_direct_roi_loads_agree():
+    """The QI kernel brings ROIs stored back to back into shared memory by bulk copies (16-byte
+    aligned ROI stride) and loads them with per-thread reads otherwise; both give the same tile, so
+    results are bit-identical. 3,000 ROIs of 100x100 u16 (several ROIs per CTA), device-resident:
+    stride 20,000 bytes (staged) against 20,008 (ROIs 8 bytes apart: direct loads)."""
+    import torch
+
+    g = load("roi100_u16.npz")
+    wl = synth.roi100_u16(3000, seed=38)
+    n = wl.rois.shape[0]
+    stream = torch.cuda.current_stream().cuda_stream
+    packed = torch.from_numpy(wl.rois.view(np.int16).copy()).cuda()
+    spaced = torch.zeros((n, 10004), dtype=torch.int16, device="cuda")
+    spaced[:, :10000] = packed.view(n, 10000)
+    outs = []
+    with make_tracker(g["settings"], int(g["mode"]), g["lut"]) as t:
+        for buf, stride in ((packed, 20000), (spaced, 20008)):
+            out = torch.zeros(n * 52, dtype=torch.uint8, device="cuda")
+            t.LocalizeDevice(buf.data_ptr(), 200, stride, abi.QTrkU16, n, out.data_ptr(), stream=stream)
+            torch.cuda.synchronize()
+            outs.append(np.frombuffer(out.cpu().numpy().tobytes(), dtype=abi.RESULT_DTYPE))
+        t.GetResultCount()  # reads the instance's error word
+        assert "staged ROI copy" not in t.GetWarnings()
+    np.testing.assert_array_equal(outs[0]["pos"], outs[1]["pos"])
+    np.testing.assert_array_equal(outs[0]["firstGuess"], outs[1]["firstGuess"])
+    np.testing.assert_array_equal(outs[0]["imageMean"], outs[1]["imageMean"])
+    np.testing.assert_array_equal(outs[0]["error"], outs[1]["error"])
+    assert np.median(np.abs(outs[0]["pos"][:, 2] - wl.true_xyz[:, 2])) < 1.0
