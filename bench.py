@@ -722,6 +722,7 @@ def serving_bench(dev, main_trk, main_rois, seconds: float, fps: float) -> dict:
 def profile_workload(args) -> int:
     """Small device workloads for ncu captures (a few launches, a few hundred MB at most):
     tensorcore  2,048 ROIs 100x100 u16, COM + QI + Z with the tcgen05 Z match (LUT 200 x 64);
+    com         10,000 ROIs 100x100 u16 (200 MB), LT_OnlyCOM (the streaming COM kernel);
     gauss5      100,000 ROIs 16x16 f32, 5-parameter Gaussian MLE;
     adjoint     2,048 ROIs 100x100 u16, QTrkB200ZLUTCostGradient with the LUT gradient;
     beadconv    QTrkFindBeads on a 2048 x 2048 frame with a 100 px sample."""
@@ -733,7 +734,16 @@ def profile_workload(args) -> int:
     dev = torch.device("cuda", 0)
     stream = torch.cuda.current_stream(dev)
     total = args.warmup + args.steps
-    if args.profile_workload in ("tensorcore", "adjoint"):
+    if args.profile_workload == "com":
+        n = N_ROIS
+        wl = make_workload(n, seed=2)
+        d = torch.from_numpy(wl.rois.view(np.int16)).to(dev)
+        res = torch.empty(n * 52, dtype=torch.uint8, device=dev)
+        with QTrkInstance(wl.settings) as t:
+            t.SetLocalizationMode(abi.LT_OnlyCOM)
+            ms = _timed(stream, lambda: t.LocalizeDevice(d.data_ptr(), 200, 20000, abi.QTrkU16, n, res.data_ptr(),
+                                                         stream=stream.cuda_stream), args.steps, args.warmup)
+    elif args.profile_workload in ("tensorcore", "adjoint"):
         n = 2048
         wl = make_workload(n, seed=2)
         lut = build_lut_on_gpu(wl)
@@ -841,7 +851,7 @@ def main(argv=None) -> int:
     ap.add_argument("--fps", type=float, default=500.0, help="frame rate per instance in the serving runs")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-workloads", action="store_true", help="skip the Gaussian / BuildLUT / adjoint workloads")
-    ap.add_argument("--profile-workload", choices=["tensorcore", "gauss5", "adjoint", "beadconv"],
+    ap.add_argument("--profile-workload", choices=["com", "tensorcore", "gauss5", "adjoint", "beadconv"],
                     help="run one small device workload --steps times for a profiler and exit")
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)

@@ -690,7 +690,7 @@ __device__ __forceinline__ float lerp_cell(const float *row, int ts, int ix, flo
 // (cpu_tracker.cpp:327-343; X = [(q1+q2) reversed | q0+q3], Y = [(q2+q3) reversed | q0+q1]) as
 // one complex value z = X + iY per position, in bit-reversed order (log2L = log2(2 nr)) or in
 // natural order when log2L < 0. All threads call; a barrier must follow before A is read.
-__device__ inline void qi_profiles_sym(const float *img, int W, int H, int ts, float cx, float cy, float mean, int nr,
+__device__ __forceinline__ void qi_profiles_sym(const float *img, int W, int H, int ts, float cx, float cy, float mean, int nr,
                                        int nang, int stride, float minr, float rstep, const float2 *dirs,
                                        const float *rweights, float4 *part, float2 *A, int log2L)
 {
@@ -992,7 +992,7 @@ __device__ inline void qi_autoconv_direct_filled(int nr, const float2 *A, float2
 // bilinear samples on the full circle (FP64 sum), or `mean` when no more than 4 samples
 // are in bounds; then NormalizeRadialProfile (utils.cpp:230-261) when asked.
 // -------------------------------------------------------------------------------------
-__device__ inline void radial_profile(const float *img, int W, int H, int ts, float cx, float cy, float mean, int nb, int nang,
+__device__ __forceinline__ void radial_profile(const float *img, int W, int H, int ts, float cx, float cy, float mean, int nb, int nang,
                                float minr, float rstep, const float2 *dirs, float *prof, bool normalize,
                                double *red)
 {

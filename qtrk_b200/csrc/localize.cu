@@ -71,10 +71,10 @@ __device__ __forceinline__ void load_z_tables(const SmemView &s, const TrackPara
         for (int i = threadIdx.x; i < P.z_angsteps; i += blockDim.x) s.zdirs[i] = zd[i];
 }
 
-// CPUTracker::ComputeQI, cpu_tracker.cpp:285-360, on the padded tile (row pitch P.sm_pitch). All
-// threads call; returns the position and the boundary flag of the last iteration.
-__device__ void qi_localize(const SmemView &s, const TrackParams &P, float mean, float &cx, float &cy, bool &bhit,
-                            const float *rweights)
+// CPUTracker::ComputeQI, cpu_tracker.cpp:285-360, on the padded tile (row pitch ts). All threads
+// call; returns the position and the boundary flag of the last iteration.
+__device__ __forceinline__ void qi_localize(const SmemView &s, const TrackParams &P, int ts, float mean, float &cx,
+                                            float &cy, bool &bhit, const float *rweights)
 {
     const int W = P.width, H = P.height, nr = P.qi_nr, L = 2 * nr;
     const bool pow2 = (L & (L - 1)) == 0 && L >= 2;
@@ -85,7 +85,7 @@ __device__ void qi_localize(const SmemView &s, const TrackParams &P, float mean,
     const float rstep = (P.qi_maxr - P.qi_minr) / (float)nr;  // also pixelsPerProfLen (cpu_tracker.cpp:311,649)
     for (int k = 0; k < P.qi_iterations; k++) {
         bhit = check_boundaries(cx, cy, P.qi_maxr, W, H);
-        qi_profiles_sym(s.img, W, H, P.sm_pitch, cx, cy, mean, nr, P.qi_nang[k], P.qi_stride[k], P.qi_minr, rstep,
+        qi_profiles_sym(s.img, W, H, ts, cx, cy, mean, nr, P.qi_nang[k], P.qi_stride[k], P.qi_minr, rstep,
                         s.qdirs, rweights, part, A, pow2 ? ilog2_pow2(L) : -1);
         __syncthreads();
         if (pow2) {
@@ -130,8 +130,9 @@ __device__ __forceinline__ void stage_next(uint8_t *tile, const TrackParams &P, 
 // (0 without a LUT). With P.zprof_f32 set, the profile is written out for the tensor-core match instead.
 // When next_src is set, the next ROI's bulk copy into the tile region starts as soon as the
 // profile's samples are taken (the compare and fit do not read the tile).
-__device__ float z_localize(const SmemView &s, const TrackParams &P, int ts, float mean, float x, float y, int bead,
-                            int roi, const uint8_t *next_src = nullptr, uint64_t *mbar = nullptr)
+__device__ __forceinline__ float z_localize(const SmemView &s, const TrackParams &P, int ts, float mean, float x,
+                                            float y, int bead, int roi, const uint8_t *next_src = nullptr,
+                                            uint64_t *mbar = nullptr)
 {
     const int nb = P.z_nbins;
     float *prof = reinterpret_cast<float *>(s.work);
@@ -216,8 +217,10 @@ constexpr uint32_t kStageWaitLimit = 1u << 22;  // mbarrier polls before a stage
 // completion) that the CTA started while it was finishing the previous ROI's Z compare and fit,
 // and are converted in place; otherwise threads load them from global memory (frame bands,
 // unaligned or odd-width ROIs). The COM's first pass is fused into that conversion. kStaged
-// selects the form (one instantiation each, so neither carries the other's registers).
-template <bool kStaged>
+// selects the form (one instantiation each, so neither carries the other's registers). TS > 0
+// is the tile pitch as a compile-time constant (tile_pitch of a common ROI width: the gathers'
+// second-row offsets become immediates), 0 takes P.sm_pitch.
+template <bool kStaged, int TS>
 __global__ void __launch_bounds__(kBlockThreads, QTRK_MIN_BLOCKS)
     localize_qi_kernel(TrackParams P, const uint8_t *__restrict__ pixels, int pitch, int64_t roi_stride,
                        const int64_t *__restrict__ roi_offsets, const LocalizationJob *__restrict__ jobs, int count,
@@ -228,7 +231,7 @@ __global__ void __launch_bounds__(kBlockThreads, QTRK_MIN_BLOCKS)
     const SmemView s = smem_view(smem, P);
     uint8_t *tile = reinterpret_cast<uint8_t *>(s.img);
     uint64_t *mbar = reinterpret_cast<uint64_t *>(reinterpret_cast<uint8_t *>(s.misc) + 32);
-    const int W = P.width, H = P.height, ts = P.sm_pitch;
+    const int W = P.width, H = P.height, ts = TS > 0 ? TS : P.sm_pitch;
     constexpr bool staged = kStaged;
     uint32_t parity = 0;
     if (staged) {
@@ -260,7 +263,7 @@ __global__ void __launch_bounds__(kBlockThreads, QTRK_MIN_BLOCKS)
         }
         float x = comx, y = comy, z = 0.0f;
         bool bhit = false;
-        if (P.mode & kLT_QI) qi_localize(s, P, com.mean, x, y, bhit, P.qi_rweights);
+        if (P.mode & kLT_QI) qi_localize(s, P, ts, com.mean, x, y, bhit, P.qi_rweights);
         if (P.mode & kLT_LocalizeZ) {
             bhit = check_boundaries(x, y, P.z_maxr, W, H);
             z = z_localize(s, P, ts, com.mean, x, y, bead, roi, next_src, mbar);
@@ -383,7 +386,7 @@ __global__ void __launch_bounds__(kBlockThreads) build_lut_kernel(TrackParams P,
         x = com.x;
         y = com.y;
         bool bhit;
-        qi_localize(s, P, mean, x, y, bhit, nullptr);
+        qi_localize(s, P, ts, mean, x, y, bhit, nullptr);
     }
     const int nb = P.z_nbins;
     float *prof = reinterpret_cast<float *>(s.work);
@@ -476,6 +479,24 @@ int gauss_warp_smem(const TrackParams &P)
     return 8 * ((W * H + 3 * (W + H) + 3) & ~3) * 4;
 }
 
+using QIKernel = void (*)(TrackParams, const uint8_t *, int, int64_t, const int64_t *, const LocalizationJob *, int,
+                          LocalizationResult *);
+
+// The QI kernel for a launch: staged ROIs get a compile-time tile pitch for the common ROI widths
+// (40, 60/64, 80, 100 and 128 px).
+static QIKernel qi_kernel(bool staged, int pitch)
+{
+    if (!staged) return localize_qi_kernel<false, 0>;
+    switch (pitch) {
+    case 44: return localize_qi_kernel<true, 44>;
+    case 70: return localize_qi_kernel<true, 70>;
+    case 84: return localize_qi_kernel<true, 84>;
+    case 102: return localize_qi_kernel<true, 102>;
+    case 134: return localize_qi_kernel<true, 134>;
+    default: return localize_qi_kernel<true, 0>;
+    }
+}
+
 static bool g_attrs_set[64];
 
 cudaError_t prepare_kernels(int device)
@@ -484,10 +505,9 @@ cudaError_t prepare_kernels(int device)
     if (g_attrs_set[device]) return cudaSuccess;
     const int max_smem = 227 * 1024;
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(localize_qi_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)))
-        return e;
-    if ((e = cudaFuncSetAttribute(localize_qi_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)))
-        return e;
+    for (const QIKernel f : {qi_kernel(true, 0), qi_kernel(true, 44), qi_kernel(true, 70), qi_kernel(true, 84),
+                             qi_kernel(true, 102), qi_kernel(true, 134), qi_kernel(false, 0)})
+        if ((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem))) return e;
     if ((e = cudaFuncSetAttribute(localize_gauss_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)))
         return e;
     if ((e = cudaFuncSetAttribute(build_lut_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem))) return e;
@@ -517,7 +537,7 @@ static int qi_grid(int smem_bytes, int count)
     }
     if (ctas == 0) {
         int per_sm = 0, sms = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, localize_qi_kernel<true>, kBlockThreads, smem_bytes) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qi_kernel(true, 0), kBlockThreads, smem_bytes) !=
                 cudaSuccess ||
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || per_sm <= 0) {
             cudaGetLastError();
@@ -557,12 +577,8 @@ cudaError_t launch_localize(const TrackParams &P, const uint8_t *pixels, int pit
                       raw <= P.sm_tile_bytes;
         Q.sm_raw = Q.stage_raw ? (int)((P.sm_tile_bytes - raw) & ~(int64_t)15) : 0;
         const int grid = qi_grid(P.smem_bytes, count);
-        if (Q.stage_raw)
-            localize_qi_kernel<true><<<grid, kBlockThreads, P.smem_bytes, stream>>>(Q, pixels, pitch, roi_stride,
-                                                                                   roi_offsets, jobs, count, results);
-        else
-            localize_qi_kernel<false><<<grid, kBlockThreads, P.smem_bytes, stream>>>(Q, pixels, pitch, roi_stride,
-                                                                                    roi_offsets, jobs, count, results);
+        qi_kernel(Q.stage_raw != 0, Q.sm_pitch)<<<grid, kBlockThreads, P.smem_bytes, stream>>>(
+            Q, pixels, pitch, roi_stride, roi_offsets, jobs, count, results);
     }
     return cudaGetLastError();
 }
@@ -651,7 +667,7 @@ void localize_node(const TrackParams &P, int count, cudaKernelNodeParams &kp)
         kp.sharedMemBytes = gauss_warp_smem(P);
     } else {
         kp.func = (P.mode & kLT_Gaussian2D) && !(P.mode & kLT_QI) ? reinterpret_cast<void *>(localize_gauss_kernel)
-                                                                   : reinterpret_cast<void *>(localize_qi_kernel<false>);
+                                                                   : reinterpret_cast<void *>(qi_kernel(false, 0));
         kp.gridDim = dim3(count);
         kp.blockDim = dim3(kBlockThreads);
         kp.sharedMemBytes = P.smem_bytes;
