@@ -12,14 +12,7 @@
 
 #include "track_params.h"
 
-#ifndef QTRK_SAMPLE_UNROLL
-#define QTRK_SAMPLE_UNROLL 1
-#endif
-
 namespace qtrk {
-
-constexpr int kSampleUnroll = QTRK_SAMPLE_UNROLL;  // angular samples per unrolled step of the QI loops
-// (measured on 10,000 100x100 ROIs: 1 -> 1.236 ms, 2 -> 1.251, 3 -> 1.271, 4 -> 1.278)
 
 // -------------------------------------------------------------------------------------
 // small helpers
@@ -256,8 +249,11 @@ __device__ __forceinline__ float finish_pixel(float v, int i, const TrackParams 
     return v;
 }
 
+// Returns this thread's FP32 partial sums of v and v^2 over the pixels it converted (the first pass
+// of CPUTracker::ComputeMeanAndCOM, cpu_tracker.cpp:687-693, so that com_from_sums need not read
+// the tile again for them; callers that do not use them pay nothing once the call is inlined).
 template <class G>
-__device__ inline void load_roi(const G &g, float *img, const uint8_t *src, int pitch, const TrackParams &P, int bead)
+__device__ inline float2 load_roi(const G &g, float *img, const uint8_t *src, int pitch, const TrackParams &P, int bead)
 {
     const int W = P.width, H = P.height, n = W * H;
     const int bpp = P.pdt == 0 ? 1 : (P.pdt == 1 ? 2 : 4);
@@ -268,6 +264,7 @@ __device__ inline void load_roi(const G &g, float *img, const uint8_t *src, int 
     }
     const bool contiguous = pitch == W * bpp && ((reinterpret_cast<uintptr_t>(src) & 15) == 0) &&
                             ((n * bpp) & 15) == 0 && ((reinterpret_cast<uintptr_t>(img) & 15) == 0);
+    float s = 0.0f, s2 = 0.0f;
     if (contiguous) {
         // Rows are back to back: the ROI is a run of n/4 chunks of four pixels (4, 8 or 16 input
         // bytes), and chunk c becomes the float4 at img + 4c, so a warp's stores fill 512
@@ -284,6 +281,14 @@ __device__ inline void load_roi(const G &g, float *img, const uint8_t *src, int 
                 f.z = finish_pixel(f.z, 4 * c + 2, P, off, gain);
                 f.w = finish_pixel(f.w, 4 * c + 3, P, off, gain);
             }
+            s += f.x;
+            s2 = fmaf(f.x, f.x, s2);
+            s += f.y;
+            s2 = fmaf(f.y, f.y, s2);
+            s += f.z;
+            s2 = fmaf(f.z, f.z, s2);
+            s += f.w;
+            s2 = fmaf(f.w, f.w, s2);
             dst[c] = f;
         };
         if (P.pdt == 0) {
@@ -358,11 +363,93 @@ __device__ inline void load_roi(const G &g, float *img, const uint8_t *src, int 
                 else
                     v = reinterpret_cast<const float *>(row)[x];
                 const int i = y * W + x;
-                img[i] = finish_pixel(v, i, P, off, gain);
+                v = finish_pixel(v, i, P, off, gain);
+                s += v;
+                s2 = fmaf(v, v, s2);
+                img[i] = v;
             }
         }
     }
     g.sync();
+    return make_float2(s, s2);
+}
+
+// load_roi for a ROI whose raw bytes (n = W*H pixels, u8/u16/f32, rows back to back) were brought
+// into shared memory by a bulk copy to img + (4 - bpp) n bytes, the end of the float tile. The
+// conversion runs in place in batches of kBatch chunks of four pixels per thread: a batch's raw
+// chunks are read into registers, a barrier passes, and the batch's float chunks are written.
+// Float chunk c (bytes 16c .. 16c+15) overlaps only raw chunks with index <= c, which the batch or
+// an earlier one has already read, so a batch never overwrites raw bytes a later batch needs. The
+// per-pixel steps and the returned partial sums are load_roi's. Requires n a multiple of 4. All
+// threads call; the tile is complete at return.
+template <class G>
+__device__ inline float2 convert_staged(const G &g, float *img, const TrackParams &P, int bead)
+{
+    const int W = P.width, H = P.height, n = W * H, nc = n >> 2;
+    const int bpp = P.pdt == 0 ? 1 : (P.pdt == 1 ? 2 : 4);
+    const uint8_t *raw = reinterpret_cast<const uint8_t *>(img) + (size_t)(4 - bpp) * n;
+    const float *off = nullptr, *gain = nullptr;
+    if (bead >= 0 && bead < P.calib_count) {
+        if (P.calib_offset) off = P.calib_offset + (size_t)bead * n;
+        if (P.calib_gain) gain = P.calib_gain + (size_t)bead * n;
+    }
+    const bool plain = !off && !gain && !(P.mode & kLT_ClearFirstFourPixels);
+    float4 *dst = reinterpret_cast<float4 *>(img);
+    float s = 0.0f, s2 = 0.0f;
+    constexpr int kBatch = 8;
+    // every thread runs the same number of batches (the loop holds a barrier)
+    for (int b0 = 0; b0 < nc; b0 += kBatch * g.size()) {
+        const int c0 = b0 + g.rank();
+        uint4 q[kBatch];
+#pragma unroll
+        for (int k = 0; k < kBatch; k++) {
+            const int c = c0 + k * g.size();
+            if (c < nc) {
+                if (P.pdt == 0) {
+                    q[k].x = reinterpret_cast<const uint32_t *>(raw)[c];
+                } else if (P.pdt == 1) {
+                    const uint2 v = reinterpret_cast<const uint2 *>(raw)[c];
+                    q[k].x = v.x;
+                    q[k].y = v.y;
+                } else {
+                    q[k] = reinterpret_cast<const uint4 *>(raw)[c];
+                }
+            }
+        }
+        g.sync();
+#pragma unroll
+        for (int k = 0; k < kBatch; k++) {
+            const int c = c0 + k * g.size();
+            if (c >= nc) continue;
+            float4 f;
+            if (P.pdt == 0)
+                f = make_float4(u_to_float(q[k].x & 0xffu), u_to_float((q[k].x >> 8) & 0xffu),
+                                u_to_float((q[k].x >> 16) & 0xffu), u_to_float(q[k].x >> 24));
+            else if (P.pdt == 1)
+                f = make_float4(u_to_float(q[k].x & 0xffffu), u_to_float(q[k].x >> 16), u_to_float(q[k].y & 0xffffu),
+                                u_to_float(q[k].y >> 16));
+            else
+                f = make_float4(__uint_as_float(q[k].x), __uint_as_float(q[k].y), __uint_as_float(q[k].z),
+                                __uint_as_float(q[k].w));
+            if (!plain) {
+                f.x = finish_pixel(f.x, 4 * c, P, off, gain);
+                f.y = finish_pixel(f.y, 4 * c + 1, P, off, gain);
+                f.z = finish_pixel(f.z, 4 * c + 2, P, off, gain);
+                f.w = finish_pixel(f.w, 4 * c + 3, P, off, gain);
+            }
+            s += f.x;
+            s2 = fmaf(f.x, f.x, s2);
+            s += f.y;
+            s2 = fmaf(f.y, f.y, s2);
+            s += f.z;
+            s2 = fmaf(f.z, f.z, s2);
+            s += f.w;
+            s2 = fmaf(f.w, f.w, s2);
+            dst[c] = f;
+        }
+    }
+    g.sync();
+    return make_float2(s, s2);
 }
 
 // -------------------------------------------------------------------------------------
@@ -373,22 +460,19 @@ struct ComResult {
     float x, y, mean, stdev;
 };
 
+// From this thread's partial sums of v and v^2 (first pass, part) and the tile: the FP64 sums
+// across the group, mean and stdev as the reference rounds them, then the background-corrected
+// moments. Each thread walks a fixed set of pixels with its column/row as float counters, keeps
+// FP32 partial sums over its few dozen pixels, and the partials are added in FP64 across the
+// group (the reference accumulates the whole image in FP64; the partial sums keep its result
+// to ~1e-7 relative, far inside the 1e-4 px COM tolerance; for integer pixels the first pass's
+// partial sums, and so the mean, are exact).
 template <class G>
-__device__ ComResult compute_com(const G &g, const float *img, int W, int H, float bgcorr)
+__device__ ComResult com_from_sums(const G &g, const float *img, int W, int H, float2 part, float bgcorr)
 {
-    // Each thread walks a fixed set of pixels with its column/row as float counters, keeps
-    // FP32 partial sums over its few dozen pixels, and the partials are added in FP64 across
-    // the group (the reference accumulates the whole image in FP64; the partial sums keep
-    // its result to ~1e-7 relative, far inside the 1e-4 px COM tolerance).
     const int n = W * H, stride = g.size();
     const int dx = stride % W, dy = stride / W;
-    float p0 = 0.0f, p1 = 0.0f;
-    for (int i = g.rank(); i < n; i += stride) {
-        const float v = img[i];
-        p0 += v;
-        p1 += v * v;
-    }
-    double s[2] = {p0, p1};
+    double s[2] = {part.x, part.y};
     g.sum(s);
     const float invN = 1.0f / (float)n;
     ComResult r;
@@ -421,247 +505,16 @@ __device__ ComResult compute_com(const G &g, const float *img, int W, int H, flo
     return r;
 }
 
-// -------------------------------------------------------------------------------------
-// Padded ROI tile for the sampling kernels. Row y of the float tile starts at img + y * ts,
-// with ts >= W even (8-byte aligned rows for float2 stores) and ts mod 32 in {6, 12, 20, 26}:
-// a warp's bilinear gathers cover a patch a few pixels wide and high around the sample points,
-// and with these pitches the rows of such a patch fall on different banks (simulated for the
-// QI and radial-profile lane layouts below on 60-200 px ROIs: ~1.3-1.4 shared-memory wavefronts
-// per gather, against 1.6 at W = 100 and up to 5 at W = 64 or 128 without padding).
-// -------------------------------------------------------------------------------------
-__host__ __device__ inline int tile_pitch(int W)
+template <class G>
+__device__ ComResult compute_com(const G &g, const float *img, int W, int H, float bgcorr)
 {
-    for (int p = W + (W & 1);; p += 2) {
-        const int m = p & 31;
-        if (m == 6 || m == 12 || m == 20 || m == 26) return p;
+    float p0 = 0.0f, p1 = 0.0f;
+    for (int i = g.rank(); i < W * H; i += g.size()) {
+        const float v = img[i];
+        p0 += v;
+        p1 += v * v;
     }
-}
-
-// Load a ROI into the padded tile (pitch ts) with the per-pixel steps of load_roi (conversion,
-// ClearFirstFourPixels, offset/gain), and return this thread's FP32 partial sums of v and v^2
-// over the pixels it converted (the first pass of CPUTracker::ComputeMeanAndCOM,
-// cpu_tracker.cpp:687-693), so the tile is not read again for them. Warps take rows, lanes take
-// pixel pairs along a row (two rows per step, all of a step's loads issued before any is used);
-// each pair is one 2/4/8-byte streaming load and one conflict-free float2 store. Rows of odd
-// width or unaligned rows are read pixel by pixel. Every thread of the CTA calls; a barrier
-// must follow before the tile is read.
-__device__ inline float2 load_roi_tile(float *img, int ts, const uint8_t *src, int pitch, const TrackParams &P,
-                                       int bead)
-{
-    const int W = P.width, H = P.height, n = W * H;
-    const int bpp = P.pdt == 0 ? 1 : (P.pdt == 1 ? 2 : 4);
-    const float *off = nullptr, *gain = nullptr;
-    if (bead >= 0 && bead < P.calib_count) {
-        if (P.calib_offset) off = P.calib_offset + (size_t)bead * n;
-        if (P.calib_gain) gain = P.calib_gain + (size_t)bead * n;
-    }
-    const bool plain = !off && !gain && !(P.mode & kLT_ClearFirstFourPixels);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    float s = 0.0f, s2 = 0.0f;
-    constexpr int kMaxPairsPerLane = 4;  // rows up to 256 pixels (wider rows: pixel by pixel)
-    const bool pairs = !(W & 1) && W <= 64 * kMaxPairsPerLane && !(reinterpret_cast<uintptr_t>(src) & (2 * bpp - 1)) &&
-                       !(pitch & (2 * bpp - 1));
-    if (pairs) {
-        const int np = W >> 1, mp = (np + 31) >> 5;
-        for (int y0 = warp; y0 < H; y0 += 2 * nw) {
-            uint2 q[2][kMaxPairsPerLane];
-#pragma unroll
-            for (int r = 0; r < 2; r++) {
-                const int y = y0 + r * nw;
-                const uint8_t *row = src + (size_t)y * pitch;
-#pragma unroll
-                for (int m = 0; m < kMaxPairsPerLane; m++) {
-                    const int k = lane + 32 * m;
-                    if (m < mp && y < H && k < np) {
-                        if (P.pdt == 0)
-                            q[r][m].x = __ldcs(reinterpret_cast<const unsigned short *>(row) + k);
-                        else if (P.pdt == 1)
-                            q[r][m].x = __ldcs(reinterpret_cast<const unsigned int *>(row) + k);
-                        else
-                            q[r][m] = __ldcs(reinterpret_cast<const uint2 *>(row) + k);
-                    }
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < 2; r++) {
-                const int y = y0 + r * nw;
-#pragma unroll
-                for (int m = 0; m < kMaxPairsPerLane; m++) {
-                    const int k = lane + 32 * m;
-                    if (m < mp && y < H && k < np) {
-                        float a, b;
-                        if (P.pdt == 0) {
-                            a = u_to_float(q[r][m].x & 0xffu);
-                            b = u_to_float((q[r][m].x >> 8) & 0xffu);
-                        } else if (P.pdt == 1) {
-                            a = u_to_float(q[r][m].x & 0xffffu);
-                            b = u_to_float(q[r][m].x >> 16);
-                        } else {
-                            a = __uint_as_float(q[r][m].x);
-                            b = __uint_as_float(q[r][m].y);
-                        }
-                        if (!plain) {
-                            a = finish_pixel(a, y * W + 2 * k, P, off, gain);
-                            b = finish_pixel(b, y * W + 2 * k + 1, P, off, gain);
-                        }
-                        s += a;
-                        s2 = fmaf(a, a, s2);
-                        s += b;
-                        s2 = fmaf(b, b, s2);
-                        reinterpret_cast<float2 *>(img + y * ts)[k] = make_float2(a, b);
-                    }
-                }
-            }
-        }
-    } else {
-        for (int y = warp; y < H; y += nw) {
-            const uint8_t *row = src + (size_t)y * pitch;
-            for (int x = lane; x < W; x += 32) {
-                float v;
-                if (P.pdt == 0)
-                    v = u_to_float(row[x]);
-                else if (P.pdt == 1)
-                    v = u_to_float(reinterpret_cast<const uint16_t *>(row)[x]);
-                else
-                    v = reinterpret_cast<const float *>(row)[x];
-                v = finish_pixel(v, y * W + x, P, off, gain);
-                s += v;
-                s2 = fmaf(v, v, s2);
-                img[y * ts + x] = v;
-            }
-        }
-    }
-    return make_float2(s, s2);
-}
-
-// load_roi_tile for a ROI whose raw rows already sit in shared memory, back to back, at
-// `raw` inside the tile region (placed at the region's end, so that raw row y starts at or after
-// the end of float row y - 1: see plan_smem). Rows are converted in groups of 2 x warps rows:
-// each group's raw pixel pairs are read into registers, a barrier passes, then the group's float
-// rows are written (they may overlap the group's own raw rows but never a later group's). W must
-// be even. Every thread calls; the tile is complete at return (a barrier ends the last group).
-__device__ inline float2 convert_staged_tile(float *img, int ts, const uint8_t *raw, const TrackParams &P, int bead)
-{
-    const int W = P.width, H = P.height, n = W * H;
-    const int bpp = P.pdt == 0 ? 1 : (P.pdt == 1 ? 2 : 4);
-    const float *off = nullptr, *gain = nullptr;
-    if (bead >= 0 && bead < P.calib_count) {
-        if (P.calib_offset) off = P.calib_offset + (size_t)bead * n;
-        if (P.calib_gain) gain = P.calib_gain + (size_t)bead * n;
-    }
-    const bool plain = !off && !gain && !(P.mode & kLT_ClearFirstFourPixels);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    constexpr int kMaxPairsPerLane = 4;  // rows up to 256 pixels
-    const int np = W >> 1, mp = (np + 31) >> 5;
-    float s = 0.0f, s2 = 0.0f;
-    for (int y0 = 0; y0 < H; y0 += 2 * nw) {
-        uint2 q[2][kMaxPairsPerLane];
-#pragma unroll
-        for (int r = 0; r < 2; r++) {
-            const int y = y0 + warp + r * nw;
-            const uint8_t *row = raw + (size_t)y * W * bpp;
-#pragma unroll
-            for (int m = 0; m < kMaxPairsPerLane; m++) {
-                const int k = lane + 32 * m;
-                if (m < mp && y < H && k < np) {
-                    if (P.pdt == 0)
-                        q[r][m].x = reinterpret_cast<const unsigned short *>(row)[k];
-                    else if (P.pdt == 1)
-                        q[r][m].x = reinterpret_cast<const unsigned int *>(row)[k];
-                    else
-                        q[r][m] = reinterpret_cast<const uint2 *>(row)[k];
-                }
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int r = 0; r < 2; r++) {
-            const int y = y0 + warp + r * nw;
-#pragma unroll
-            for (int m = 0; m < kMaxPairsPerLane; m++) {
-                const int k = lane + 32 * m;
-                if (m < mp && y < H && k < np) {
-                    float a, b;
-                    if (P.pdt == 0) {
-                        a = u_to_float(q[r][m].x & 0xffu);
-                        b = u_to_float((q[r][m].x >> 8) & 0xffu);
-                    } else if (P.pdt == 1) {
-                        a = u_to_float(q[r][m].x & 0xffffu);
-                        b = u_to_float(q[r][m].x >> 16);
-                    } else {
-                        a = __uint_as_float(q[r][m].x);
-                        b = __uint_as_float(q[r][m].y);
-                    }
-                    if (!plain) {
-                        a = finish_pixel(a, y * W + 2 * k, P, off, gain);
-                        b = finish_pixel(b, y * W + 2 * k + 1, P, off, gain);
-                    }
-                    s += a;
-                    s2 = fmaf(a, a, s2);
-                    s += b;
-                    s2 = fmaf(b, b, s2);
-                    reinterpret_cast<float2 *>(img + y * ts)[k] = make_float2(a, b);
-                }
-            }
-        }
-        __syncthreads();
-    }
-    return make_float2(s, s2);
-}
-
-// CPUTracker::ComputeMeanAndCOM (cpu_tracker.cpp:681-729) on a padded tile whose pass-1 partial
-// sums (v, v^2) come from load_roi_tile: mean and stdev as the reference rounds them, then the
-// background-corrected moments over the tile (rows by warps, pixel pairs by lanes), FP32 per
-// thread and FP64 across the CTA. All threads call; every thread gets the result.
-__device__ inline ComResult com_tile(const float *img, int ts, int W, int H, float2 part, float bgcorr, double *red)
-{
-    BlockGroup g{red};
-    double s[2] = {part.x, part.y};
-    g.sum(s);
-    const int n = W * H;
-    const float invN = 1.0f / (float)n;
-    ComResult r;
-    r.mean = (float)(s[0] * (double)invN);
-    r.stdev = sqrtf((float)(s[1] * (double)invN - (double)(r.mean * r.mean)));
-    const float thr = bgcorr * r.stdev;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    float q0 = 0.0f, qx = 0.0f, qy = 0.0f;
-    if (!(W & 1)) {
-        const int np = W >> 1;
-        for (int y = warp; y < H; y += nw) {
-            const float2 *row = reinterpret_cast<const float2 *>(img + y * ts);
-            float r0 = 0.0f, rx = 0.0f;
-            for (int k = lane; k < np; k += 32) {
-                const float2 v = row[k];
-                const float a = fmaxf(0.0f, fabsf(v.x - r.mean) - thr);
-                const float b = fmaxf(0.0f, fabsf(v.y - r.mean) - thr);
-                const float x = (float)(2 * k);
-                r0 += a + b;
-                rx = fmaf(x, a, rx);
-                rx = fmaf(x + 1.0f, b, rx);
-            }
-            q0 += r0;
-            qx += rx;
-            qy = fmaf((float)y, r0, qy);
-        }
-    } else {
-        for (int y = warp; y < H; y += nw) {
-            float r0 = 0.0f, rx = 0.0f;
-            for (int x = lane; x < W; x += 32) {
-                const float a = fmaxf(0.0f, fabsf(img[y * ts + x] - r.mean) - thr);
-                r0 += a;
-                rx = fmaf((float)x, a, rx);
-            }
-            q0 += r0;
-            qx += rx;
-            qy = fmaf((float)y, r0, qy);
-        }
-    }
-    double m[3] = {q0, qx, qy};
-    g.sum(m);
-    r.x = (float)(m[1] / m[0]);
-    r.y = (float)(m[2] / m[0]);
-    return r;
+    return com_from_sums(g, img, W, H, make_float2(p0, p1), bgcorr);
 }
 
 // Bilinear value at a sample whose truncated corner (ix, row) and fractions are known: row points
@@ -683,7 +536,7 @@ __device__ __forceinline__ float lerp_cell(const float *row, int ts, int ix, flo
 // coordinates are shared by four samples. Coordinates are formed as the reference forms them
 // (d.x r rounded, then added to the centre). Layout: S = blockDim/nr direction subsets
 // (directions sub, sub + S, ...); a warp holds R = 32/A radii x A = min(S, 4) adjacent subsets,
-// so its gathers fall into a small patch (see tile_pitch). Per quadrant and radius the bin value
+// so its gathers fall into a small patch. Per quadrant and radius the bin value
 // is the mean of the in-bounds samples (the image mean when fewer than 4), times the radial
 // weight; the subsets' partial sums meet through warp shuffles (and `part`, 2 KB of shared
 // memory, when S > A). The thread of subset 0 writes the X and Y concatenations
@@ -704,9 +557,13 @@ __device__ __forceinline__ void qi_profiles_sym(const float *img, int W, int H, 
         const int i = rb * R + lane / Aw, sub = sb * Aw + lane % Aw;
         float sm[4] = {0.0f, 0.0f, 0.0f, 0.0f};
         int cnt[4] = {0, 0, 0, 0};
+        const float r = __fadd_rn(minr, __fmul_rn(rstep, (float)i));
+        // One path per warp: when any lane's circle may leave the image, the whole warp takes the
+        // checked body (a warp running both bodies one after the other would hold up the CTA's
+        // other warps at the next barrier).
+        const bool fast = __all_sync(0xffffffffu, i >= nr || circle_inside(cx, cy, fabsf(r), W, H));
         if (i < nr) {
-            const float r = __fadd_rn(minr, __fmul_rn(rstep, (float)i));
-            if (circle_inside(cx, cy, fabsf(r), W, H)) {
+            if (fast) {
                 for (int a = sub; a < nang; a += S) {
                     const float2 d = dirs[stride * a];
                     const float dx = __fmul_rn(d.x, r), dy = __fmul_rn(d.y, r);
@@ -727,18 +584,38 @@ __device__ __forceinline__ void qi_profiles_sym(const float *img, int W, int H, 
                 const int c = sub < nang ? (nang - sub + S - 1) / S : 0;
                 cnt[0] = cnt[1] = cnt[2] = cnt[3] = c;
             } else {
+                // bilinear()'s rule per coordinate: a sample is inside when -1 < x < W-1 and
+                // -1 < y < H-1, and its cell starts at the truncation of max(x, 0)
+                const float xhi = (float)(W - 1), yhi = (float)(H - 1);
                 for (int a = sub; a < nang; a += S) {
                     const float2 d = dirs[stride * a];
                     const float dx = __fmul_rn(d.x, r), dy = __fmul_rn(d.y, r);
                     const float xp = __fadd_rn(cx, dx), xm = __fadd_rn(cx, -dx);
                     const float yp = __fadd_rn(cy, dy), ym = __fadd_rn(cy, -dy);
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        float v;
-                        if (bilinear(img, W, H, ts, (q == 0 || q == 3) ? xp : xm, q < 2 ? yp : ym, v)) {
-                            sm[q] += v;
-                            cnt[q]++;
-                        }
+                    const bool vxp = xp > -1.0f && xp < xhi, vxm = xm > -1.0f && xm < xhi;
+                    const bool vyp = yp > -1.0f && yp < yhi, vym = ym > -1.0f && ym < yhi;
+                    const float txp = __fadd_rz(fmaxf(xp, 0.0f), kMagic), txm = __fadd_rz(fmaxf(xm, 0.0f), kMagic);
+                    const float typ = __fadd_rz(fmaxf(yp, 0.0f), kMagic), tym = __fadd_rz(fmaxf(ym, 0.0f), kMagic);
+                    const float fxp = xp - (txp - kMagic), fxm = xm - (txm - kMagic);
+                    const float fyp = yp - (typ - kMagic), fym = ym - (tym - kMagic);
+                    const int ixp = __float_as_int(txp) - 0x4B000000, ixm = __float_as_int(txm) - 0x4B000000;
+                    const float *rowp = img + (__float_as_int(typ) - 0x4B000000) * ts;
+                    const float *rowm = img + (__float_as_int(tym) - 0x4B000000) * ts;
+                    if (vxp && vyp) {
+                        sm[0] += lerp_cell(rowp, ts, ixp, fxp, fyp);
+                        cnt[0]++;
+                    }
+                    if (vxm && vyp) {
+                        sm[1] += lerp_cell(rowp, ts, ixm, fxm, fyp);
+                        cnt[1]++;
+                    }
+                    if (vxm && vym) {
+                        sm[2] += lerp_cell(rowm, ts, ixm, fxm, fym);
+                        cnt[2]++;
+                    }
+                    if (vxp && vym) {
+                        sm[3] += lerp_cell(rowm, ts, ixp, fxp, fym);
+                        cnt[3]++;
                     }
                 }
             }
@@ -808,63 +685,6 @@ __device__ __forceinline__ int lanes_per_bin(int nbins)
     return 1 << (31 - __clz(t));
 }
 
-// -------------------------------------------------------------------------------------
-// CPUTracker::ComputeQuadrantProfile, cpu_tracker.cpp:631-677, for all four quadrants at
-// once. qprof[q*nr + i] = mean of the in-bounds bilinear samples on the quarter arc of
-// radius minr + rstep*i (the image mean when fewer than 4 are in bounds), times the
-// radial weight. Directions come from the quadrant table at stride `stride`.
-// -------------------------------------------------------------------------------------
-__device__ inline void qi_quadrant_profiles(const float *img, int W, int H, int ts, float cx, float cy, float mean, int nr, int nang,
-                                     int stride, float minr, float rstep, const float2 *dirs, const float *rweights,
-                                     float *qprof)
-{
-    const int nbins = 4 * nr;
-    const int tpb = lanes_per_bin(nbins);
-    const int total = nbins * tpb;
-    for (int base = 0; base < total; base += blockDim.x) {
-        const int t = base + threadIdx.x;
-        const int bin = t / tpb, sub = t - bin * tpb;
-        float sum = 0.0f;
-        int cnt = 0;
-        int i = 0;
-        if (bin < nbins) {
-            const int q = bin / nr;
-            i = bin - q * nr;
-            const float r = minr + rstep * (float)i;
-            // quadrant signs (cpu_tracker.cpp:634-640): q0 (+,+), q1 (-,+), q2 (-,-), q3 (+,-)
-            const float sx = (q == 0 || q == 3) ? r : -r;
-            const float sy = (q < 2) ? r : -r;
-            if (circle_inside(cx, cy, fabsf(r), W, H)) {
-#pragma unroll kSampleUnroll
-                for (int a = sub; a < nang; a += tpb) {
-                    const float2 d = dirs[stride * a];
-                    sum += bilinear_inside(img, ts, cx + d.x * sx, cy + d.y * sy);
-                }
-                cnt = (nang - sub + tpb - 1) / tpb;
-            } else {
-#pragma unroll kSampleUnroll
-                for (int a = sub; a < nang; a += tpb) {
-                    const float2 d = dirs[stride * a];
-                    float v;
-                    if (bilinear(img, W, H, ts, cx + d.x * sx, cy + d.y * sy, v)) {
-                        sum += v;
-                        cnt++;
-                    }
-                }
-            }
-        }
-        for (int o = tpb >> 1; o > 0; o >>= 1) {
-            sum += __shfl_xor_sync(0xffffffffu, sum, o);
-            cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-        }
-        if (bin < nbins && sub == 0) {
-            float v = cnt >= 4 ? sum / (float)cnt : mean;
-            if (rweights) v *= rweights[i];
-            qprof[bin] = v;
-        }
-    }
-}
-
 // Radix-2 decimation-in-time FFT of length L (power of two, input in bit-reversed order),
 // executed by one warp over shared memory. tw[k] = e^{-2 pi i k / L}, k < L/2.
 // Stage s pairs (i, i + 2^(s-1)) with twiddle tw[(i mod 2^(s-1)) * (L >> s)]. Two consecutive
@@ -916,28 +736,14 @@ __device__ inline void warp_fft(float2 *buf, int L, int log2L, const float2 *tw,
     }
 }
 
-// Profile value n (0 <= n < 2nr) of the X (k=0) or Y (k=1) concatenated QI profile,
-// cpu_tracker.cpp:327-343: X = [ (q1+q2) reversed | q0+q3 ], Y = [ (q2+q3) reversed | q0+q1 ].
-__device__ __forceinline__ float2 qi_concat(const float *qprof, int nr, int n)
-{
-    const float *q0 = qprof, *q1 = qprof + nr, *q2 = qprof + 2 * nr, *q3 = qprof + 3 * nr;
-    if (n < nr) {
-        const int r = nr - 1 - n;
-        return make_float2(q1[r] + q2[r], q2[r] + q3[r]);
-    }
-    const int r = n - nr;
-    return make_float2(q0[r] + q3[r], q0[r] + q1[r]);
-}
-
 // The unnormalised correlation of each concatenated profile p with its reverse, as
 // produced by CPUTracker::QI_ComputeOffset (cpu_tracker.cpp:375-401):
 //   out[n] = L * sum_m p[(n+m) mod L] * p[L-1-m].
 // Both axes are packed into one complex signal z = px + i py. Because
 // FFT(reverse(p))* = e^{-2 pi i k/L} FFT(p) for real p, the product the reference forms
 // from two forward FFTs equals e^{-2 pi i k/L} P[k]^2, so one forward and one inverse
-// FFT per iteration give both axes. Result: ac[n] = (out_x[n], out_y[n]). Warp 0 only.
-// qi_autoconv_fft with A already holding the packed profile in bit-reversed order (as
-// qi_profiles_sym writes it). Warp 0 only.
+// FFT per iteration give both axes. Result: ac[n] = (out_x[n], out_y[n]). A holds the packed
+// profile in bit-reversed order on entry (as qi_profiles_sym writes it). Warp 0 only.
 __device__ inline void qi_autoconv_fft_filled(int nr, float2 *A, float2 *ac, const float2 *tw)
 {
     const int lane = threadIdx.x & 31;
@@ -959,14 +765,6 @@ __device__ inline void qi_autoconv_fft_filled(int nr, float2 *A, float2 *ac, con
     warp_fft(ac, L, log2L, tw, true);
 }
 
-__device__ inline void qi_autoconv_fft(const float *qprof, int nr, float2 *A, float2 *ac, const float2 *tw)
-{
-    const int lane = threadIdx.x & 31;
-    const int L = 2 * nr, log2L = ilog2_pow2(L);
-    for (int n = lane; n < L; n += 32) A[bitrev(n, log2L)] = qi_concat(qprof, nr, n);
-    __syncwarp();
-    qi_autoconv_fft_filled(nr, A, ac, tw);
-}
 
 // Same quantity by direct summation (any L; used when 2nr is not a power of two), A already
 // holding the packed profile in natural order and a barrier passed. All threads.
@@ -1003,11 +801,12 @@ __device__ __forceinline__ void radial_profile(const float *img, int W, int H, i
         const int bin = t / tpb, sub = t - bin * tpb;
         double sum = 0.0;
         int cnt = 0;
+        const float r = minr + rstep * (float)bin;
+        // one path per warp (see qi_profiles_sym)
+        const bool inside = __all_sync(0xffffffffu, bin >= nb || circle_inside(cx, cy, fabsf(r), W, H));
         if (bin < nb) {
-            const float r = minr + rstep * (float)bin;
             // FP32 sums over groups of 8 samples, folded into an FP64 total (the reference
             // adds every sample in FP64; 8-sample FP32 groups stay within ~1e-7 of it).
-            const bool inside = circle_inside(cx, cy, fabsf(r), W, H);
             for (int a0 = sub; a0 < nang; a0 += 8 * tpb) {
                 float part = 0.0f;
                 if (inside) {

@@ -1,11 +1,10 @@
 // Localization kernels for sm_100a.
 //
-// localize_qi_kernel: each CTA walks a queue of ROIs and runs the whole per-ROI pipeline of
-//   QueuedCPUTracker::ProcessJob (cputrack/QueuedCPUTracker.cpp:273-361) on a padded float tile
-//   of the ROI in shared memory: stage (bulk copy of the next ROI during the current one's Z
-//   stage) + convert (+ calibration) fused with the first COM pass -> COM -> QI iterations ->
-//   radial profile -> Z-LUT match -> result. Pixels are read from HBM exactly once; everything
-//   after the copy works on-chip.
+// localize_qi_kernel: one CTA per ROI runs the whole per-ROI pipeline of
+//   QueuedCPUTracker::ProcessJob (cputrack/QueuedCPUTracker.cpp:273-361) on a float tile of the
+//   ROI in shared memory: bulk copy (or batched loads) + convert (+ calibration) fused with the
+//   first COM pass -> COM -> QI iterations -> radial profile -> Z-LUT match -> result. Pixels are
+//   read from HBM exactly once; everything after the load works on-chip.
 // localize_gauss_kernel: one CTA per ROI, COM -> 2D Gaussian MLE (-> Z) on a plain tile.
 // gauss_warp_kernel: one warp per small ROI (<= 32x32) for the Gaussian-only mode.
 // build_lut_kernel / finalize_lut_kernel: QueuedCPUTracker::BuildLUT / FinalizeLUT
@@ -14,7 +13,6 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdio>
-#include <mutex>
 #include <cuda_runtime.h>
 
 #include <cuda_bf16.h>
@@ -71,10 +69,10 @@ __device__ __forceinline__ void load_z_tables(const SmemView &s, const TrackPara
         for (int i = threadIdx.x; i < P.z_angsteps; i += blockDim.x) s.zdirs[i] = zd[i];
 }
 
-// CPUTracker::ComputeQI, cpu_tracker.cpp:285-360, on the padded tile (row pitch ts). All threads
-// call; returns the position and the boundary flag of the last iteration.
-__device__ __forceinline__ void qi_localize(const SmemView &s, const TrackParams &P, int ts, float mean, float &cx,
-                                            float &cy, bool &bhit, const float *rweights)
+// CPUTracker::ComputeQI, cpu_tracker.cpp:285-360. All threads call; returns the position and the
+// boundary flag of the last iteration.
+__device__ void qi_localize(const SmemView &s, const TrackParams &P, float mean, float &cx, float &cy, bool &bhit,
+                            const float *rweights)
 {
     const int W = P.width, H = P.height, nr = P.qi_nr, L = 2 * nr;
     const bool pow2 = (L & (L - 1)) == 0 && L >= 2;
@@ -85,7 +83,7 @@ __device__ __forceinline__ void qi_localize(const SmemView &s, const TrackParams
     const float rstep = (P.qi_maxr - P.qi_minr) / (float)nr;  // also pixelsPerProfLen (cpu_tracker.cpp:311,649)
     for (int k = 0; k < P.qi_iterations; k++) {
         bhit = check_boundaries(cx, cy, P.qi_maxr, W, H);
-        qi_profiles_sym(s.img, W, H, ts, cx, cy, mean, nr, P.qi_nang[k], P.qi_stride[k], P.qi_minr, rstep,
+        qi_profiles_sym(s.img, W, H, W, cx, cy, mean, nr, P.qi_nang[k], P.qi_stride[k], P.qi_minr, rstep,
                         s.qdirs, rweights, part, A, pow2 ? ilog2_pow2(L) : -1);
         __syncthreads();
         if (pow2) {
@@ -117,22 +115,9 @@ __device__ __forceinline__ void qi_localize(const SmemView &s, const TrackParams
     }
 }
 
-// Starts the bulk copy of the next ROI's raw bytes into the tile region (thread 0; the CTA's reads
-// of the tile must be complete and ordered by a barrier). No-op when next_src is null.
-__device__ __forceinline__ void stage_next(uint8_t *tile, const TrackParams &P, const uint8_t *next_src, uint64_t *mbar)
-{
-    if (next_src && threadIdx.x == 0)
-        bulk_load(tile + P.sm_raw, next_src, (uint32_t)(P.width * P.height * (P.pdt == 0 ? 1 : (P.pdt == 1 ? 2 : 4))),
-                  mbar);
-}
-
-// Radial profile + Z-LUT compare (QueuedCPUTracker.cpp:319-338) on a tile of row pitch ts. Returns z
-// (0 without a LUT). With P.zprof_f32 set, the profile is written out for the tensor-core match instead.
-// When next_src is set, the next ROI's bulk copy into the tile region starts as soon as the
-// profile's samples are taken (the compare and fit do not read the tile).
-__device__ __forceinline__ float z_localize(const SmemView &s, const TrackParams &P, int ts, float mean, float x,
-                                            float y, int bead, int roi, const uint8_t *next_src = nullptr,
-                                            uint64_t *mbar = nullptr)
+// Radial profile + Z-LUT compare (QueuedCPUTracker.cpp:319-338). Returns z (0 without a LUT). With
+// P.zprof_f32 set, the profile is written out for the tensor-core match instead.
+__device__ float z_localize(const SmemView &s, const TrackParams &P, float mean, float x, float y, int bead, int roi)
 {
     const int nb = P.z_nbins;
     float *prof = reinterpret_cast<float *>(s.work);
@@ -140,9 +125,8 @@ __device__ __forceinline__ float z_localize(const SmemView &s, const TrackParams
     const float rstep = (P.z_maxr - P.z_minr) / (float)nb;
     load_z_tables(s, P);
     __syncthreads();
-    radial_profile(s.img, P.width, P.height, ts, x, y, mean, nb, P.z_angsteps, P.z_minr, rstep, s.zdirs, prof,
+    radial_profile(s.img, P.width, P.height, P.width, x, y, mean, nb, P.z_angsteps, P.z_minr, rstep, s.zdirs, prof,
                    (P.mode & kLT_NormalizeProfile) != 0, s.red);
-    stage_next(reinterpret_cast<uint8_t *>(s.img), P, next_src, mbar);
     if (P.zprof_f32) {
         // [hi | lo] BF16 split of the weighted profile: v = hi + lo + O(2^-16 v)
         __nv_bfloat16 *pb = static_cast<__nv_bfloat16 *>(P.zprof_bf16) + (size_t)roi * 2 * P.zprof_nbp;
@@ -204,80 +188,71 @@ __device__ __forceinline__ void write_result(LocalizationResult *results, int i,
     o[12] = __float_as_uint(mean);
 }
 
-#ifndef QTRK_MIN_BLOCKS
-#define QTRK_MIN_BLOCKS 4
-#endif
+constexpr int kMinBlocks = 4;  // CTAs per SM the QI and Gaussian kernels are compiled for (64 registers)
 
 constexpr uint32_t kStageWaitLimit = 1u << 22;  // mbarrier polls before a staged copy counts as lost
 
-// COM / QI (+ Z): QueuedCPUTracker::ProcessJob (QueuedCPUTracker.cpp:273-361) for ROIs r =
-// blockIdx.x, blockIdx.x + gridDim.x, ... (the launcher sizes the grid to the CTAs that fit on
-// the GPU at once, so each CTA walks a queue of ROIs). Each ROI becomes a padded float tile in
-// shared memory: with P.stage_raw its raw bytes arrive by one bulk copy (cp.async.bulk, mbarrier
-// completion) that the CTA started while it was finishing the previous ROI's Z compare and fit,
-// and are converted in place; otherwise threads load them from global memory (frame bands,
-// unaligned or odd-width ROIs). The COM's first pass is fused into that conversion. kStaged
-// selects the form (one instantiation each, so neither carries the other's registers). TS > 0
-// is the tile pitch as a compile-time constant (tile_pitch of a common ROI width: the gathers'
-// second-row offsets become immediates), 0 takes P.sm_pitch.
-template <bool kStaged, int TS>
-__global__ void __launch_bounds__(kBlockThreads, QTRK_MIN_BLOCKS)
+// COM / QI (+ Z): QueuedCPUTracker::ProcessJob (QueuedCPUTracker.cpp:273-361), one CTA per ROI.
+// The ROI becomes a float tile in shared memory. With kStaged (ROIs back to back, 16-byte
+// aligned, whole 16-byte chunks) its raw bytes arrive by one bulk copy (cp.async.bulk, completion
+// on an mbarrier) started by thread 0 as the CTA begins, while the other threads fetch the QI
+// tables, and are converted in place; otherwise the threads load them with batched streaming
+// loads (frame bands, unaligned ROIs). The COM's first pass is fused into either conversion.
+// One instantiation per form, so neither carries the other's registers.
+template <bool kStaged>
+__global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
     localize_qi_kernel(TrackParams P, const uint8_t *__restrict__ pixels, int pitch, int64_t roi_stride,
                        const int64_t *__restrict__ roi_offsets, const LocalizationJob *__restrict__ jobs, int count,
                        LocalizationResult *__restrict__ results)
 {
     extern __shared__ __align__(16) uint8_t smem[];
-    if ((int)blockIdx.x >= count) return;
+    const int roi = blockIdx.x;
+    if (roi >= count) return;
     const SmemView s = smem_view(smem, P);
-    uint8_t *tile = reinterpret_cast<uint8_t *>(s.img);
+    const int W = P.width, H = P.height;
+    BlockGroup g{s.red};
     uint64_t *mbar = reinterpret_cast<uint64_t *>(reinterpret_cast<uint8_t *>(s.misc) + 32);
-    const int W = P.width, H = P.height, ts = TS > 0 ? TS : P.sm_pitch;
-    constexpr bool staged = kStaged;
-    uint32_t parity = 0;
-    if (staged) {
-        if (threadIdx.x == 0) mbar_init(mbar);
-        __syncthreads();
-        stage_next(tile, P, pixels + (int64_t)blockIdx.x * roi_stride, mbar);
+    if constexpr (kStaged) {
+        if (threadIdx.x == 0) {
+            const int bpp = P.pdt == 0 ? 1 : (P.pdt == 1 ? 2 : 4);
+            const int n = W * H;
+            mbar_init(mbar);
+            bulk_load(reinterpret_cast<uint8_t *>(s.img) + (size_t)(4 - bpp) * n, pixels + (int64_t)roi * roi_stride,
+                      (uint32_t)(bpp * n), mbar);
+        }
     }
-    for (int roi = blockIdx.x; roi < count; roi += gridDim.x) {
-        const int next = roi + (int)gridDim.x;
-        const uint8_t *next_src = (staged && next < count) ? pixels + (int64_t)next * roi_stride : nullptr;
-        uint32_t job[6];
-        read_job(jobs, roi, job);
-        const int bead = (int)job[2];
-        load_qi_tables(s, P);
-        float2 part;
-        if constexpr (staged) {
-            if (!mbar_wait(mbar, parity, kStageWaitLimit) && P.err_flag) atomicOr(P.err_flag, 4u);
-            parity ^= 1u;
-            part = convert_staged_tile(s.img, ts, tile + P.sm_raw, P, bead);
-        } else {
-            const int64_t off = roi_offsets ? roi_offsets[roi] : (int64_t)roi * roi_stride;
-            part = load_roi_tile(s.img, ts, pixels + off, pitch, P, bead);
-        }
-        const ComResult com = com_tile(s.img, ts, W, H, part, P.com_bgcorrection, s.red);
-        float comx = com.x, comy = com.y;
-        if (isnan(comx) || isnan(comy)) {  // QueuedCPUTracker.cpp:294-295
-            comx = (float)(W / 2);
-            comy = (float)(H / 2);
-        }
-        float x = comx, y = comy, z = 0.0f;
-        bool bhit = false;
-        if (P.mode & kLT_QI) qi_localize(s, P, ts, com.mean, x, y, bhit, P.qi_rweights);
-        if (P.mode & kLT_LocalizeZ) {
-            bhit = check_boundaries(x, y, P.z_maxr, W, H);
-            z = z_localize(s, P, ts, com.mean, x, y, bead, roi, next_src, mbar);
-        } else {
-            stage_next(tile, P, next_src, mbar);  // the last tile reads ended at a barrier
-        }
-        if (threadIdx.x == 0) write_result(results, roi, job, x, y, z, comx, comy, bhit ? 1u : 0u, com.mean);
-        __syncthreads();  // tables, work and misc are rewritten by the next ROI
+    uint32_t job[6];
+    read_job(jobs, roi, job);
+    const int bead = (int)job[2];
+    load_qi_tables(s, P);
+    float2 part;
+    if constexpr (kStaged) {
+        __syncthreads();  // the mbarrier is initialised
+        if (!mbar_wait(mbar, 0, kStageWaitLimit) && P.err_flag) atomicOr(P.err_flag, 4u);
+        part = convert_staged(g, s.img, P, bead);
+    } else {
+        const int64_t off = roi_offsets ? roi_offsets[roi] : (int64_t)roi * roi_stride;
+        part = load_roi(g, s.img, pixels + off, pitch, P, bead);
     }
+    const ComResult com = com_from_sums(g, s.img, W, H, part, P.com_bgcorrection);
+    float comx = com.x, comy = com.y;
+    if (isnan(comx) || isnan(comy)) {  // QueuedCPUTracker.cpp:294-295
+        comx = (float)(W / 2);
+        comy = (float)(H / 2);
+    }
+    float x = comx, y = comy, z = 0.0f;
+    bool bhit = false;
+    if (P.mode & kLT_QI) qi_localize(s, P, com.mean, x, y, bhit, P.qi_rweights);
+    if (P.mode & kLT_LocalizeZ) {
+        bhit = check_boundaries(x, y, P.z_maxr, W, H);
+        z = z_localize(s, P, com.mean, x, y, bead, roi);
+    }
+    if (threadIdx.x == 0) write_result(results, roi, job, x, y, z, comx, comy, bhit ? 1u : 0u, com.mean);
 }
 
 // 2D Gaussian MLE (+ Z) for ROIs above 32x32 or with QI/Z bits: one CTA per ROI on a plain tile.
 // Kept apart from the QI kernel so that its register budget is free of the MLE's FP64 solve.
-__global__ void __launch_bounds__(kBlockThreads, QTRK_MIN_BLOCKS)
+__global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
     localize_gauss_kernel(TrackParams P, const uint8_t *__restrict__ pixels, int pitch, int64_t roi_stride,
                           const int64_t *__restrict__ roi_offsets, const LocalizationJob *__restrict__ jobs, int count,
                           LocalizationResult *__restrict__ results)
@@ -314,7 +289,7 @@ __global__ void __launch_bounds__(kBlockThreads, QTRK_MIN_BLOCKS)
     __syncthreads();
     if (P.mode & kLT_LocalizeZ) {
         bhit = check_boundaries(x, y, P.z_maxr, W, H);
-        z = z_localize(s, P, W, com.mean, x, y, bead, roi);
+        z = z_localize(s, P, com.mean, x, y, bead, roi);
     }
     if (threadIdx.x == 0) write_result(results, roi, job, x, y, z, comx, comy, bhit ? 1u : 0u, com.mean);
 }
@@ -373,20 +348,19 @@ __global__ void __launch_bounds__(kBlockThreads) build_lut_kernel(TrackParams P,
     if (bead >= nbeads) return;
     const SmemView s = smem_view(smem, P);
     load_qi_tables(s, P);
-    const int ts = P.sm_pitch;
-    const float2 part = load_roi_tile(s.img, ts, pixels + (size_t)pitch * P.height * bead, pitch, P, bead);
+    BlockGroup g{s.red};
+    const float2 part = load_roi(g, s.img, pixels + (size_t)pitch * P.height * bead, pitch, P, bead);
     float x, y, mean = 0.0f;
     if (known_pos) {
-        __syncthreads();
         x = known_pos[bead].x;
         y = known_pos[bead].y;
     } else {
-        const ComResult com = com_tile(s.img, ts, P.width, P.height, part, 0.0f, s.red);
+        const ComResult com = com_from_sums(g, s.img, P.width, P.height, part, 0.0f);
         mean = com.mean;
         x = com.x;
         y = com.y;
         bool bhit;
-        qi_localize(s, P, ts, mean, x, y, bhit, nullptr);
+        qi_localize(s, P, mean, x, y, bhit, nullptr);
     }
     const int nb = P.z_nbins;
     float *prof = reinterpret_cast<float *>(s.work);
@@ -394,7 +368,7 @@ __global__ void __launch_bounds__(kBlockThreads) build_lut_kernel(TrackParams P,
     __syncthreads();
     load_z_tables(s, P);
     __syncthreads();
-    radial_profile(s.img, P.width, P.height, ts, x, y, mean, nb, P.z_angsteps, P.z_minr, rstep, s.zdirs, prof,
+    radial_profile(s.img, P.width, P.height, P.width, x, y, mean, nb, P.z_angsteps, P.z_minr, rstep, s.zdirs, prof,
                    normalize != 0, s.red);
     float *dst = lut + ((size_t)bead * P.lut_planes + plane) * nb;
     for (int r = threadIdx.x; r < nb; r += blockDim.x) dst[r] += prof[r];
@@ -451,13 +425,8 @@ void plan_smem(TrackParams &P)
 {
     const int W = P.width, H = P.height;
     const int nr = P.qi_nr > 0 ? P.qi_nr : 1, L = 2 * nr;
-    P.sm_pitch = tile_pitch(W);
     P.sm_img = 0;
-    // padded tile (the plain tile of the other kernels fits in it) + 16 bytes of slack, so that a
-    // staged raw ROI placed at the region's end, 16-byte aligned, starts after the float tile's
-    // last row would require (convert_staged_tile)
-    P.sm_tile_bytes = align16(H * P.sm_pitch * 4) + 16;
-    P.sm_tables = P.sm_tile_bytes;
+    P.sm_tables = align16(W * H * 4);
     const int qi_tables = (P.qi_angpq + nr) * 8, z_tables = P.z_angsteps * 8;
     P.sm_work = P.sm_tables + align16(qi_tables > z_tables ? qi_tables : z_tables);
     // [ ac | A ] (L complex each) + 2 KB of subset partials when the QI directions are split over warps
@@ -479,24 +448,6 @@ int gauss_warp_smem(const TrackParams &P)
     return 8 * ((W * H + 3 * (W + H) + 3) & ~3) * 4;
 }
 
-using QIKernel = void (*)(TrackParams, const uint8_t *, int, int64_t, const int64_t *, const LocalizationJob *, int,
-                          LocalizationResult *);
-
-// The QI kernel for a launch: staged ROIs get a compile-time tile pitch for the common ROI widths
-// (40, 60/64, 80, 100 and 128 px).
-static QIKernel qi_kernel(bool staged, int pitch)
-{
-    if (!staged) return localize_qi_kernel<false, 0>;
-    switch (pitch) {
-    case 44: return localize_qi_kernel<true, 44>;
-    case 70: return localize_qi_kernel<true, 70>;
-    case 84: return localize_qi_kernel<true, 84>;
-    case 102: return localize_qi_kernel<true, 102>;
-    case 134: return localize_qi_kernel<true, 134>;
-    default: return localize_qi_kernel<true, 0>;
-    }
-}
-
 static bool g_attrs_set[64];
 
 cudaError_t prepare_kernels(int device)
@@ -505,9 +456,10 @@ cudaError_t prepare_kernels(int device)
     if (g_attrs_set[device]) return cudaSuccess;
     const int max_smem = 227 * 1024;
     cudaError_t e;
-    for (const QIKernel f : {qi_kernel(true, 0), qi_kernel(true, 44), qi_kernel(true, 70), qi_kernel(true, 84),
-                             qi_kernel(true, 102), qi_kernel(true, 134), qi_kernel(false, 0)})
-        if ((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem))) return e;
+    if ((e = cudaFuncSetAttribute(localize_qi_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)))
+        return e;
+    if ((e = cudaFuncSetAttribute(localize_qi_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)))
+        return e;
     if ((e = cudaFuncSetAttribute(localize_gauss_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem)))
         return e;
     if ((e = cudaFuncSetAttribute(build_lut_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem))) return e;
@@ -515,39 +467,6 @@ cudaError_t prepare_kernels(int device)
     if ((e = cudaFuncSetAttribute(gauss_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem))) return e;
     g_attrs_set[device] = true;
     return cudaSuccess;
-}
-
-// CTAs of the QI kernel for `count` ROIs: as many as fit on the GPU at once (its ROI loop takes
-// the rest), looked up once per device and shared-memory size.
-static int qi_grid(int smem_bytes, int count)
-{
-    struct Entry {
-        int device, smem, ctas;
-    };
-    static std::mutex mu;
-    static Entry cache[16];
-    static int ncache = 0;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    int ctas = 0;
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        for (int i = 0; i < ncache; i++)
-            if (cache[i].device == dev && cache[i].smem == smem_bytes) ctas = cache[i].ctas;
-    }
-    if (ctas == 0) {
-        int per_sm = 0, sms = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, qi_kernel(true, 0), kBlockThreads, smem_bytes) !=
-                cudaSuccess ||
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || per_sm <= 0) {
-            cudaGetLastError();
-            return count;  // one CTA per ROI
-        }
-        ctas = per_sm * sms;
-        std::lock_guard<std::mutex> lk(mu);
-        if (ncache < 16) cache[ncache++] = Entry{dev, smem_bytes, ctas};
-    }
-    return count < ctas ? count : ctas;
 }
 
 bool use_gauss_warp(const TrackParams &P)
@@ -569,16 +488,18 @@ cudaError_t launch_localize(const TrackParams &P, const uint8_t *pixels, int pit
         localize_gauss_kernel<<<count, kBlockThreads, P.smem_bytes, stream>>>(P, pixels, pitch, roi_stride,
                                                                               roi_offsets, jobs, count, results);
     } else {
-        TrackParams Q = P;
+        // bulk-copy staging: ROIs back to back at a 16-byte aligned stride, and a pixel count for
+        // which the copy size and the in-place offset (4 - bpp) n are whole 16-byte units
         const int bpp = P.pdt == 0 ? 1 : (P.pdt == 1 ? 2 : 4);
-        const int64_t raw = (int64_t)P.width * P.height * bpp;
-        Q.stage_raw = !roi_offsets && pitch == P.width * bpp && !(P.width & 1) && P.width <= 256 &&
-                      !(reinterpret_cast<uintptr_t>(pixels) & 15) && !(roi_stride & 15) && !(raw & 15) &&
-                      raw <= P.sm_tile_bytes;
-        Q.sm_raw = Q.stage_raw ? (int)((P.sm_tile_bytes - raw) & ~(int64_t)15) : 0;
-        const int grid = qi_grid(P.smem_bytes, count);
-        qi_kernel(Q.stage_raw != 0, Q.sm_pitch)<<<grid, kBlockThreads, P.smem_bytes, stream>>>(
-            Q, pixels, pitch, roi_stride, roi_offsets, jobs, count, results);
+        const int n = P.width * P.height;
+        const bool staged = !roi_offsets && pitch == P.width * bpp && !(reinterpret_cast<uintptr_t>(pixels) & 15) &&
+                            !(roi_stride & 15) && !(n & 15);
+        if (staged)
+            localize_qi_kernel<true><<<count, kBlockThreads, P.smem_bytes, stream>>>(P, pixels, pitch, roi_stride,
+                                                                                    roi_offsets, jobs, count, results);
+        else
+            localize_qi_kernel<false><<<count, kBlockThreads, P.smem_bytes, stream>>>(P, pixels, pitch, roi_stride,
+                                                                                     roi_offsets, jobs, count, results);
     }
     return cudaGetLastError();
 }
@@ -667,7 +588,7 @@ void localize_node(const TrackParams &P, int count, cudaKernelNodeParams &kp)
         kp.sharedMemBytes = gauss_warp_smem(P);
     } else {
         kp.func = (P.mode & kLT_Gaussian2D) && !(P.mode & kLT_QI) ? reinterpret_cast<void *>(localize_gauss_kernel)
-                                                                   : reinterpret_cast<void *>(qi_kernel(false, 0));
+                                                                   : reinterpret_cast<void *>(localize_qi_kernel<false>);
         kp.gridDim = dim3(count);
         kp.blockDim = dim3(kBlockThreads);
         kp.sharedMemBytes = P.smem_bytes;

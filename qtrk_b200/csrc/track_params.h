@@ -80,15 +80,9 @@ struct TrackParams {
     int calib_count;
     float offset_factor, gain_factor;
 
-    // Dynamic shared-memory layout (byte offsets), filled by the host; sm_pitch is the row pitch
-    // (floats) of the padded ROI tile of the QI kernels (tile_pitch(width)); the tile region is
-    // sm_tile_bytes long (the tile plus 16 bytes of slack for a staged raw ROI, see sm_raw)
-    int sm_img, sm_tables, sm_work, sm_red, sm_misc, smem_bytes, sm_pitch, sm_tile_bytes;
-    // Set per launch by the launcher: 1 when the QI kernel brings each ROI's raw bytes into
-    // shared memory with one bulk copy (ROIs back to back, 16-byte aligned, whole 16-byte
-    // chunks, even width); the raw bytes land at byte offset sm_raw of the tile region.
-    int stage_raw, sm_raw;
-    unsigned *err_flag;  // mapped host word: |= 4 when a staged ROI copy did not arrive in time
+    // Dynamic shared-memory layout (byte offsets), filled by the host
+    int sm_img, sm_tables, sm_work, sm_red, sm_misc, smem_bytes;
+    unsigned *err_flag;  // mapped host word: |= 4 when a staged ROI copy did not arrive in time (QI kernel)
 };
 
 }  // namespace qtrk

@@ -59,7 +59,8 @@ def test_calibration_images_match_reference(ref, roi60, which):
     gain = gain if which in ("gain", "both") else None
     r_ref = ref.track(wl.settings, wl.mode, wl.rois, lut, zlut_index=idx, calib=(off, gain))
     r = _ours(wl.settings, wl.mode, lut, wl.rois, idx, off, gain)
-    check_results(r, r_ref["pos"], r_ref["firstGuess"], r_ref["error"], r_ref["imageMean"])
+    check_results(r, r_ref["pos"], r_ref["firstGuess"], r_ref["error"], r_ref["imageMean"],
+                      lut_planes=lut.shape[1])
     # the calibration must have changed the answer, or the comparison proves nothing
     plain = ref.track(wl.settings, wl.mode, wl.rois, lut, zlut_index=idx)
     assert np.abs(plain["imageMean"] - r_ref["imageMean"]).max() > 1e-3
@@ -77,7 +78,8 @@ def test_calibration_u16_and_clear_first_four(ref):
     for mode in (wl.mode, wl.mode | abi.LT_ClearFirstFourPixels):
         r_ref = ref.track(wl.settings, mode, wl.rois, lut, zlut_index=idx, calib=(off, gain))
         r = _ours(wl.settings, mode, lut, wl.rois, idx, off, gain)
-        check_results(r, r_ref["pos"], r_ref["firstGuess"], r_ref["error"], r_ref["imageMean"])
+        check_results(r, r_ref["pos"], r_ref["firstGuess"], r_ref["error"], r_ref["imageMean"],
+                      lut_planes=lut.shape[1])
 
 
 def test_calibration_factors_scale_the_images(ref, roi60):
@@ -88,7 +90,8 @@ def test_calibration_factors_scale_the_images(ref, roi60):
     off, gain = _calibration(wl.rois.shape[1:], 45)
     r_ref = ref.track(wl.settings, wl.mode, wl.rois, lut, zlut_index=idx, calib=(off * 2.0, gain * 0.5))
     r = _ours(wl.settings, wl.mode, lut, wl.rois, idx, off, gain, factors=(2.0, 0.5))
-    check_results(r, r_ref["pos"], r_ref["firstGuess"], r_ref["error"], r_ref["imageMean"])
+    check_results(r, r_ref["pos"], r_ref["firstGuess"], r_ref["error"], r_ref["imageMean"],
+                      lut_planes=lut.shape[1])
 
 
 def test_removing_calibration_restores_plain_results(roi60):
