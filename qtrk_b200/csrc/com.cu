@@ -18,8 +18,11 @@
 // multiply-add on top of the background correction, and only chunks that cross a row end pay
 // for Sw.
 #include <cstdint>
+#include <mutex>
+
 #include <cuda_runtime.h>
 
+#include "bulk_copy.cuh"
 #include "device_common.cuh"
 #include "kernels.h"
 
@@ -100,64 +103,18 @@ __device__ __forceinline__ void cta_sum(double (&v)[N], double (*red)[N])
 
 }  // namespace
 
-// One CTA per ROI; ROI r is the n*bpp bytes at pixels + r * roi_stride (16-byte aligned, n*bpp a
-// multiple of 16). Thread t holds chunks t, t + T, ..., t + (K-1) T.
+namespace {
+
+constexpr int kComMaxStages = 4;
+constexpr uint32_t kComWaitLimit = 1u << 22;  // mbarrier polls before a staged ROI counts as lost
+
+// Pass 2 of ComputeMeanAndCOM on this thread's chunks (see the chunk moments above): returns the
+// FP32 partial sums of v', x v' and y v'.
 template <int PDT, int K>
-__global__ void __launch_bounds__(kComMaxThreads) com_kernel(TrackParams P, const uint8_t *__restrict__ pixels,
-                                                              int64_t roi_stride,
-                                                              const LocalizationJob *__restrict__ jobs, int count,
-                                                              LocalizationResult *__restrict__ results)
+__device__ __forceinline__ float3 com_moments(const float (&v)[K][ChunkPixels<PDT>::n], int t, int T, int nchunks, int W,
+                                              float mean, float thr)
 {
     constexpr int ppc = ChunkPixels<PDT>::n;
-    __shared__ double red2[32][2];
-    __shared__ double red3[32][3];
-    const int roi = blockIdx.x;
-    if (roi >= count) return;
-    const int W = P.width, n = W * P.height, nchunks = n / ppc, T = blockDim.x, t = threadIdx.x;
-    const uint4 *src = reinterpret_cast<const uint4 *>(pixels + (int64_t)roi * roi_stride);
-    uint4 q[K];
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-        const int c = t + k * T;
-        q[k] = c < nchunks ? __ldcs(src + c) : make_uint4(0, 0, 0, 0);
-    }
-    uint32_t job[6];
-    if (t == 0) {
-        if (jobs) {
-            const uint32_t *p = reinterpret_cast<const uint32_t *>(jobs) + (size_t)roi * 6;
-#pragma unroll
-            for (int k = 0; k < 6; k++) job[k] = p[k];
-        } else {
-            job[0] = (uint32_t)roi;
-#pragma unroll
-            for (int k = 1; k < 6; k++) job[k] = 0;
-        }
-    }
-
-    float v[K][ppc];
-#pragma unroll
-    for (int k = 0; k < K; k++) unpack<PDT>(q[k], v[k]);
-    if ((P.mode & kLT_ClearFirstFourPixels) && t == 0)  // QueuedCPUTracker.cpp:280-282
-#pragma unroll
-        for (int j = 0; j < 4; j++) v[0][j] = 0.0f;
-
-    // pass 1: sum and sum of squares (chunks past the ROI hold zeros)
-    float s = 0.0f, s2 = 0.0f;
-#pragma unroll
-    for (int k = 0; k < K; k++)
-#pragma unroll
-        for (int j = 0; j < ppc; j++) {
-            s += v[k][j];
-            s2 = fmaf(v[k][j], v[k][j], s2);
-        }
-    double m1[2] = {(double)s, (double)s2};
-    cta_sum<2>(m1, red2);
-    const float invN = 1.0f / (float)n;
-    const float mean = (float)(m1[0] * (double)invN);
-    const float stdev = sqrtf((float)(m1[1] * (double)invN - (double)(mean * mean)));
-    const float thr = P.com_bgcorrection * stdev;
-
-    // pass 2: background-corrected moments
     float q0 = 0.0f, qx = 0.0f, qy = 0.0f;
 #pragma unroll
     for (int k = 0; k < K; k++) {
@@ -185,30 +142,222 @@ __global__ void __launch_bounds__(kComMaxThreads) com_kernel(TrackParams P, cons
             qy += fmaf((float)y0, S, Sw);
         }
     }
-    double m2[3] = {(double)q0, (double)qx, (double)qy};
-    cta_sum<3>(m2, red3);
-    if (t == 0) {
-        float cx = (float)(m2[1] / m2[0]), cy = (float)(m2[2] / m2[0]);
-        if (isnan(cx) || isnan(cy)) {  // QueuedCPUTracker.cpp:294-295
-            cx = (float)(W / 2);
-            cy = (float)(P.height / 2);
-        }
-        uint32_t *o = reinterpret_cast<uint32_t *>(results) + (size_t)roi * 13;
+    return make_float3(q0, qx, qy);
+}
+
+// The 13-word LocalizationResult of a COM-only localization (thread 0).
+__device__ __forceinline__ void com_result(LocalizationResult *results, int roi, const LocalizationJob *jobs,
+                                           const double (&m)[3], float mean, int W, int H)
+{
+    float cx = (float)(m[1] / m[0]), cy = (float)(m[2] / m[0]);
+    if (isnan(cx) || isnan(cy)) {  // QueuedCPUTracker.cpp:294-295
+        cx = (float)(W / 2);
+        cy = (float)(H / 2);
+    }
+    uint32_t *o = reinterpret_cast<uint32_t *>(results) + (size_t)roi * 13;
+    if (jobs) {
+        const uint32_t *p = reinterpret_cast<const uint32_t *>(jobs) + (size_t)roi * 6;
 #pragma unroll
-        for (int k = 0; k < 6; k++) o[k] = job[k];
-        o[6] = __float_as_uint(cx);
-        o[7] = __float_as_uint(cy);
-        o[8] = 0u;
-        o[9] = __float_as_uint(cx);
-        o[10] = __float_as_uint(cy);
-        o[11] = 0u;
-        o[12] = __float_as_uint(mean);
+        for (int k = 0; k < 6; k++) o[k] = p[k];
+    } else {
+        o[0] = (uint32_t)roi;
+#pragma unroll
+        for (int k = 1; k < 6; k++) o[k] = 0u;
+    }
+    o[6] = __float_as_uint(cx);
+    o[7] = __float_as_uint(cy);
+    o[8] = 0u;
+    o[9] = __float_as_uint(cx);
+    o[10] = __float_as_uint(cy);
+    o[11] = 0u;
+    o[12] = __float_as_uint(mean);
+}
+
+}  // namespace
+
+// One CTA per ROI; ROI r is the n*bpp bytes at pixels + r * roi_stride (16-byte aligned, n*bpp a
+// multiple of 16). Thread t holds chunks t, t + T, ..., t + (K-1) T.
+template <int PDT, int K>
+__global__ void __launch_bounds__(kComMaxThreads) com_kernel(TrackParams P, const uint8_t *__restrict__ pixels,
+                                                              int64_t roi_stride,
+                                                              const LocalizationJob *__restrict__ jobs, int count,
+                                                              LocalizationResult *__restrict__ results)
+{
+    constexpr int ppc = ChunkPixels<PDT>::n;
+    __shared__ double red2[32][2];
+    __shared__ double red3[32][3];
+    const int roi = blockIdx.x;
+    if (roi >= count) return;
+    const int W = P.width, n = W * P.height, nchunks = n / ppc, T = blockDim.x, t = threadIdx.x;
+    const uint4 *src = reinterpret_cast<const uint4 *>(pixels + (int64_t)roi * roi_stride);
+    uint4 q[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        const int c = t + k * T;
+        q[k] = c < nchunks ? __ldcs(src + c) : make_uint4(0, 0, 0, 0);
+    }
+    float v[K][ppc];
+#pragma unroll
+    for (int k = 0; k < K; k++) unpack<PDT>(q[k], v[k]);
+    if ((P.mode & kLT_ClearFirstFourPixels) && t == 0)  // QueuedCPUTracker.cpp:280-282
+#pragma unroll
+        for (int j = 0; j < 4; j++) v[0][j] = 0.0f;
+
+    // pass 1: sum and sum of squares (chunks past the ROI hold zeros)
+    float s = 0.0f, s2 = 0.0f;
+#pragma unroll
+    for (int k = 0; k < K; k++)
+#pragma unroll
+        for (int j = 0; j < ppc; j++) {
+            s += v[k][j];
+            s2 = fmaf(v[k][j], v[k][j], s2);
+        }
+    double m1[2] = {(double)s, (double)s2};
+    cta_sum<2>(m1, red2);
+    const float invN = 1.0f / (float)n;
+    const float mean = (float)(m1[0] * (double)invN);
+    const float stdev = sqrtf((float)(m1[1] * (double)invN - (double)(mean * mean)));
+    const float thr = P.com_bgcorrection * stdev;
+
+    // pass 2: background-corrected moments
+    const float3 mo = com_moments<PDT, K>(v, t, T, nchunks, W, mean, thr);
+    double m2[3] = {(double)mo.x, (double)mo.y, (double)mo.z};
+    cta_sum<3>(m2, red3);
+    if (t == 0) com_result(results, roi, jobs, m2, mean, W, P.height);
+}
+
+
+// The streaming form: CTAs stay resident (the grid is what fits on the GPU) and walk the ROIs
+// r = blockIdx.x, blockIdx.x + gridDim.x, ...; each keeps `stages` ROIs in flight in a ring of
+// shared-memory buffers, filled by bulk copies (cp.async.bulk, one per ROI, issued by thread 0,
+// completion on one mbarrier per buffer). A ROI's buffer is read into registers once (16-byte
+// shared loads, conversion to float), its buffer refilled with the ROI `stages` steps ahead as soon
+// as every thread has read it, and both passes of the COM run on the registers, so HBM keeps
+// streaming while the CTA reduces. ring_stride: bytes per buffer (the ROI's bytes rounded up to
+// 128).
+template <int PDT, int K>
+__global__ void __launch_bounds__(kComMaxThreads) com_stream_kernel(TrackParams P, const uint8_t *__restrict__ pixels,
+                                                                     int64_t roi_stride,
+                                                                     const LocalizationJob *__restrict__ jobs,
+                                                                     int count, LocalizationResult *__restrict__ results,
+                                                                     int stages, int ring_stride)
+{
+    constexpr int ppc = ChunkPixels<PDT>::n;
+    extern __shared__ __align__(128) uint8_t ring[];
+    __shared__ uint64_t mbar[kComMaxStages];
+    __shared__ double red2[32][2];
+    __shared__ double red3[32][3];
+    const int W = P.width, H = P.height, n = W * H, nchunks = n / ppc, T = blockDim.x, t = threadIdx.x;
+    const int G = gridDim.x;
+    const uint32_t bytes = (uint32_t)(n * (16 / ppc));
+    if ((int)blockIdx.x >= count) return;
+    if (t == 0) {
+        for (int s = 0; s < stages; s++) mbar_init(&mbar[s]);
+        for (int s = 0; s < stages; s++) {
+            const int r = blockIdx.x + s * G;
+            if (r < count) bulk_load(ring + (size_t)s * ring_stride, pixels + (int64_t)r * roi_stride, bytes, &mbar[s]);
+        }
+    }
+    __syncthreads();
+    const float invN = 1.0f / (float)n;
+    int it = 0;
+    for (int roi = blockIdx.x; roi < count; roi += G, it++) {
+        const int s = it % stages;
+        if (!mbar_wait(&mbar[s], (uint32_t)(it / stages) & 1u, kComWaitLimit) && P.err_flag)
+            atomicOr(P.err_flag, 4u);
+        const uint4 *src = reinterpret_cast<const uint4 *>(ring + (size_t)s * ring_stride);
+        float v[K][ppc];
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            const int c = t + k * T;
+            unpack<PDT>(c < nchunks ? src[c] : make_uint4(0, 0, 0, 0), v[k]);
+        }
+        if ((P.mode & kLT_ClearFirstFourPixels) && t == 0)  // QueuedCPUTracker.cpp:280-282
+#pragma unroll
+            for (int j = 0; j < 4; j++) v[0][j] = 0.0f;
+        float s1 = 0.0f, s2 = 0.0f;
+#pragma unroll
+        for (int k = 0; k < K; k++)
+#pragma unroll
+            for (int j = 0; j < ppc; j++) {
+                s1 += v[k][j];
+                s2 = fmaf(v[k][j], v[k][j], s2);
+            }
+        double m1[2] = {(double)s1, (double)s2};
+        cta_sum<2>(m1, red2);  // every thread has read buffer s
+        if (t == 0) {
+            const int r = roi + stages * G;
+            if (r < count) bulk_load(ring + (size_t)s * ring_stride, pixels + (int64_t)r * roi_stride, bytes, &mbar[s]);
+        }
+        const float mean = (float)(m1[0] * (double)invN);
+        const float stdev = sqrtf((float)(m1[1] * (double)invN - (double)(mean * mean)));
+        const float3 q = com_moments<PDT, K>(v, t, T, nchunks, W, mean, P.com_bgcorrection * stdev);
+        double m2[3] = {(double)q.x, (double)q.y, (double)q.z};
+        cta_sum<3>(m2, red3);
+        if (t == 0) com_result(results, roi, jobs, m2, mean, W, H);
     }
 }
 
 namespace {
 
 using ComKernel = void (*)(TrackParams, const uint8_t *, int64_t, const LocalizationJob *, int, LocalizationResult *);
+using ComStreamKernel = void (*)(TrackParams, const uint8_t *, int64_t, const LocalizationJob *, int,
+                                 LocalizationResult *, int, int);
+
+template <int PDT, int K>
+ComStreamKernel com_stream_at(int k)
+{
+    if constexpr (K > ChunkPixels<PDT>::max_chunks)
+        return nullptr;
+    else
+        return k == K ? com_stream_kernel<PDT, K> : com_stream_at<PDT, K + 1>(k);
+}
+
+// Ring of the streaming form: 3 buffers while they fit in 72 KB (3 CTAs of 320 threads per SM
+// for 100x100 u16 ROIs), else 2 within 200 KB; larger ROIs take the one-CTA-per-ROI form.
+bool com_stream_plan(int64_t roi_bytes, int &stages, int &stride)
+{
+    stride = (int)((roi_bytes + 127) & ~(int64_t)127);
+    if (3 * (int64_t)stride <= 72 * 1024)
+        stages = 3;
+    else if (2 * (int64_t)stride <= 200 * 1024)
+        stages = 2;
+    else
+        return false;
+    return true;
+}
+
+// CTAs of a streaming COM kernel that fit on the current device at once (cached per kernel,
+// device and shared-memory size); 0 when the query fails.
+int com_stream_ctas(ComStreamKernel f, int threads, int smem)
+{
+    struct Entry {
+        ComStreamKernel f;
+        int device, threads, smem, ctas;
+    };
+    static std::mutex mu;
+    static Entry cache[64];
+    static int ncache = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        for (int i = 0; i < ncache; i++)
+            if (cache[i].f == f && cache[i].device == dev && cache[i].threads == threads && cache[i].smem == smem)
+                return cache[i].ctas;
+    }
+    int per_sm = 0, sms = 0;
+    if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, threads, smem) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    const int ctas = per_sm * sms;
+    std::lock_guard<std::mutex> lk(mu);
+    if (ncache < 64) cache[ncache++] = Entry{f, dev, threads, smem, ctas};
+    return ctas;
+}
 
 // com_kernel<PDT, K> for K = k (1 <= k <= ChunkPixels<PDT>::max_chunks)
 template <int PDT, int K>
@@ -273,6 +422,19 @@ cudaError_t launch_com(const TrackParams &P, const uint8_t *pixels, int64_t roi_
     if (count <= 0) return cudaSuccess;
     int T, K;
     if (!com_shape(P, T, K)) return cudaErrorInvalidValue;
+    int stages = 0, stride = 0;
+    const int64_t roi_bytes = (int64_t)P.width * P.height * bytes_per_pixel(P.pdt);
+    if (com_stream_plan(roi_bytes, stages, stride)) {
+        ComStreamKernel f = P.pdt == 0 ? com_stream_at<0, 1>(K)
+                                       : (P.pdt == 1 ? com_stream_at<1, 1>(K) : com_stream_at<2, 1>(K));
+        const int smem = stages * stride;
+        const int ctas = f ? com_stream_ctas(f, T, smem) : 0;
+        if (ctas > 0) {
+            f<<<count < ctas ? count : ctas, T, smem, stream>>>(P, pixels, roi_stride, jobs, count, results, stages,
+                                                               stride);
+            return cudaGetLastError();
+        }
+    }
     ComKernel f = P.pdt == 0 ? com_kernel_at<0, 1>(K) : (P.pdt == 1 ? com_kernel_at<1, 1>(K) : com_kernel_at<2, 1>(K));
     if (!f) return cudaErrorInvalidValue;
     f<<<count, T, 0, stream>>>(P, pixels, roi_stride, jobs, count, results);

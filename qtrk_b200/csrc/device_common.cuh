@@ -548,13 +548,17 @@ __device__ __forceinline__ void qi_profiles_sym(const float *img, int W, int H, 
                                        const float *rweights, float4 *part, float2 *A, int log2L)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int S = nr >= (int)blockDim.x ? 1 : (int)blockDim.x / nr;
-    const int Aw = S < 4 ? S : 4, R = 32 / Aw;
-    const int nwr = nr >= R ? nr / R : 1, nsb = S / Aw;
+    // nr and blockDim are powers of two (QTrkComputedConfig::Update rounds qi_radialsteps,
+    // QueuedTracker.cpp:20), so the layout is all shifts: S = 2^lS subsets, Aw = 2^lA of them per
+    // warp, R = 2^lR radii per warp, nwr = 2^lw warps along the radius, nsb subset blocks
+    const int lnr = ilog2_pow2(nr), lbd = ilog2_pow2(blockDim.x);
+    const int lS = lnr >= lbd ? 0 : lbd - lnr, lA = lS < 2 ? lS : 2, lR = 5 - lA;
+    const int lw = lnr >= lR ? lnr - lR : 0;
+    const int S = 1 << lS, Aw = 1 << lA, nwr = 1 << lw, nsb = 1 << (lS - lA);
     const float kMagic = 8388608.0f;
     for (int wi = warp; wi < nwr * nsb; wi += nw) {
-        const int rb = wi % nwr, sb = wi / nwr;
-        const int i = rb * R + lane / Aw, sub = sb * Aw + lane % Aw;
+        const int rb = wi & (nwr - 1), sb = wi >> lw;
+        const int i = (rb << lR) + (lane >> lA), sub = (sb << lA) + (lane & (Aw - 1));
         float sm[4] = {0.0f, 0.0f, 0.0f, 0.0f};
         int cnt[4] = {0, 0, 0, 0};
         const float r = __fadd_rn(minr, __fmul_rn(rstep, (float)i));
@@ -581,7 +585,7 @@ __device__ __forceinline__ void qi_profiles_sym(const float *img, int W, int H, 
                     sm[2] += lerp_cell(rowm, ts, ixm, fxm, fym);  // q2 (-, -)
                     sm[3] += lerp_cell(rowm, ts, ixp, fxp, fym);  // q3 (+, -)
                 }
-                const int c = sub < nang ? (nang - sub + S - 1) / S : 0;
+                const int c = sub < nang ? (nang - sub + S - 1) >> lS : 0;
                 cnt[0] = cnt[1] = cnt[2] = cnt[3] = c;
             } else {
                 // bilinear()'s rule per coordinate: a sample is inside when -1 < x < W-1 and
@@ -628,14 +632,14 @@ __device__ __forceinline__ void qi_profiles_sym(const float *img, int W, int H, 
                 cnt[q] += __shfl_xor_sync(0xffffffffu, cnt[q], o);
             }
         if (nsb > 1) {  // subsets spread over warps (nr < blockDim/4): meet in shared memory
-            if (lane % Aw == 0 && i < nr) {
+            if ((lane & (Aw - 1)) == 0 && i < nr) {
                 part[2 * (sb * nr + i)] = make_float4(sm[0], sm[1], sm[2], sm[3]);
                 part[2 * (sb * nr + i) + 1] = make_float4(__int_as_float(cnt[0]), __int_as_float(cnt[1]),
                                                           __int_as_float(cnt[2]), __int_as_float(cnt[3]));
             }
             continue;
         }
-        if (lane % Aw == 0 && i < nr) {
+        if ((lane & (Aw - 1)) == 0 && i < nr) {
             float v[4];
 #pragma unroll
             for (int q = 0; q < 4; q++) {
@@ -794,11 +798,11 @@ __device__ __forceinline__ void radial_profile(const float *img, int W, int H, i
                                float minr, float rstep, const float2 *dirs, float *prof, bool normalize,
                                double *red)
 {
-    const int tpb = lanes_per_bin(nb);
+    const int tpb = lanes_per_bin(nb), ltpb = ilog2_pow2(tpb);
     const int total = nb * tpb;
     for (int base = 0; base < total; base += blockDim.x) {
         const int t = base + threadIdx.x;
-        const int bin = t / tpb, sub = t - bin * tpb;
+        const int bin = t >> ltpb, sub = t & (tpb - 1);
         double sum = 0.0;
         int cnt = 0;
         const float r = minr + rstep * (float)bin;

@@ -192,6 +192,10 @@ Tracker::Tracker(const QTrkSettings &settings)
     P.com_bgcorrection = s.com_bgcorrection;
     P.qi_iterations = s.qi_iterations;
     P.qi_nr = cfg.qi_radialsteps;
+    // the QI kernel lays its threads out by shifts: compute_config rounds the step count to a
+    // power of two (QueuedTracker.cpp:20), as the reference's FFT length 2 * nr assumes
+    if (P.qi_nr < 1 || (P.qi_nr & (P.qi_nr - 1)))
+        throw std::runtime_error("QI radial step count must be a power of two");
     P.qi_angpq = cfg.qi_angstepspq;
     P.qi_minr = s.qi_minradius;
     P.qi_maxr = cfg.qi_maxradius;
@@ -1637,9 +1641,10 @@ int Tracker::LocalizeDeviceNoAlloc(const void *d_pixels, int pitch, int64_t roi_
     TrackParams P;
     ZMatchParams Q;
     bool tc;
+    float *zprof = nullptr;
+    __nv_bfloat16 *zbf = nullptr;
     {
         std::lock_guard<std::mutex> lk(mu_);
-        P = LaunchParams(pdt);
         tc = UseTensorCoreMatch() && !d_jobs;  // device-side jobs: plain match, as LocalizeDevice
         if (tc) {
             const int nb = cfg.zlut_radialsteps, nbp = zmatch_padded_bins(nb);
@@ -1658,8 +1663,8 @@ int Tracker::LocalizeDeviceNoAlloc(const void *d_pixels, int pitch, int64_t roi_
                      " bytes of profile scratch; the fixed array holds " + std::to_string(scratch_bytes));
                 return -3;
             }
-            float *zprof = static_cast<float *>(scratch);
-            __nv_bfloat16 *zbf = reinterpret_cast<__nv_bfloat16 *>(static_cast<uint8_t *>(scratch) + prof_bytes);
+            zprof = static_cast<float *>(scratch);
+            zbf = reinterpret_cast<__nv_bfloat16 *>(static_cast<uint8_t *>(scratch) + prof_bytes);
             if (tc_lut_stale_) {  // refresh in place: one kernel launch into buffers of this shape
                 CheckCuda(cudaEventRecord(noalloc_order_, stream), "cudaEventRecord");
                 CheckCuda(cudaStreamWaitEvent(lut_stream_, noalloc_order_, 0), "cudaStreamWaitEvent");
@@ -1670,9 +1675,6 @@ int Tracker::LocalizeDeviceNoAlloc(const void *d_pixels, int pitch, int64_t roi_
                 CheckCuda(cudaEventRecord(lut_ready_, lut_stream_), "cudaEventRecord");
                 tc_lut_stale_ = false;
             }
-            P.zprof_f32 = zprof;
-            P.zprof_bf16 = zbf;
-            P.zprof_nbp = nbp;
             Q = TensorCoreParams();
             Q.prof_f32 = zprof;
             Q.prof_bf16 = zbf;
@@ -1681,6 +1683,13 @@ int Tracker::LocalizeDeviceNoAlloc(const void *d_pixels, int pitch, int64_t roi_
             Q.count = count;
             Q.uniform_bead = 0;
             Q.results = d_results;
+        }
+        // after the checks above, so that a refused call launches nothing
+        P = LaunchParams(pdt);
+        if (tc) {
+            P.zprof_f32 = zprof;
+            P.zprof_bf16 = zbf;
+            P.zprof_nbp = Q.nbp;
         }
     }
     CheckCuda(cudaStreamWaitEvent(stream, lut_ready_, 0), "cudaStreamWaitEvent");
