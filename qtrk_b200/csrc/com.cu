@@ -108,41 +108,89 @@ namespace {
 constexpr int kComMaxStages = 4;
 constexpr uint32_t kComWaitLimit = 1u << 22;  // mbarrier polls before a staged ROI counts as lost
 
+// Where this thread's first chunk starts (pixel t * ppc of the ROI, as float column and row) and
+// how far its next chunk is (T * ppc pixels: fdx columns and fdy rows, fdx < W), so that pass 2
+// walks its chunks with float counters instead of dividing by W per chunk.
+struct ChunkWalk {
+    float fx, fy, fdx, fdy;
+};
+
+__device__ __forceinline__ ChunkWalk chunk_walk(int t, int T, int ppc, int W)
+{
+    const int i0 = t * ppc, step = T * ppc;
+    ChunkWalk w;
+    w.fx = (float)(i0 % W);
+    w.fy = (float)(i0 / W);
+    w.fdx = (float)(step % W);
+    w.fdy = (float)(step / W);
+    return w;
+}
+
 // Pass 2 of ComputeMeanAndCOM on this thread's chunks (see the chunk moments above): returns the
-// FP32 partial sums of v', x v' and y v'.
-template <int PDT, int K>
-__device__ __forceinline__ float3 com_moments(const float (&v)[K][ChunkPixels<PDT>::n], int t, int T, int nchunks, int W,
-                                              float mean, float thr)
+// FP32 partial sums of v', x v' and y v'. kThr: a background threshold is set (v' = max(0, |v -
+// mean| - thr)); without one v' = |v - mean| exactly.
+template <int PDT, int K, bool kThr>
+__device__ __forceinline__ float3 com_moments(const float (&v)[K][ChunkPixels<PDT>::n], ChunkWalk w, int t, int T,
+                                              int nchunks, int W, float mean, float thr)
 {
     constexpr int ppc = ChunkPixels<PDT>::n;
+    const float fW = (float)W;
     float q0 = 0.0f, qx = 0.0f, qy = 0.0f;
 #pragma unroll
     for (int k = 0; k < K; k++) {
         const int c = t + k * T;
         if (c < nchunks) {
-            const int i0 = c * ppc;
-            const int y0 = i0 / W, x0 = i0 - y0 * W;
             float a[ppc];
             float S = 0.0f, Sj = 0.0f;
 #pragma unroll
             for (int j = 0; j < ppc; j++) {
-                a[j] = fmaxf(0.0f, fabsf(v[k][j] - mean) - thr);
+                a[j] = kThr ? fmaxf(0.0f, fabsf(v[k][j] - mean) - thr) : fabsf(v[k][j] - mean);
                 S += a[j];
                 if (j > 0) Sj = fmaf((float)j, a[j], Sj);
             }
-            const int split = W - x0;  // first j on the next row
+            const float split = fW - w.fx;  // first j on the next row
             float Sw = 0.0f;
-            if (split < ppc) {
+            if (split < (float)ppc) {
 #pragma unroll
                 for (int j = 0; j < ppc; j++)
-                    if (j >= split) Sw += a[j];
+                    if ((float)j >= split) Sw += a[j];
             }
             q0 += S;
-            qx += fmaf((float)x0, S, Sj) - (float)W * Sw;
-            qy += fmaf((float)y0, S, Sw);
+            qx += fmaf(w.fx, S, Sj) - fW * Sw;
+            qy += fmaf(w.fy, S, Sw);
+        }
+        w.fx += w.fdx;
+        w.fy += w.fdy;
+        if (w.fx >= fW) {
+            w.fx -= fW;
+            w.fy += 1.0f;
         }
     }
     return make_float3(q0, qx, qy);
+}
+
+// Pass 1 partial sums (v, and v^2 when a background threshold needs the standard deviation) of
+// this thread's converted pixels.
+template <int PDT, int K>
+__device__ __forceinline__ float2 com_pass1(const float (&v)[K][ChunkPixels<PDT>::n], bool squares)
+{
+    constexpr int ppc = ChunkPixels<PDT>::n;
+    float s = 0.0f, s2 = 0.0f;
+    if (squares) {
+#pragma unroll
+        for (int k = 0; k < K; k++)
+#pragma unroll
+            for (int j = 0; j < ppc; j++) {
+                s += v[k][j];
+                s2 = fmaf(v[k][j], v[k][j], s2);
+            }
+    } else {
+#pragma unroll
+        for (int k = 0; k < K; k++)
+#pragma unroll
+            for (int j = 0; j < ppc; j++) s += v[k][j];
+    }
+    return make_float2(s, s2);
 }
 
 // The 13-word LocalizationResult of a COM-only localization (thread 0).
@@ -203,16 +251,10 @@ __global__ void __launch_bounds__(kComMaxThreads) com_kernel(TrackParams P, cons
 #pragma unroll
         for (int j = 0; j < 4; j++) v[0][j] = 0.0f;
 
-    // pass 1: sum and sum of squares (chunks past the ROI hold zeros)
-    float s = 0.0f, s2 = 0.0f;
-#pragma unroll
-    for (int k = 0; k < K; k++)
-#pragma unroll
-        for (int j = 0; j < ppc; j++) {
-            s += v[k][j];
-            s2 = fmaf(v[k][j], v[k][j], s2);
-        }
-    double m1[2] = {(double)s, (double)s2};
+    // pass 1: sum and, for a background threshold, sum of squares (chunks past the ROI hold zeros)
+    const bool bg = P.com_bgcorrection != 0.0f;
+    const float2 p1 = com_pass1<PDT, K>(v, bg);
+    double m1[2] = {(double)p1.x, (double)p1.y};
     cta_sum<2>(m1, red2);
     const float invN = 1.0f / (float)n;
     const float mean = (float)(m1[0] * (double)invN);
@@ -220,7 +262,9 @@ __global__ void __launch_bounds__(kComMaxThreads) com_kernel(TrackParams P, cons
     const float thr = P.com_bgcorrection * stdev;
 
     // pass 2: background-corrected moments
-    const float3 mo = com_moments<PDT, K>(v, t, T, nchunks, W, mean, thr);
+    const ChunkWalk wk = chunk_walk(t, T, ppc, W);
+    const float3 mo = bg ? com_moments<PDT, K, true>(v, wk, t, T, nchunks, W, mean, thr)
+                         : com_moments<PDT, K, false>(v, wk, t, T, nchunks, W, mean, 0.0f);
     double m2[3] = {(double)mo.x, (double)mo.y, (double)mo.z};
     cta_sum<3>(m2, red3);
     if (t == 0) com_result(results, roi, jobs, m2, mean, W, P.height);
@@ -260,6 +304,8 @@ __global__ void __launch_bounds__(kComMaxThreads) com_stream_kernel(TrackParams 
     }
     __syncthreads();
     const float invN = 1.0f / (float)n;
+    const bool bg = P.com_bgcorrection != 0.0f;
+    const ChunkWalk wk = chunk_walk(t, T, ppc, W);
     int it = 0;
     for (int roi = blockIdx.x; roi < count; roi += G, it++) {
         const int s = it % stages;
@@ -275,15 +321,8 @@ __global__ void __launch_bounds__(kComMaxThreads) com_stream_kernel(TrackParams 
         if ((P.mode & kLT_ClearFirstFourPixels) && t == 0)  // QueuedCPUTracker.cpp:280-282
 #pragma unroll
             for (int j = 0; j < 4; j++) v[0][j] = 0.0f;
-        float s1 = 0.0f, s2 = 0.0f;
-#pragma unroll
-        for (int k = 0; k < K; k++)
-#pragma unroll
-            for (int j = 0; j < ppc; j++) {
-                s1 += v[k][j];
-                s2 = fmaf(v[k][j], v[k][j], s2);
-            }
-        double m1[2] = {(double)s1, (double)s2};
+        const float2 p1 = com_pass1<PDT, K>(v, bg);
+        double m1[2] = {(double)p1.x, (double)p1.y};
         cta_sum<2>(m1, red2);  // every thread has read buffer s
         if (t == 0) {
             const int r = roi + stages * G;
@@ -291,7 +330,8 @@ __global__ void __launch_bounds__(kComMaxThreads) com_stream_kernel(TrackParams 
         }
         const float mean = (float)(m1[0] * (double)invN);
         const float stdev = sqrtf((float)(m1[1] * (double)invN - (double)(mean * mean)));
-        const float3 q = com_moments<PDT, K>(v, t, T, nchunks, W, mean, P.com_bgcorrection * stdev);
+        const float3 q = bg ? com_moments<PDT, K, true>(v, wk, t, T, nchunks, W, mean, P.com_bgcorrection * stdev)
+                            : com_moments<PDT, K, false>(v, wk, t, T, nchunks, W, mean, 0.0f);
         double m2[3] = {(double)q.x, (double)q.y, (double)q.z};
         cta_sum<3>(m2, red3);
         if (t == 0) com_result(results, roi, jobs, m2, mean, W, H);

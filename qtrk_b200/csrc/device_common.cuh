@@ -480,7 +480,40 @@ __device__ ComResult com_from_sums(const G &g, const float *img, int W, int H, f
     r.stdev = sqrtf((float)(s[1] * (double)invN - (double)(r.mean * r.mean)));
     const float thr = bgcorr * r.stdev;
     float q0 = 0.0f, qx = 0.0f, qy = 0.0f;
-    {
+    if (!(W & 3) && !(reinterpret_cast<uintptr_t>(img) & 15)) {
+        // rows are whole float4 chunks: chunk c holds pixels 4c .. 4c+3 of one row, at column fx
+        // and row fy; per chunk S = sum v', Sj = sum j v', so sum x v' = fx S + Sj
+        const int nc = n >> 2, cstride = stride * 4;
+        const float fW = (float)W, fdx = (float)(cstride % W), fdy = (float)(cstride / W);
+        float fx = (float)((4 * g.rank()) % W), fy = (float)((4 * g.rank()) / W);
+        const float4 *img4 = reinterpret_cast<const float4 *>(img);
+        for (int c = g.rank(); c < nc; c += stride) {
+            const float4 q = img4[c];
+            float a0, a1, a2, a3;
+            if (thr == 0.0f) {  // max(0, |d| - 0) is |d|
+                a0 = fabsf(q.x - r.mean);
+                a1 = fabsf(q.y - r.mean);
+                a2 = fabsf(q.z - r.mean);
+                a3 = fabsf(q.w - r.mean);
+            } else {
+                a0 = fmaxf(0.0f, fabsf(q.x - r.mean) - thr);
+                a1 = fmaxf(0.0f, fabsf(q.y - r.mean) - thr);
+                a2 = fmaxf(0.0f, fabsf(q.z - r.mean) - thr);
+                a3 = fmaxf(0.0f, fabsf(q.w - r.mean) - thr);
+            }
+            const float S = (a0 + a1) + (a2 + a3);
+            const float Sj = fmaf(3.0f, a3, fmaf(2.0f, a2, a1));
+            q0 += S;
+            qx += fmaf(fx, S, Sj);
+            qy = fmaf(fy, S, qy);
+            fx += fdx;
+            fy += fdy;
+            if (fx >= fW) {
+                fx -= fW;
+                fy += 1.0f;
+            }
+        }
+    } else {
         int x = g.rank() % W, y = g.rank() / W;
         float fx = (float)x, fy = (float)y;
         for (int i = g.rank(); i < n; i += stride) {
@@ -639,13 +672,15 @@ __device__ __forceinline__ void qi_profiles_sym(const float *img, int W, int H, 
             }
             continue;
         }
+        float v[4];
         if ((lane & (Aw - 1)) == 0 && i < nr) {
-            float v[4];
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                v[q] = cnt[q] >= 4 ? sm[q] / (float)cnt[q] : mean;
-                if (rweights) v[q] *= rweights[i];
+            for (int k = 0; k < 4; k++) {
+                v[k] = cnt[k] >= 4 ? sm[k] / (float)cnt[k] : mean;
+                if (rweights) v[k] *= rweights[i];
             }
+        }
+        if ((lane & (Aw - 1)) == 0 && i < nr) {
             const int n0 = nr - 1 - i, n1 = nr + i;
             A[log2L >= 0 ? (int)bitrev(n0, log2L) : n0] = make_float2(v[1] + v[2], v[2] + v[3]);
             A[log2L >= 0 ? (int)bitrev(n1, log2L) : n1] = make_float2(v[0] + v[3], v[0] + v[1]);
