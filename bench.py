@@ -171,6 +171,26 @@ def dist_env():
     return e.world_size, e.rank, e.local_rank
 
 
+def issue_limits(profile_json: Path, kernel_ms: float, sm_mhz: float | None) -> dict:
+    """What binds a kernel that is not HBM-bound: its warp instructions per launch over the SMs'
+    issue capacity in the measured time (148 SMs x 4 schedulers x SM clock), and its shared-memory
+    wavefronts over the shared-memory data pipe (one wavefront per SM per clock). The per-launch
+    counts come from the ncu capture summarised in profiles/ (the same workload and kernel)."""
+    out = {"binding_limit": None, "issue_frac": None, "smem_pipe_frac": None}
+    if not profile_json.exists() or not sm_mhz or kernel_ms <= 0:
+        return out
+    d = json.loads(profile_json.read_text())
+    cycles = sm_mhz * 1e6 * kernel_ms / 1e3
+    if d.get("warp_instructions_per_launch"):
+        out["issue_frac"] = d["warp_instructions_per_launch"] / (148 * 4 * cycles)
+    if d.get("smem_wavefronts_per_launch"):
+        out["smem_pipe_frac"] = d["smem_wavefronts_per_launch"] / (148 * cycles)
+    fr = {"instruction issue": out["issue_frac"] or 0.0, "shared-memory pipe": out["smem_pipe_frac"] or 0.0}
+    out["binding_limit"] = max(fr, key=fr.get)
+    out["counts_source"] = str(profile_json.relative_to(ROOT))
+    return out
+
+
 def measured_peaks() -> tuple[dict, str]:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -625,7 +645,7 @@ def workloads_bench(dev, steps: int, warmup: int) -> dict:
 COM_BYTES_PER_ROI = 100 * 100 * 2 + 52  # pixels in, result out (no job records: jobs pointer is null)
 
 
-def com_only_bench(dev, settings, d_rois, n: int, steps: int, warmup: int) -> dict:
+def com_only_bench(dev, settings, d_rois, n: int, steps: int, warmup: int, sm_mhz: float | None = None) -> dict:
     """LT_OnlyCOM on the headline stack (n ROIs of 100x100 u16 resident in HBM): the register-held
     streaming COM kernel, one launch per step, with its roofline against the measured HBM copy rate."""
     import torch
@@ -647,11 +667,13 @@ def com_only_bench(dev, settings, d_rois, n: int, steps: int, warmup: int) -> di
     tfile = ROOT / "profiles" / "com_100x100_u16_traffic.json"
     if tfile.exists():
         traffic = json.loads(tfile.read_text()).get("dram_bytes_per_launch")
+    roof_extra = issue_limits(tfile, ms, sm_mhz)
     return {"workload": f"LT_OnlyCOM, {n:,} ROIs of 100x100 u16 resident in HBM (200 MB > L2), one launch per step",
             "rois_per_s": n / (ms / 1e3), "ms_per_launch": ms, "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "qtrk::com_kernel<1, 4>", "kernel_ms": ms, "bytes_per_roi": COM_BYTES_PER_ROI}}
+                         "kernel": "qtrk::com_stream_kernel<1, 4>", "kernel_ms": ms,
+                         "bytes_per_roi": COM_BYTES_PER_ROI, **roof_extra}}
 
 
 def serving_bench(dev, main_trk, main_rois, seconds: float, fps: float) -> dict:
@@ -1051,7 +1073,8 @@ def main(argv=None) -> int:
         workloads = workloads_bench(dev, args.steps, args.warmup)
     if rank == 0 and ws == 1 and not args.ncu:
         workloads = workloads or {"gpu_launches": 0}
-        workloads["com_only_100x100_u16"] = com_only_bench(dev, s, d_rois, N_ROIS, args.steps, args.warmup)
+        workloads["com_only_100x100_u16"] = com_only_bench(dev, s, d_rois, N_ROIS, args.steps, args.warmup,
+                                                            clocks.get("sm_mhz"))
         workloads["gpu_launches"] += workloads["com_only_100x100_u16"]["gpu_launches"]
 
     # ---- roofline of the localization kernel ----
@@ -1063,8 +1086,9 @@ def main(argv=None) -> int:
         traffic = json.loads(tfile.read_text()).get("dram_bytes_per_launch")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_kind": peak_kind,
-                "kernel": "qtrk::localize_kernel<false>", "kernel_ms": kernel_ms,
+                "kernel": "qtrk::localize_qi_kernel<true>", "kernel_ms": kernel_ms,
                 "bytes_per_roi": BYTES_PER_ROI}
+    roofline.update(issue_limits(tfile, kernel_ms, clocks.get("sm_mhz")))
 
     # ---- accuracy vs truth (stated pixel size) ----
     err_xy = np.hypot(res_dev["pos"][:, 0] - wl.true_xyz[:, 0], res_dev["pos"][:, 1] - wl.true_xyz[:, 1])

@@ -843,22 +843,36 @@ __device__ __forceinline__ void radial_profile(const float *img, int W, int H, i
         const float r = minr + rstep * (float)bin;
         // one path per warp (see qi_profiles_sym)
         const bool inside = __all_sync(0xffffffffu, bin >= nb || circle_inside(cx, cy, fabsf(r), W, H));
-        if (bin < nb) {
-            // FP32 sums over groups of 8 samples, folded into an FP64 total (the reference
-            // adds every sample in FP64; 8-sample FP32 groups stay within ~1e-7 of it).
+        if (bin < nb && inside) {
+            // This lane's directions are sub, sub + tpb, ...: nl of them, taken in groups of 8
+            // summed in FP32 and folded into an FP64 total (the reference adds every sample in
+            // FP64; 8-sample FP32 groups stay within ~1e-7 of it). Whole groups run without
+            // per-sample checks, then the remainder.
+            const int nl = sub < nang ? (nang - sub + tpb - 1) >> ltpb : 0;
+            const float2 *dl = dirs + sub;
+            int k = 0;
+            for (; k + 8 <= nl; k += 8) {
+                float part = 0.0f;
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const float2 d = dl[(k + u) << ltpb];
+                    part += bilinear_inside(img, ts, cx + d.x * r, cy + d.y * r);
+                }
+                sum += (double)part;
+            }
+            if (k < nl) {
+                float part = 0.0f;
+                for (; k < nl; k++) {
+                    const float2 d = dl[k << ltpb];
+                    part += bilinear_inside(img, ts, cx + d.x * r, cy + d.y * r);
+                }
+                sum += (double)part;
+            }
+            cnt = nl;
+        } else if (bin < nb) {
             for (int a0 = sub; a0 < nang; a0 += 8 * tpb) {
                 float part = 0.0f;
-                if (inside) {
-#pragma unroll
-                    for (int k = 0; k < 8; k++) {
-                        const int a = a0 + k * tpb;
-                        if (a < nang) {
-                            const float2 d = dirs[a];
-                            part += bilinear_inside(img, ts, cx + d.x * r, cy + d.y * r);
-                            cnt++;
-                        }
-                    }
-                } else {
+                {
 #pragma unroll
                     for (int k = 0; k < 8; k++) {
                         const int a = a0 + k * tpb;
