@@ -571,10 +571,9 @@ def workloads_bench(dev, steps: int, warmup: int) -> dict:
         cb = reference_cpu("buildlut", -1, settings=cs, stack=hs[:40])
         if cb is not None:
             cb["host"] = host_cpu()
-            cb["sample"] = "BeginLUT / 40 x BuildLUT(256 ROIs) / FinalizeLUT (planes 0-39 of the stack), numThreads=-1"
-            one = reference_cpu("buildlut", 1, settings=cs, stack=hs[:4])
-            one["sample"] = "4 planes x 256 ROIs, numThreads=1"
-            cb["single_thread"] = one
+            cb["sample"] = ("BeginLUT / 40 x BuildLUT(256 ROIs) / FinalizeLUT (planes 0-39 of the stack); the "
+                            "reference's BuildLUT spreads each plane's beads over every host thread whatever "
+                            "numThreads says (parallel_for, threads.h:252-261)")
         out["buildlut_256x200_80x80_u16"]["cpu_baseline"] = cb
         del d_plane
         flat = d_stack.view(-1, 80, 80)
@@ -635,8 +634,15 @@ def workloads_bench(dev, steps: int, warmup: int) -> dict:
         from oracle import RefOracle
 
         rr = RefOracle().track(s1, wl1.mode, wl1.rois, lut1)
-        out["roi60_f32_1000"]["vs_reference_max_dxy_px"] = float(np.abs(res1["pos"][:, :2] - rr["pos"][:, :2]).max())
-        out["roi60_f32_1000"]["vs_reference_max_dz_planes"] = float(np.abs(res1["pos"][:, 2] - rr["pos"][:, 2]).max())
+        # as in the parity tests: ROIs whose QI walked > 5 px from the COM (the bead was lost) and z
+        # values beyond the LUT (parabola vertex extrapolated past its edge) are ill-conditioned in
+        # the reference's own arithmetic and are counted, not compared
+        conv = np.hypot(rr["pos"][:, 0] - rr["firstGuess"][:, 0], rr["pos"][:, 1] - rr["firstGuess"][:, 1]) <= 5
+        zin = conv & (rr["pos"][:, 2] >= 0) & (rr["pos"][:, 2] <= lut1.shape[1] - 1)
+        out["roi60_f32_1000"]["vs_reference_max_dxy_px"] = float(np.abs(res1["pos"][conv, :2] - rr["pos"][conv, :2]).max())
+        out["roi60_f32_1000"]["vs_reference_max_dz_planes"] = float(np.abs(res1["pos"][zin, 2] - rr["pos"][zin, 2]).max())
+        out["roi60_f32_1000"]["rois_where_qi_lost_the_bead"] = int((~conv).sum())
+        out["roi60_f32_1000"]["rois_with_z_past_the_lut"] = int((conv & ~zin).sum())
     out["roi60_f32_1000"]["cpu_baseline"] = cb
     out["gpu_launches"] = int(launches)
     return out

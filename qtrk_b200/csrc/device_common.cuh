@@ -577,8 +577,8 @@ __device__ __forceinline__ float lerp_cell(const float *row, int ts, int ix, flo
 // one complex value z = X + iY per position, in bit-reversed order (log2L = log2(2 nr)) or in
 // natural order when log2L < 0. All threads call; a barrier must follow before A is read.
 __device__ __forceinline__ void qi_profiles_sym(const float *img, int W, int H, int ts, float cx, float cy, float mean, int nr,
-                                       int nang, int stride, float minr, float rstep, const float2 *dirs,
-                                       const float *rweights, float4 *part, float2 *A, int log2L)
+                                       int nang, float inv_nang, int stride, float minr, float rstep,
+                                       const float2 *dirs, const float *rweights, float4 *part, float2 *A, int log2L)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     // nr and blockDim are powers of two (QTrkComputedConfig::Update rounds qi_radialsteps,
@@ -657,12 +657,13 @@ __device__ __forceinline__ void qi_profiles_sym(const float *img, int W, int H, 
                 }
             }
         }
-        // subsets of one radius: lanes that differ in their low log2(Aw) bits
+        // subsets of one radius: lanes that differ in their low log2(Aw) bits (on the fast path
+        // every count is nang: only the sums travel)
         for (int o = 1; o < Aw; o <<= 1)
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 sm[q] += __shfl_xor_sync(0xffffffffu, sm[q], o);
-                cnt[q] += __shfl_xor_sync(0xffffffffu, cnt[q], o);
+                if (!fast || nsb > 1) cnt[q] += __shfl_xor_sync(0xffffffffu, cnt[q], o);
             }
         if (nsb > 1) {  // subsets spread over warps (nr < blockDim/4): meet in shared memory
             if ((lane & (Aw - 1)) == 0 && i < nr) {
@@ -674,10 +675,16 @@ __device__ __forceinline__ void qi_profiles_sym(const float *img, int W, int H, 
         }
         float v[4];
         if ((lane & (Aw - 1)) == 0 && i < nr) {
+            const float rw = rweights ? rweights[i] : 1.0f;
+            if (fast) {  // nang >= 4 in-bounds samples per bin: the mean, as sum * (1 / nang)
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                v[k] = cnt[k] >= 4 ? sm[k] / (float)cnt[k] : mean;
-                if (rweights) v[k] *= rweights[i];
+                for (int k = 0; k < 4; k++) v[k] = rweights ? (sm[k] * inv_nang) * rw : sm[k] * inv_nang;
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    v[k] = cnt[k] >= 4 ? sm[k] / (float)cnt[k] : mean;
+                    if (rweights) v[k] *= rw;
+                }
             }
         }
         if ((lane & (Aw - 1)) == 0 && i < nr) {

@@ -30,6 +30,7 @@ __device__ const float kZLUTWeights[7] = {0.15f, 0.5f, 0.85f, 1.0f, 0.85f, 0.5f,
 struct SmemView {
     float *img, *misc;
     float2 *qdirs, *tw, *zdirs;
+    float *qrw;  // QI radial weights (qi_nr floats after the twiddles)
     uint8_t *work;
     double *red;
 };
@@ -44,6 +45,7 @@ __device__ __forceinline__ SmemView smem_view(uint8_t *smem, const TrackParams &
     float2 *tab = reinterpret_cast<float2 *>(smem + P.sm_tables);
     v.qdirs = tab;
     v.tw = tab + P.qi_angpq;  // L/2 = qi_nr twiddles
+    v.qrw = reinterpret_cast<float *>(v.tw + P.qi_nr);
     v.zdirs = tab;            // loaded over the QI tables once QI is done (load_z_tables)
     return v;
 }
@@ -58,6 +60,8 @@ __device__ __forceinline__ void load_qi_tables(const SmemView &s, const TrackPar
         for (int i = threadIdx.x; i < P.qi_angpq; i += blockDim.x) s.qdirs[i] = qd[i];
     if (tw)
         for (int i = threadIdx.x; i < P.qi_nr; i += blockDim.x) s.tw[i] = tw[i];
+    if (P.qi_rweights)
+        for (int i = threadIdx.x; i < P.qi_nr; i += blockDim.x) s.qrw[i] = P.qi_rweights[i];
 }
 
 // Copy the full-circle direction table over the QI tables (all threads; the QI stage must
@@ -83,7 +87,7 @@ __device__ void qi_localize(const SmemView &s, const TrackParams &P, float mean,
     const float rstep = (P.qi_maxr - P.qi_minr) / (float)nr;  // also pixelsPerProfLen (cpu_tracker.cpp:311,649)
     for (int k = 0; k < P.qi_iterations; k++) {
         bhit = check_boundaries(cx, cy, P.qi_maxr, W, H);
-        qi_profiles_sym(s.img, W, H, W, cx, cy, mean, nr, P.qi_nang[k], P.qi_stride[k], P.qi_minr, rstep,
+        qi_profiles_sym(s.img, W, H, W, cx, cy, mean, nr, P.qi_nang[k], P.qi_inv_nang[k], P.qi_stride[k], P.qi_minr, rstep,
                         s.qdirs, rweights, part, A, pow2 ? ilog2_pow2(L) : -1);
         __syncthreads();
         if (pow2) {
@@ -242,7 +246,7 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
     }
     float x = comx, y = comy, z = 0.0f;
     bool bhit = false;
-    if (P.mode & kLT_QI) qi_localize(s, P, com.mean, x, y, bhit, P.qi_rweights);
+    if (P.mode & kLT_QI) qi_localize(s, P, com.mean, x, y, bhit, P.qi_rweights ? s.qrw : nullptr);
     if (P.mode & kLT_LocalizeZ) {
         bhit = check_boundaries(x, y, P.z_maxr, W, H);
         z = z_localize(s, P, com.mean, x, y, bead, roi);
@@ -427,7 +431,7 @@ void plan_smem(TrackParams &P)
     const int nr = P.qi_nr > 0 ? P.qi_nr : 1, L = 2 * nr;
     P.sm_img = 0;
     P.sm_tables = align16(W * H * 4);
-    const int qi_tables = (P.qi_angpq + nr) * 8, z_tables = P.z_angsteps * 8;
+    const int qi_tables = (P.qi_angpq + nr) * 8 + nr * 4, z_tables = P.z_angsteps * 8;
     P.sm_work = P.sm_tables + align16(qi_tables > z_tables ? qi_tables : z_tables);
     // [ ac | A ] (L complex each) + 2 KB of subset partials when the QI directions are split over warps
     const int qi_work = 2 * L * 8 + (nr < kBlockThreads / 4 ? 2048 : 0);

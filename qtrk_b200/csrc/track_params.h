@@ -43,6 +43,7 @@ struct TrackParams {
     float qi_minr, qi_maxr;
     int qi_nang[kMaxQIIterations];    // angular samples per quadrant in iteration k (>= 4)
     int qi_stride[kMaxQIIterations];  // direction-table stride in iteration k (cpu_tracker.cpp:655-657)
+    float qi_inv_nang[kMaxQIIterations];  // 1 / qi_nang[k] (bins whose samples are all in bounds)
     const void *qi_dirs;              // float2[qi_angpq]: quadrant directions (cos, sin)
     const float *qi_rweights;         // float[qi_nr] radial bin window or nullptr
     const void *qi_twiddles;          // float2[L/2], e^{-2 pi i k / L}, L = 2 qi_nr

@@ -207,6 +207,7 @@ Tracker::Tracker(const QTrkSettings &settings)
             if (n < 4) n = 4;
             const float angstepf = (float)cfg.qi_angstepspq / n;
             P.qi_nang[k] = n;
+            P.qi_inv_nang[k] = 1.0f / (float)n;
             P.qi_stride[k] = (int)angstepf;
             angsteps *= s.qi_angstep_factor;
         }
