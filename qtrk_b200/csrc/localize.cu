@@ -231,8 +231,10 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
     load_qi_tables(s, P);
     float2 part;
     if constexpr (kStaged) {
-        __syncthreads();  // the mbarrier is initialised
-        if (!mbar_wait(mbar, 0, kStageWaitLimit) && P.err_flag) atomicOr(P.err_flag, 4u);
+        // one thread waits for the copy (its acquire, then the barrier, order the copied bytes
+        // before every thread's reads); the others wait at the barrier without polling
+        if (threadIdx.x == 0 && !mbar_wait(mbar, 0, kStageWaitLimit) && P.err_flag) atomicOr(P.err_flag, 4u);
+        __syncthreads();
         part = convert_staged(g, s.img, P, bead);
     } else {
         const int64_t off = roi_offsets ? roi_offsets[roi] : (int64_t)roi * roi_stride;
