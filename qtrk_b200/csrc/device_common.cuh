@@ -110,6 +110,20 @@ __device__ __forceinline__ float bilinear_inside(const float *img, int ts, float
     return v0 + (v1 - v0) * fy;
 }
 
+// Two bilinear samples at once with the packed FP32x2 operations of sm_100 (each component
+// rounds as the scalar operation does): cells at p and q, fractions fx = (fx_p, fx_q) and
+// fy = (fy_p, fy_q). Same arithmetic as lerp_cell, one instruction per pair of samples; the
+// differences v10 - v00 are fma(v00, -1, v10), exact before their one rounding.
+__device__ __forceinline__ float2 lerp_cell2(const float *p, const float *q, int ts, float2 fx, float2 fy)
+{
+    const float2 m1 = make_float2(-1.0f, -1.0f);
+    const float2 v00 = make_float2(p[0], q[0]), v10 = make_float2(p[1], q[1]);
+    const float2 v01 = make_float2(p[ts], q[ts]), v11 = make_float2(p[ts + 1], q[ts + 1]);
+    const float2 v0 = __ffma2_rn(__ffma2_rn(v00, m1, v10), fx, v00);
+    const float2 v1 = __ffma2_rn(__ffma2_rn(v01, m1, v11), fx, v01);
+    return __ffma2_rn(__ffma2_rn(v0, m1, v1), fy, v0);
+}
+
 // True when every point cx + a*r, cy + b*r with |a|, |b| <= 1 (any sample of a circle of radius
 // r around (cx, cy)) lies strictly inside (0, w-1) x (0, h-1), rounding of the sample
 // coordinates included (margin 1e-3 px, far above one ulp of the coordinates).
@@ -567,7 +581,10 @@ __device__ __forceinline__ float lerp_cell(const float *row, int ts, int ix, flo
 // thread takes one radius and a strided subset of the directions and produces all four samples
 // of each: the products d.x r, d.y r, the truncations and fractions of the two x and two y
 // coordinates are shared by four samples. Coordinates are formed as the reference forms them
-// (d.x r rounded, then added to the centre). Layout: S = blockDim/nr direction subsets
+// (d.x r rounded, then added to the centre). The table holds each direction as (d.x, d.x, d.y, d.y)
+// so that on the fast path x = (cx, cx) + (d.x, d.x) * (r, -r) gives (x+, x-) in one packed
+// multiply and one packed add; the diagonal quadrants q0 (+, +) and q2 (-, -) then share
+// fractions (fx+, fx-), (fy+, fy-) and are sampled as one pair, q3 (+, -) and q1 (-, +) as another. Layout: S = blockDim/nr direction subsets
 // (directions sub, sub + S, ...); a warp holds R = 32/A radii x A = min(S, 4) adjacent subsets,
 // so its gathers fall into a small patch. Per quadrant and radius the bin value
 // is the mean of the in-bounds samples (the image mean when fewer than 4), times the radial
@@ -578,7 +595,7 @@ __device__ __forceinline__ float lerp_cell(const float *row, int ts, int ix, flo
 // natural order when log2L < 0. All threads call; a barrier must follow before A is read.
 __device__ __forceinline__ void qi_profiles_sym(const float *img, int W, int H, int ts, float cx, float cy, float mean, int nr,
                                        int nang, float inv_nang, int stride, float minr, float rstep,
-                                       const float2 *dirs, const float *rweights, float4 *part, float2 *A, int log2L)
+                                       const float4 *dirs, const float *rweights, float4 *part, float2 *A, int log2L)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     // nr and blockDim are powers of two (QTrkComputedConfig::Update rounds qi_radialsteps,
@@ -601,23 +618,27 @@ __device__ __forceinline__ void qi_profiles_sym(const float *img, int W, int H, 
         const bool fast = __all_sync(0xffffffffu, i >= nr || circle_inside(cx, cy, fabsf(r), W, H));
         if (i < nr) {
             if (fast) {
+                const float2 rr = make_float2(r, -r), cxx = make_float2(cx, cx), cyy = make_float2(cy, cy);
+                const float2 K = make_float2(kMagic, kMagic), nK = make_float2(-kMagic, -kMagic);
+                const float2 m1 = make_float2(-1.0f, -1.0f);
+                float2 s02 = make_float2(0.0f, 0.0f), s31 = make_float2(0.0f, 0.0f);
                 for (int a = sub; a < nang; a += S) {
-                    const float2 d = dirs[stride * a];
-                    const float dx = __fmul_rn(d.x, r), dy = __fmul_rn(d.y, r);
-                    const float xp = __fadd_rn(cx, dx), xm = __fadd_rn(cx, -dx);
-                    const float yp = __fadd_rn(cy, dy), ym = __fadd_rn(cy, -dy);
-                    const float txp = __fadd_rz(xp, kMagic), txm = __fadd_rz(xm, kMagic);
-                    const float typ = __fadd_rz(yp, kMagic), tym = __fadd_rz(ym, kMagic);
-                    const float fxp = xp - (txp - kMagic), fxm = xm - (txm - kMagic);
-                    const float fyp = yp - (typ - kMagic), fym = ym - (tym - kMagic);
-                    const int ixp = __float_as_int(txp) - 0x4B000000, ixm = __float_as_int(txm) - 0x4B000000;
-                    const float *rowp = img + (__float_as_int(typ) - 0x4B000000) * ts;
-                    const float *rowm = img + (__float_as_int(tym) - 0x4B000000) * ts;
-                    sm[0] += lerp_cell(rowp, ts, ixp, fxp, fyp);  // q0 (+, +)
-                    sm[1] += lerp_cell(rowp, ts, ixm, fxm, fyp);  // q1 (-, +)
-                    sm[2] += lerp_cell(rowm, ts, ixm, fxm, fym);  // q2 (-, -)
-                    sm[3] += lerp_cell(rowm, ts, ixp, fxp, fym);  // q3 (+, -)
+                    const float4 d = dirs[stride * a];
+                    const float2 X = __fadd2_rn(cxx, __fmul2_rn(make_float2(d.x, d.y), rr));  // (x+, x-)
+                    const float2 Y = __fadd2_rn(cyy, __fmul2_rn(make_float2(d.z, d.w), rr));  // (y+, y-)
+                    const float2 TX = __fadd2_rz(X, K), TY = __fadd2_rz(Y, K);
+                    const float2 FX = __ffma2_rn(__fadd2_rn(TX, nK), m1, X);  // X - trunc(X)
+                    const float2 FY = __ffma2_rn(__fadd2_rn(TY, nK), m1, Y);
+                    const int ixp = __float_as_int(TX.x) - 0x4B000000, ixm = __float_as_int(TX.y) - 0x4B000000;
+                    const float *rowp = img + (__float_as_int(TY.x) - 0x4B000000) * ts;
+                    const float *rowm = img + (__float_as_int(TY.y) - 0x4B000000) * ts;
+                    s02 = __fadd2_rn(s02, lerp_cell2(rowp + ixp, rowm + ixm, ts, FX, FY));
+                    s31 = __fadd2_rn(s31, lerp_cell2(rowm + ixp, rowp + ixm, ts, FX, make_float2(FY.y, FY.x)));
                 }
+                sm[0] = s02.x;
+                sm[1] = s31.y;
+                sm[2] = s02.y;
+                sm[3] = s31.x;
                 const int c = sub < nang ? (nang - sub + S - 1) >> lS : 0;
                 cnt[0] = cnt[1] = cnt[2] = cnt[3] = c;
             } else {
@@ -625,8 +646,8 @@ __device__ __forceinline__ void qi_profiles_sym(const float *img, int W, int H, 
                 // -1 < y < H-1, and its cell starts at the truncation of max(x, 0)
                 const float xhi = (float)(W - 1), yhi = (float)(H - 1);
                 for (int a = sub; a < nang; a += S) {
-                    const float2 d = dirs[stride * a];
-                    const float dx = __fmul_rn(d.x, r), dy = __fmul_rn(d.y, r);
+                    const float4 d = dirs[stride * a];
+                    const float dx = __fmul_rn(d.x, r), dy = __fmul_rn(d.z, r);
                     const float xp = __fadd_rn(cx, dx), xm = __fadd_rn(cx, -dx);
                     const float yp = __fadd_rn(cy, dy), ym = __fadd_rn(cy, -dy);
                     const bool vxp = xp > -1.0f && xp < xhi, vxm = xm > -1.0f && xm < xhi;

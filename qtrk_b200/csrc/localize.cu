@@ -29,7 +29,8 @@ __device__ const float kZLUTWeights[7] = {0.15f, 0.5f, 0.85f, 1.0f, 0.85f, 0.5f,
 
 struct SmemView {
     float *img, *misc;
-    float2 *qdirs, *tw, *zdirs;
+    float4 *qdirs;  // QI quadrant directions as (d.x, d.x, d.y, d.y)
+    float2 *tw, *zdirs;
     float *qrw;  // QI radial weights (qi_nr floats after the twiddles)
     uint8_t *work;
     double *red;
@@ -43,8 +44,8 @@ __device__ __forceinline__ SmemView smem_view(uint8_t *smem, const TrackParams &
     v.red = reinterpret_cast<double *>(smem + P.sm_red);
     v.work = smem + P.sm_work;
     float2 *tab = reinterpret_cast<float2 *>(smem + P.sm_tables);
-    v.qdirs = tab;
-    v.tw = tab + P.qi_angpq;  // L/2 = qi_nr twiddles
+    v.qdirs = reinterpret_cast<float4 *>(tab);
+    v.tw = tab + 2 * P.qi_angpq;  // L/2 = qi_nr twiddles
     v.qrw = reinterpret_cast<float *>(v.tw + P.qi_nr);
     v.zdirs = tab;            // loaded over the QI tables once QI is done (load_z_tables)
     return v;
@@ -57,7 +58,10 @@ __device__ __forceinline__ void load_qi_tables(const SmemView &s, const TrackPar
     const float2 *qd = static_cast<const float2 *>(P.qi_dirs);
     const float2 *tw = static_cast<const float2 *>(P.qi_twiddles);
     if (qd)
-        for (int i = threadIdx.x; i < P.qi_angpq; i += blockDim.x) s.qdirs[i] = qd[i];
+        for (int i = threadIdx.x; i < P.qi_angpq; i += blockDim.x) {
+            const float2 d = qd[i];
+            s.qdirs[i] = make_float4(d.x, d.x, d.y, d.y);
+        }
     if (tw)
         for (int i = threadIdx.x; i < P.qi_nr; i += blockDim.x) s.tw[i] = tw[i];
     if (P.qi_rweights)
@@ -433,7 +437,7 @@ void plan_smem(TrackParams &P)
     const int nr = P.qi_nr > 0 ? P.qi_nr : 1, L = 2 * nr;
     P.sm_img = 0;
     P.sm_tables = align16(W * H * 4);
-    const int qi_tables = (P.qi_angpq + nr) * 8 + nr * 4, z_tables = P.z_angsteps * 8;
+    const int qi_tables = P.qi_angpq * 16 + nr * 8 + nr * 4, z_tables = P.z_angsteps * 8;
     P.sm_work = P.sm_tables + align16(qi_tables > z_tables ? qi_tables : z_tables);
     // [ ac | A ] (L complex each) + 2 KB of subset partials when the QI directions are split over warps
     const int qi_work = 2 * L * 8 + (nr < kBlockThreads / 4 ? 2048 : 0);
