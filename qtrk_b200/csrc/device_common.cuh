@@ -124,6 +124,19 @@ __device__ __forceinline__ float2 lerp_cell2(const float *p, const float *q, int
     return __ffma2_rn(__ffma2_rn(v0, m1, v1), fy, v0);
 }
 
+// bilinear_inside for two samples at (X.x, Y.x) and (X.y, Y.y) with packed FP32x2 arithmetic
+// (each component rounded as bilinear_inside rounds it).
+__device__ __forceinline__ float2 bilinear_inside2(const float *img, int ts, float2 X, float2 Y)
+{
+    const float2 K = make_float2(8388608.0f, 8388608.0f), nK = make_float2(-8388608.0f, -8388608.0f);
+    const float2 m1 = make_float2(-1.0f, -1.0f);
+    const float2 TX = __fadd2_rz(X, K), TY = __fadd2_rz(Y, K);
+    const float2 FX = __ffma2_rn(__fadd2_rn(TX, nK), m1, X), FY = __ffma2_rn(__fadd2_rn(TY, nK), m1, Y);
+    const float *p = img + ((__float_as_int(TY.x) - 0x4B000000) * ts + (__float_as_int(TX.x) - 0x4B000000));
+    const float *q = img + ((__float_as_int(TY.y) - 0x4B000000) * ts + (__float_as_int(TX.y) - 0x4B000000));
+    return lerp_cell2(p, q, ts, FX, FY);
+}
+
 // True when every point cx + a*r, cy + b*r with |a|, |b| <= 1 (any sample of a circle of radius
 // r around (cx, cy)) lies strictly inside (0, w-1) x (0, h-1), rounding of the sample
 // coordinates included (margin 1e-3 px, far above one ulp of the coordinates).
@@ -858,11 +871,15 @@ __device__ inline void qi_autoconv_direct_filled(int nr, const float2 *A, float2
 // are in bounds; then NormalizeRadialProfile (utils.cpp:230-261) when asked.
 // -------------------------------------------------------------------------------------
 __device__ __forceinline__ void radial_profile(const float *img, int W, int H, int ts, float cx, float cy, float mean, int nb, int nang,
-                               float minr, float rstep, const float2 *dirs, float *prof, bool normalize,
+                               float minr, float rstep, const float4 *dirs, float *prof, bool normalize,
                                double *red)
 {
+    // dirs[j] = (d_j.x, d_{j+h}.x, d_j.y, d_{j+h}.y) for j < h = nang/2, and d_{nang-1} alone in
+    // dirs[h] when nang is odd: each lane takes pairs j = sub, sub + tpb, ... (two samples per
+    // step, packed FP32x2) and lane 0 of each bin the unpaired direction.
     const int tpb = lanes_per_bin(nb), ltpb = ilog2_pow2(tpb);
-    const int total = nb * tpb;
+    const int total = nb * tpb, h = nang >> 1;
+    const bool odd = (nang & 1) != 0;
     for (int base = 0; base < total; base += blockDim.x) {
         const int t = base + threadIdx.x;
         const int bin = t >> ltpb, sub = t & (tpb - 1);
@@ -872,46 +889,66 @@ __device__ __forceinline__ void radial_profile(const float *img, int W, int H, i
         // one path per warp (see qi_profiles_sym)
         const bool inside = __all_sync(0xffffffffu, bin >= nb || circle_inside(cx, cy, fabsf(r), W, H));
         if (bin < nb && inside) {
-            // This lane's directions are sub, sub + tpb, ...: nl of them, taken in groups of 8
-            // summed in FP32 and folded into an FP64 total (the reference adds every sample in
-            // FP64; 8-sample FP32 groups stay within ~1e-7 of it). Whole groups run without
-            // per-sample checks, then the remainder.
-            const int nl = sub < nang ? (nang - sub + tpb - 1) >> ltpb : 0;
-            const float2 *dl = dirs + sub;
+            // Whole groups of 4 pairs (8 samples) are summed in FP32 and folded into an FP64
+            // total (the reference adds every sample in FP64; 8-sample FP32 groups stay within
+            // ~1e-7 of it), then the remaining pairs, then the unpaired direction.
+            const float2 rr = make_float2(r, r), cxx = make_float2(cx, cx), cyy = make_float2(cy, cy);
+            const int np = sub < h ? (h - sub + tpb - 1) >> ltpb : 0;
+            const float4 *dl = dirs + sub;
             int k = 0;
-            for (; k + 8 <= nl; k += 8) {
-                float part = 0.0f;
+            for (; k + 4 <= np; k += 4) {
+                float2 part = make_float2(0.0f, 0.0f);
 #pragma unroll
-                for (int u = 0; u < 8; u++) {
-                    const float2 d = dl[(k + u) << ltpb];
-                    part += bilinear_inside(img, ts, cx + d.x * r, cy + d.y * r);
+                for (int u = 0; u < 4; u++) {
+                    const float4 d = dl[(k + u) << ltpb];
+                    part = __fadd2_rn(part, bilinear_inside2(img, ts, __ffma2_rn(make_float2(d.x, d.y), rr, cxx),
+                                                             __ffma2_rn(make_float2(d.z, d.w), rr, cyy)));
                 }
-                sum += (double)part;
+                sum += (double)(part.x + part.y);
             }
-            if (k < nl) {
-                float part = 0.0f;
-                for (; k < nl; k++) {
-                    const float2 d = dl[k << ltpb];
-                    part += bilinear_inside(img, ts, cx + d.x * r, cy + d.y * r);
+            if (k < np) {
+                float2 part = make_float2(0.0f, 0.0f);
+                for (; k < np; k++) {
+                    const float4 d = dl[k << ltpb];
+                    part = __fadd2_rn(part, bilinear_inside2(img, ts, __ffma2_rn(make_float2(d.x, d.y), rr, cxx),
+                                                             __ffma2_rn(make_float2(d.z, d.w), rr, cyy)));
                 }
-                sum += (double)part;
+                sum += (double)(part.x + part.y);
             }
-            cnt = nl;
+            cnt = 2 * np;
+            if (odd && sub == 0) {
+                const float4 d = dirs[h];
+                sum += (double)bilinear_inside(img, ts, cx + d.x * r, cy + d.z * r);
+                cnt++;
+            }
         } else if (bin < nb) {
-            for (int a0 = sub; a0 < nang; a0 += 8 * tpb) {
+            // every sample checked; FP32 partials of up to 8 samples folded into FP64
+            for (int j0 = sub; j0 < h; j0 += 4 * tpb) {
                 float part = 0.0f;
-                {
 #pragma unroll
-                    for (int k = 0; k < 8; k++) {
-                        const int a = a0 + k * tpb;
-                        float v;
-                        if (a < nang && bilinear(img, W, H, ts, cx + dirs[a].x * r, cy + dirs[a].y * r, v)) {
-                            part += v;
-                            cnt++;
-                        }
+                for (int u = 0; u < 4; u++) {
+                    const int j = j0 + u * tpb;
+                    if (j >= h) break;
+                    const float4 d = dirs[j];
+                    float v;
+                    if (bilinear(img, W, H, ts, cx + d.x * r, cy + d.z * r, v)) {
+                        part += v;
+                        cnt++;
+                    }
+                    if (bilinear(img, W, H, ts, cx + d.y * r, cy + d.w * r, v)) {
+                        part += v;
+                        cnt++;
                     }
                 }
                 sum += (double)part;
+            }
+            if (odd && sub == 0) {
+                const float4 d = dirs[h];
+                float v;
+                if (bilinear(img, W, H, ts, cx + d.x * r, cy + d.z * r, v)) {
+                    sum += (double)v;
+                    cnt++;
+                }
             }
         }
         for (int o = tpb >> 1; o > 0; o >>= 1) {

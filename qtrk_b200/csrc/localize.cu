@@ -30,7 +30,8 @@ __device__ const float kZLUTWeights[7] = {0.15f, 0.5f, 0.85f, 1.0f, 0.85f, 0.5f,
 struct SmemView {
     float *img, *misc;
     float4 *qdirs;  // QI quadrant directions as (d.x, d.x, d.y, d.y)
-    float2 *tw, *zdirs;
+    float2 *tw;
+    float4 *zdirs;  // full-circle directions in pairs (j, j + n/2), see load_z_tables
     float *qrw;  // QI radial weights (qi_nr floats after the twiddles)
     uint8_t *work;
     double *red;
@@ -47,7 +48,7 @@ __device__ __forceinline__ SmemView smem_view(uint8_t *smem, const TrackParams &
     v.qdirs = reinterpret_cast<float4 *>(tab);
     v.tw = tab + 2 * P.qi_angpq;  // L/2 = qi_nr twiddles
     v.qrw = reinterpret_cast<float *>(v.tw + P.qi_nr);
-    v.zdirs = tab;            // loaded over the QI tables once QI is done (load_z_tables)
+    v.zdirs = reinterpret_cast<float4 *>(tab);  // loaded over the QI tables once QI is done
     return v;
 }
 
@@ -74,7 +75,82 @@ __device__ __forceinline__ void load_z_tables(const SmemView &s, const TrackPara
 {
     const float2 *zd = static_cast<const float2 *>(P.z_dirs);
     if (zd)
-        for (int i = threadIdx.x; i < P.z_angsteps; i += blockDim.x) s.zdirs[i] = zd[i];
+        for (int j = threadIdx.x; j < (P.z_angsteps + 1) >> 1; j += blockDim.x) {
+            // entry j = (d_j.x, d_{j+h}.x, d_j.y, d_{j+h}.y), h = n/2 rounded down; with n odd the
+            // last entry holds d_{n-1} alone (zeros in the second place, never read)
+            const int h = P.z_angsteps >> 1;
+            const float2 a = zd[j < h ? j : P.z_angsteps - 1];
+            const float2 b = j < h ? zd[j + h] : make_float2(0.0f, 0.0f);
+            s.zdirs[j] = make_float4(a.x, b.x, a.y, b.y);
+        }
+}
+
+// The QI position update from the two autoconvolutions (cpu_tracker.cpp:345-357, 400-410):
+// ComputeMaxInterp over autoconv[x] = ac[(x + nr) mod L] for X (.x) and Y (.y), by one warp: a
+// two-axis argmax over the warp (first index of the maximum, as warp_argmax), then the 7-point
+// fits of both axes side by side (even lanes X, odd lanes Y). Lanes 0 and 1 write the new x and y
+// to misc[0] and misc[1]. Runs on the warp that made ac, right after it, with no CTA barrier.
+__device__ __forceinline__ void qi_fit_xy(const float2 *ac, int nr, float cx, float cy, float rstep, float *misc)
+{
+    const int lane = threadIdx.x & 31, L = 2 * nr;
+    float bx = 0.0f, by = 0.0f;
+    int ix = -1, iy = -1;
+    for (int x = lane; x < L; x += 32) {
+        int n = x + nr;
+        if (n >= L) n -= L;
+        const float2 v = ac[n];
+        if (v.x == v.x && (ix < 0 || v.x > bx)) {
+            bx = v.x;
+            ix = x;
+        }
+        if (v.y == v.y && (iy < 0 || v.y > by)) {
+            by = v.y;
+            iy = x;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float ox = __shfl_xor_sync(0xffffffffu, bx, o), oy = __shfl_xor_sync(0xffffffffu, by, o);
+        const int oix = __shfl_xor_sync(0xffffffffu, ix, o), oiy = __shfl_xor_sync(0xffffffffu, iy, o);
+        if (oix >= 0 && (ix < 0 || ox > bx || (ox == bx && oix < ix))) {
+            bx = ox;
+            ix = oix;
+        }
+        if (oiy >= 0 && (iy < 0 || oy > by || (oy == by && oiy < iy))) {
+            by = oy;
+            iy = oiy;
+        }
+    }
+    ix = ix < 0 ? 0 : ix;
+    iy = iy < 0 ? 0 : iy;
+    const bool yaxis = (lane & 1) != 0;
+    float m;
+    if (ix >= 3 && ix + 4 <= L && iy >= 3 && iy + 4 <= L) {  // both windows inside: per-lane fits
+        auto at = [&](int x) {
+            int n = x + nr;
+            if (n >= L) n -= L;
+            return yaxis ? ac[n].y : ac[n].x;
+        };
+        m = max_interp7_sym(at, L, yaxis ? iy : ix, kQIWeights);
+    } else {  // a clipped window takes the warp-wide fit, one axis after the other
+        auto atx = [&](int x) {
+            int n = x + nr;
+            if (n >= L) n -= L;
+            return ac[n].x;
+        };
+        auto aty = [&](int x) {
+            int n = x + nr;
+            if (n >= L) n -= L;
+            return ac[n].y;
+        };
+        const float mx = max_interp7_sym(atx, L, ix, kQIWeights);
+        const float my = max_interp7_sym(aty, L, iy, kQIWeights);
+        m = yaxis ? my : mx;
+    }
+    if (lane < 2) {
+        const float off = (m - (float)nr) * (3.14159265359f / 4);
+        misc[lane] = (yaxis ? cy : cx) + off * rstep;
+    }
 }
 
 // CPUTracker::ComputeQI, cpu_tracker.cpp:285-360. All threads call; returns the position and the
@@ -95,31 +171,19 @@ __device__ void qi_localize(const SmemView &s, const TrackParams &P, float mean,
                         s.qdirs, rweights, part, A, pow2 ? ilog2_pow2(L) : -1);
         __syncthreads();
         if (pow2) {
-            if (threadIdx.x < 32) qi_autoconv_fft_filled(nr, A, ac, s.tw);
+            if (threadIdx.x < 32) {  // transform and fits on warp 0, the others wait at the next barrier
+                qi_autoconv_fft_filled(nr, A, ac, s.tw);
+                qi_fit_xy(ac, nr, cx, cy, rstep, s.misc);
+            }
         } else {
             qi_autoconv_direct_filled(nr, A, ac);
-        }
-        if (pow2) __syncthreads();  // the FFT ran on warp 0 only
-        if (threadIdx.x < 64) {
-            // warp 0 fits the X profile, warp 1 the Y profile, concurrently.
-            // autoconv[x] = out[(x + nr) mod L] (cpu_tracker.cpp:400-402)
-            const bool yaxis = threadIdx.x >= 32;
-            auto at = [&](int x) {
-                int n = x + nr;
-                if (n >= L) n -= L;
-                return yaxis ? ac[n].y : ac[n].x;
-            };
-            const int im = warp_argmax(at, L);
-            const float m = max_interp7_sym(at, L, im, kQIWeights);
-            if ((threadIdx.x & 31) == 0) {
-                const float off = (m - (float)nr) * (3.14159265359f / 4);
-                s.misc[yaxis ? 1 : 0] = (yaxis ? cy : cx) + off * rstep;
-            }
+            if (threadIdx.x < 32) qi_fit_xy(ac, nr, cx, cy, rstep, s.misc);
         }
         __syncthreads();
+        // misc[0..1] is written again only after the next iteration's first barrier, which every
+        // thread reaches after these reads
         cx = s.misc[0];
         cy = s.misc[1];
-        __syncthreads();
     }
 }
 
@@ -229,9 +293,8 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
                       (uint32_t)(bpp * n), mbar);
         }
     }
-    uint32_t job[6];
-    read_job(jobs, roi, job);
-    const int bead = (int)job[2];
+    // the job's words are read again for the result (no registers held through QI and Z)
+    const int bead = jobs ? (int)reinterpret_cast<const uint32_t *>(jobs)[(size_t)roi * 6 + 2] : 0;
     load_qi_tables(s, P);
     float2 part;
     if constexpr (kStaged) {
@@ -257,7 +320,11 @@ __global__ void __launch_bounds__(kBlockThreads, kMinBlocks)
         bhit = check_boundaries(x, y, P.z_maxr, W, H);
         z = z_localize(s, P, com.mean, x, y, bead, roi);
     }
-    if (threadIdx.x == 0) write_result(results, roi, job, x, y, z, comx, comy, bhit ? 1u : 0u, com.mean);
+    if (threadIdx.x == 0) {
+        uint32_t job[6];
+        read_job(jobs, roi, job);
+        write_result(results, roi, job, x, y, z, comx, comy, bhit ? 1u : 0u, com.mean);
+    }
 }
 
 // 2D Gaussian MLE (+ Z) for ROIs above 32x32 or with QI/Z bits: one CTA per ROI on a plain tile.
@@ -437,7 +504,7 @@ void plan_smem(TrackParams &P)
     const int nr = P.qi_nr > 0 ? P.qi_nr : 1, L = 2 * nr;
     P.sm_img = 0;
     P.sm_tables = align16(W * H * 4);
-    const int qi_tables = P.qi_angpq * 16 + nr * 8 + nr * 4, z_tables = P.z_angsteps * 8;
+    const int qi_tables = P.qi_angpq * 16 + nr * 8 + nr * 4, z_tables = ((P.z_angsteps + 1) >> 1) * 16;
     P.sm_work = P.sm_tables + align16(qi_tables > z_tables ? qi_tables : z_tables);
     // [ ac | A ] (L complex each) + 2 KB of subset partials when the QI directions are split over warps
     const int qi_work = 2 * L * 8 + (nr < kBlockThreads / 4 ? 2048 : 0);
