@@ -377,6 +377,10 @@ __device__ inline float2 load_roi(const G &g, float *img, const uint8_t *src, in
     } else {
         // Rows at a pitch (a ROI inside a frame): warps over rows, lanes along a row, so loads
         // are coalesced along the row and the stores are conflict-free.
+        // With whole 4-pixel chunks the partial sums are then taken from the tile in the chunk
+        // order of the contiguous loads, so that a ROI gives bit-identical results whichever way
+        // it arrived (FP32 partial sums depend on which pixels each thread adds).
+        const bool chunked = !(n & 3) && !(reinterpret_cast<uintptr_t>(img) & 15);
         const int lane = g.rank() & 31, wg = g.rank() >> 5, nwg = g.size() >> 5;
         for (int y = wg; y < H; y += nwg) {
             const uint8_t *row = src + (size_t)y * pitch;
@@ -391,9 +395,26 @@ __device__ inline float2 load_roi(const G &g, float *img, const uint8_t *src, in
                     v = reinterpret_cast<const float *>(row)[x];
                 const int i = y * W + x;
                 v = finish_pixel(v, i, P, off, gain);
-                s += v;
-                s2 = fmaf(v, v, s2);
+                if (!chunked) {
+                    s += v;
+                    s2 = fmaf(v, v, s2);
+                }
                 img[i] = v;
+            }
+        }
+        if (chunked) {
+            g.sync();
+            const float4 *img4 = reinterpret_cast<const float4 *>(img);
+            for (int c = g.rank(); c < (n >> 2); c += g.size()) {
+                const float4 f = img4[c];
+                s += f.x;
+                s2 = fmaf(f.x, f.x, s2);
+                s += f.y;
+                s2 = fmaf(f.y, f.y, s2);
+                s += f.z;
+                s2 = fmaf(f.z, f.z, s2);
+                s += f.w;
+                s2 = fmaf(f.w, f.w, s2);
             }
         }
     }

@@ -260,7 +260,7 @@ __device__ __forceinline__ void write_result(LocalizationResult *results, int i,
     o[12] = __float_as_uint(mean);
 }
 
-constexpr int kMinBlocks = 4;  // CTAs per SM the QI and Gaussian kernels are compiled for (64 registers)
+constexpr int kMinBlocks = 5;  // CTAs per SM the QI and Gaussian kernels are compiled for (<= 96 registers)
 
 constexpr uint32_t kStageWaitLimit = 1u << 22;  // mbarrier polls before a staged copy counts as lost
 

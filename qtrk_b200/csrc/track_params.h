@@ -17,7 +17,10 @@ struct float2_host { float x, y; };
 namespace qtrk {
 
 constexpr int kMaxQIIterations = 32;
-constexpr int kBlockThreads = 256;  // threads per localization CTA (one ROI per CTA)
+// Threads per localization CTA (one ROI per CTA). Four warps: with a 100x100 float tile (45 KB of
+// shared memory) five CTAs fit on an SM, and the one-warp sections of each ROI (QI transform and
+// fits, Z fit) leave three warps idle rather than seven.
+constexpr int kBlockThreads = 128;
 
 // Mode bits (cputrack/qtrk_c_api.h:5-20 plus the library's extension bits).
 enum : int {
