@@ -652,8 +652,9 @@ COM_BYTES_PER_ROI = 100 * 100 * 2 + 52  # pixels in, result out (no job records:
 
 
 def com_only_bench(dev, settings, d_rois, n: int, steps: int, warmup: int, sm_mhz: float | None = None) -> dict:
-    """LT_OnlyCOM on the headline stack (n ROIs of 100x100 u16 resident in HBM): the register-held
-    streaming COM kernel, one launch per step, with its roofline against the measured HBM copy rate."""
+    """LT_OnlyCOM on the headline stack (n ROIs of 100x100 u16 resident in HBM): the warp-per-ROI
+    COM kernel (bulk-copied ROI buffers, shuffle reductions), one launch per step, with its roofline
+    against the measured HBM copy rate."""
     import torch
 
     from qtrk_b200 import abi
@@ -678,7 +679,7 @@ def com_only_bench(dev, settings, d_rois, n: int, steps: int, warmup: int, sm_mh
             "rois_per_s": n / (ms / 1e3), "ms_per_launch": ms, "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "qtrk::com_stream_kernel<1, 4>", "kernel_ms": ms,
+                         "kernel": "qtrk::com_warp_kernel<1>", "kernel_ms": ms,
                          "bytes_per_roi": COM_BYTES_PER_ROI, **roof_extra}}
 
 

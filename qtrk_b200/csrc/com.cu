@@ -126,45 +126,90 @@ __device__ __forceinline__ ChunkWalk chunk_walk(int t, int T, int ppc, int W)
     return w;
 }
 
-// Pass 2 of ComputeMeanAndCOM on this thread's chunks (see the chunk moments above): returns the
-// FP32 partial sums of v', x v' and y v'. kThr: a background threshold is set (v' = max(0, |v -
+// The moments of one chunk at walk position w (see the chunk moments above), added to the FP32
+// sums q0 (v'), qx (x v') and qy (y v'). kThr: a background threshold is set (v' = max(0, |v -
 // mean| - thr)); without one v' = |v - mean| exactly.
+template <int PDT, bool kThr>
+__device__ __forceinline__ void chunk_moments(const float (&v)[ChunkPixels<PDT>::n], const ChunkWalk &w, float fW,
+                                              float mean, float thr, float &q0, float &qx, float &qy)
+{
+    constexpr int ppc = ChunkPixels<PDT>::n;
+    float a[ppc];
+    float S = 0.0f, Sj = 0.0f;
+#pragma unroll
+    for (int j = 0; j < ppc; j++) {
+        a[j] = kThr ? fmaxf(0.0f, fabsf(v[j] - mean) - thr) : fabsf(v[j] - mean);
+        S += a[j];
+        if (j > 0) Sj = fmaf((float)j, a[j], Sj);
+    }
+    const float split = fW - w.fx;  // first j on the next row
+    float Sw = 0.0f;
+    if (split < (float)ppc) {
+#pragma unroll
+        for (int j = 0; j < ppc; j++)
+            if ((float)j >= split) Sw += a[j];
+    }
+    q0 += S;
+    qx += fmaf(w.fx, S, Sj) - fW * Sw;
+    qy += fmaf(w.fy, S, Sw);
+}
+
+// chunk_moments for a chunk of 8 u16 pixels without a background threshold, on packed FP32x2
+// pairs: v - mean is formed per pixel exactly as the scalar form forms it (the pixel is exact in
+// FP32), and the sums S and Sj run as two interleaved halves added at the end.
+__device__ __forceinline__ void chunk_moments_u16(const uint4 &q, const ChunkWalk &w, float fW, float mean, float &q0,
+                                                  float &qx, float &qy)
+{
+    const float2 nK = make_float2(-8388608.0f, -8388608.0f), nm = make_float2(-mean, -mean);
+    const uint32_t wd[4] = {q.x, q.y, q.z, q.w};
+    float2 a[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const float2 x = make_float2(__uint_as_float(__byte_perm(wd[k], 0x4B000000u, 0x7410u)),
+                                     __uint_as_float(__byte_perm(wd[k], 0x4B000000u, 0x7432u)));
+        const float2 d = __fadd2_rn(__fadd2_rn(x, nK), nm);
+        a[k] = make_float2(fabsf(d.x), fabsf(d.y));
+    }
+    const float2 S2 = __fadd2_rn(__fadd2_rn(a[0], a[1]), __fadd2_rn(a[2], a[3]));
+    float2 J2 = __fmul2_rn(a[0], make_float2(0.0f, 1.0f));
+    J2 = __ffma2_rn(a[1], make_float2(2.0f, 3.0f), J2);
+    J2 = __ffma2_rn(a[2], make_float2(4.0f, 5.0f), J2);
+    J2 = __ffma2_rn(a[3], make_float2(6.0f, 7.0f), J2);
+    const float S = S2.x + S2.y, Sj = J2.x + J2.y;
+    const float split = fW - w.fx;  // first j on the next row
+    float Sw = 0.0f;
+    if (split < 8.0f) {
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+            if ((float)j >= split) Sw += (j & 1) ? a[j >> 1].y : a[j >> 1].x;
+    }
+    q0 += S;
+    qx += fmaf(w.fx, S, Sj) - fW * Sw;
+    qy += fmaf(w.fy, S, Sw);
+}
+
+__device__ __forceinline__ void walk_step(ChunkWalk &w, float fW)
+{
+    w.fx += w.fdx;
+    w.fy += w.fdy;
+    if (w.fx >= fW) {
+        w.fx -= fW;
+        w.fy += 1.0f;
+    }
+}
+
+// Pass 2 of ComputeMeanAndCOM on this thread's chunks t, t + T, ... (K of them, those below
+// nchunks): the FP32 partial sums of v', x v' and y v'.
 template <int PDT, int K, bool kThr>
 __device__ __forceinline__ float3 com_moments(const float (&v)[K][ChunkPixels<PDT>::n], ChunkWalk w, int t, int T,
                                               int nchunks, int W, float mean, float thr)
 {
-    constexpr int ppc = ChunkPixels<PDT>::n;
     const float fW = (float)W;
     float q0 = 0.0f, qx = 0.0f, qy = 0.0f;
 #pragma unroll
     for (int k = 0; k < K; k++) {
-        const int c = t + k * T;
-        if (c < nchunks) {
-            float a[ppc];
-            float S = 0.0f, Sj = 0.0f;
-#pragma unroll
-            for (int j = 0; j < ppc; j++) {
-                a[j] = kThr ? fmaxf(0.0f, fabsf(v[k][j] - mean) - thr) : fabsf(v[k][j] - mean);
-                S += a[j];
-                if (j > 0) Sj = fmaf((float)j, a[j], Sj);
-            }
-            const float split = fW - w.fx;  // first j on the next row
-            float Sw = 0.0f;
-            if (split < (float)ppc) {
-#pragma unroll
-                for (int j = 0; j < ppc; j++)
-                    if ((float)j >= split) Sw += a[j];
-            }
-            q0 += S;
-            qx += fmaf(w.fx, S, Sj) - fW * Sw;
-            qy += fmaf(w.fy, S, Sw);
-        }
-        w.fx += w.fdx;
-        w.fy += w.fdy;
-        if (w.fx >= fW) {
-            w.fx -= fW;
-            w.fy += 1.0f;
-        }
+        if (t + k * T < nchunks) chunk_moments<PDT, kThr>(v[k], w, fW, mean, thr, q0, qx, qy);
+        walk_step(w, fW);
     }
     return make_float3(q0, qx, qy);
 }
@@ -340,6 +385,230 @@ __global__ void __launch_bounds__(kComMaxThreads) com_stream_kernel(TrackParams 
 
 namespace {
 
+constexpr int kComWarpGroup = 32;  // pixels per FP32 partial sum before it is folded into FP64
+constexpr int kComMaxGroups = 15;  // ROI buffers per CTA of the warp-group form (named barriers 1..15)
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// The first four pixels of a chunk set to zero (LT_ClearFirstFourPixels, QueuedCPUTracker.cpp:280-282).
+template <int PDT>
+__device__ __forceinline__ void clear_first_four(uint4 &q)
+{
+    if (PDT == 0) {
+        q.x = 0u;
+    } else if (PDT == 1) {
+        q.x = 0u;
+        q.y = 0u;
+    } else {
+        q = make_uint4(0u, 0u, 0u, 0u);
+    }
+}
+
+}  // namespace
+
+// Named barrier over the `n` threads of one warp group (id 1..15; 0 is __syncthreads).
+__device__ __forceinline__ void group_sync(int id, int n)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+// The same barrier, returning whether `v` holds in every thread of the group.
+__device__ __forceinline__ bool group_all(bool v, int id, int n)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id), "r"(n)
+        : "memory");
+    return r != 0;
+}
+
+// The warp-group form: a group of `wg` warps (1, 2 or 4) per ROI and one shared-memory buffer
+// (buf_stride bytes) per group, with no CTA-wide barrier. A bulk copy (cp.async.bulk, completion
+// on the group's mbarrier) fills the buffer with the group's ROI; the group runs both passes of
+// ComputeMeanAndCOM over it (16-byte shared loads; thread t of the group on chunks t, t + 32 wg,
+// ...), reduces with shuffles and then across its warps through a named barrier, writes the
+// result, and only then starts the copy of its next ROI into the same buffer. The other groups of
+// the SM keep the copy engine busy meanwhile, so each group's copy latency is hidden by its
+// neighbours' work; splitting a ROI over several warps puts more warps on the SM than there are
+// buffers. Pass 1 of integer pixels without a background threshold is an exact integer sum
+// (dp2a / dp4a); otherwise FP32 partial sums over 32 pixels are folded into FP64, as in the CTA
+// form. Every warp of a group adds the group's partials in the same order, so all hold the same
+// totals.
+template <int PDT>
+__global__ void __launch_bounds__(1024, 1) com_warp_kernel(TrackParams P, const uint8_t *__restrict__ pixels,
+                                                            int64_t roi_stride, const LocalizationJob *__restrict__ jobs,
+                                                            int count, LocalizationResult *__restrict__ results,
+                                                            int buf_stride, int wg)
+{
+    constexpr int ppc = ChunkPixels<PDT>::n, G = kComWarpGroup / ppc < 1 ? 1 : kComWarpGroup / ppc;
+    extern __shared__ __align__(128) uint8_t bufs[];
+    __shared__ uint64_t mbar[kComMaxGroups];
+    __shared__ double red1[kComMaxGroups][4][2];
+    __shared__ double red2[kComMaxGroups][4][3];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int grp = warp / wg, r = warp - grp * wg, ngrp = (blockDim.x >> 5) / wg;
+    const int T = 32 * wg, t = 32 * r + lane, bar_id = 1 + grp;
+    const bool leader = t == 0;
+    const int W = P.width, H = P.height, n = W * H, nchunks = n / ppc;
+    const uint32_t bytes = (uint32_t)(n * (16 / ppc));
+    uint8_t *gbuf = bufs + (size_t)grp * buf_stride;
+    const uint4 *buf = reinterpret_cast<const uint4 *>(gbuf);
+    uint64_t *mb = &mbar[grp];
+    const int stride = gridDim.x * ngrp;
+    int roi = blockIdx.x * ngrp + grp;
+    if (leader) {
+        mbar_init(mb);
+        if (roi < count) bulk_load(gbuf, pixels + (int64_t)roi * roi_stride, bytes, mb);
+    }
+    const bool clear4 = (P.mode & kLT_ClearFirstFourPixels) != 0;
+    const bool bg = P.com_bgcorrection != 0.0f;
+    const float invN = 1.0f / (float)n, fW = (float)W;
+    const ChunkWalk wk0 = chunk_walk(t, T, ppc, W);
+    for (uint32_t it = 0; roi < count; roi += stride, it++) {
+        // the leader waits for the copy; the barrier passes the completed copy (and, on the
+        // first ROI, the mbarrier's initialisation) to the group, and makes the outcome uniform
+        const bool ok = leader ? mbar_wait(mb, it & 1u, kComWaitLimit) : true;
+        if (!group_all(ok, bar_id, T)) {
+            // the copy did not complete: flag it, give it a last bounded wait (it writes into this
+            // CTA's shared memory) and stop the group
+            if (leader) {
+                if (P.err_flag) atomicOr(P.err_flag, 4u);
+                mbar_wait(mb, it & 1u, kComWaitLimit);
+            }
+            return;
+        }
+        // pass 1: sum (and sum of squares for a background threshold)
+        double m1[2] = {0.0, 0.0};
+        if (PDT != 2 && !bg) {
+            uint32_t si = 0u;  // exact below 2^20 pixels (u16)
+            for (int c = t; c < nchunks; c += T) {
+                uint4 q = buf[c];
+                if (clear4 && c == 0) clear_first_four<PDT>(q);
+                if (PDT == 0) {
+                    si = __dp4a(q.x, 0x01010101u, si);
+                    si = __dp4a(q.y, 0x01010101u, si);
+                    si = __dp4a(q.z, 0x01010101u, si);
+                    si = __dp4a(q.w, 0x01010101u, si);
+                } else {
+                    si = __dp2a_lo(q.x, 0x0101u, si);
+                    si = __dp2a_lo(q.y, 0x0101u, si);
+                    si = __dp2a_lo(q.z, 0x0101u, si);
+                    si = __dp2a_lo(q.w, 0x0101u, si);
+                }
+            }
+            m1[0] = (double)si;
+        } else {
+            for (int c0 = t; c0 < nchunks; c0 += T * G) {
+                float s = 0.0f, s2 = 0.0f;
+#pragma unroll
+                for (int g = 0; g < G; g++) {
+                    const int c = c0 + T * g;
+                    if (c < nchunks) {
+                        uint4 q = buf[c];
+                        if (clear4 && c == 0) clear_first_four<PDT>(q);
+                        float v[ppc];
+                        unpack<PDT>(q, v);
+#pragma unroll
+                        for (int j = 0; j < ppc; j++) {
+                            s += v[j];
+                            s2 = fmaf(v[j], v[j], s2);
+                        }
+                    }
+                }
+                m1[0] += (double)s;
+                m1[1] += (double)s2;
+            }
+        }
+        m1[0] = warp_sum(m1[0]);
+        if (bg) m1[1] = warp_sum(m1[1]);
+        if (lane == 0) {
+            red1[grp][r][0] = m1[0];
+            red1[grp][r][1] = m1[1];
+        }
+        group_sync(bar_id, T);
+        m1[0] = m1[1] = 0.0;
+        for (int k = 0; k < wg; k++) {
+            m1[0] += red1[grp][k][0];
+            m1[1] += red1[grp][k][1];
+        }
+        const float mean = (float)(m1[0] * (double)invN);
+        const float thr = bg ? P.com_bgcorrection * sqrtf((float)(m1[1] * (double)invN - (double)(mean * mean))) : 0.0f;
+        // pass 2: background-corrected moments
+        double m2[3] = {0.0, 0.0, 0.0};
+        ChunkWalk w = wk0;
+        for (int c0 = t; c0 < nchunks; c0 += T * G) {
+            float q0 = 0.0f, qx = 0.0f, qy = 0.0f;
+#pragma unroll
+            for (int g = 0; g < G; g++) {
+                const int c = c0 + T * g;
+                if (c < nchunks) {
+                    uint4 q = buf[c];
+                    if (clear4 && c == 0) clear_first_four<PDT>(q);
+                    if (PDT == 1 && !bg) {
+                        chunk_moments_u16(q, w, fW, mean, q0, qx, qy);
+                    } else {
+                        float v[ppc];
+                        unpack<PDT>(q, v);
+                        if (bg)
+                            chunk_moments<PDT, true>(v, w, fW, mean, thr, q0, qx, qy);
+                        else
+                            chunk_moments<PDT, false>(v, w, fW, mean, 0.0f, q0, qx, qy);
+                    }
+                }
+                walk_step(w, fW);
+            }
+            m2[0] += (double)q0;
+            m2[1] += (double)qx;
+            m2[2] += (double)qy;
+        }
+#pragma unroll
+        for (int k = 0; k < 3; k++) m2[k] = warp_sum(m2[k]);
+        if (lane == 0)
+#pragma unroll
+            for (int k = 0; k < 3; k++) red2[grp][r][k] = m2[k];
+        // after this barrier every thread of the group has finished reading the buffer, so the
+        // leader may start the next copy into it
+        group_sync(bar_id, T);
+        if (leader) {
+            double m[3] = {0.0, 0.0, 0.0};
+            for (int k = 0; k < wg; k++)
+#pragma unroll
+                for (int q = 0; q < 3; q++) m[q] += red2[grp][k][q];
+            com_result(results, roi, jobs, m, mean, W, H);
+            const int next = roi + stride;
+            if (next < count) bulk_load(gbuf, pixels + (int64_t)next * roi_stride, bytes, mb);
+        }
+    }
+}
+
+namespace {
+
+using ComWarpKernel = void (*)(TrackParams, const uint8_t *, int64_t, const LocalizationJob *, int,
+                               LocalizationResult *, int, int);
+
+// Buffers (ROIs in flight) and warps per ROI of the warp-group form: as many ROI buffers as fit in
+// 220 KB, at most 15, and the most warps per ROI (1, 2 or 4) that keep the CTA within 32 warps.
+// Fewer than 4 buffers (ROIs above 55 KB) leaves the ROI to the CTA forms.
+bool com_warp_plan(int64_t roi_bytes, int &groups, int &wg, int &stride)
+{
+    stride = (int)((roi_bytes + 127) & ~(int64_t)127);
+    groups = (int)((220 * 1024) / stride);
+    if (groups > kComMaxGroups) groups = kComMaxGroups;
+    wg = 4;
+    while (wg > 1 && groups * wg > 32) wg >>= 1;
+    return groups >= 4;
+}
+
 using ComKernel = void (*)(TrackParams, const uint8_t *, int64_t, const LocalizationJob *, int, LocalizationResult *);
 using ComStreamKernel = void (*)(TrackParams, const uint8_t *, int64_t, const LocalizationJob *, int,
                                  LocalizationResult *, int, int);
@@ -368,7 +637,9 @@ bool com_stream_plan(int64_t roi_bytes, int &stages, int &stride)
 }
 
 // CTAs of a streaming COM kernel that fit on the current device at once (cached per kernel,
-// device and shared-memory size); 0 when the query fails.
+// device and shared-memory size); 0 when the query fails. The kernel's dynamic shared-memory limit
+// is raised to the device's opt-in maximum (less its static shared memory) rather than to `smem`,
+// so that a later query for a smaller size cannot lower it under a size already cached.
 int com_stream_ctas(ComStreamKernel f, int threads, int smem)
 {
     struct Entry {
@@ -386,8 +657,12 @@ int com_stream_ctas(ComStreamKernel f, int threads, int smem)
             if (cache[i].f == f && cache[i].device == dev && cache[i].threads == threads && cache[i].smem == smem)
                 return cache[i].ctas;
     }
-    int per_sm = 0, sms = 0;
-    if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+    int per_sm = 0, sms = 0, optin = 0;
+    cudaFuncAttributes fa{};
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+        cudaFuncGetAttributes(&fa, f) != cudaSuccess || smem > optin - (int)fa.sharedSizeBytes ||
+        cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes) !=
+            cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, threads, smem) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
         cudaGetLastError();
@@ -464,6 +739,18 @@ cudaError_t launch_com(const TrackParams &P, const uint8_t *pixels, int64_t roi_
     if (!com_shape(P, T, K)) return cudaErrorInvalidValue;
     int stages = 0, stride = 0;
     const int64_t roi_bytes = (int64_t)P.width * P.height * bytes_per_pixel(P.pdt);
+    int groups = 0, wg = 1;
+    if (com_warp_plan(roi_bytes, groups, wg, stride)) {
+        ComWarpKernel f = P.pdt == 0 ? com_warp_kernel<0> : (P.pdt == 1 ? com_warp_kernel<1> : com_warp_kernel<2>);
+        const int smem = groups * stride, threads = groups * wg * 32;
+        const int ctas = com_stream_ctas(reinterpret_cast<ComStreamKernel>(f), threads, smem);
+        if (ctas > 0) {
+            const int need = (count + groups - 1) / groups;
+            f<<<need < ctas ? need : ctas, threads, smem, stream>>>(P, pixels, roi_stride, jobs, count, results, stride,
+                                                                   wg);
+            return cudaGetLastError();
+        }
+    }
     if (com_stream_plan(roi_bytes, stages, stride)) {
         ComStreamKernel f = P.pdt == 0 ? com_stream_at<0, 1>(K)
                                        : (P.pdt == 1 ? com_stream_at<1, 1>(K) : com_stream_at<2, 1>(K));
