@@ -553,6 +553,7 @@ def workloads_bench(dev, steps: int, warmup: int) -> dict:
         l0 = t.KernelLaunchCount()
         times = []
         for _ in range(2):  # the first build also allocates the instance's staging buffers
+            t.SetRadialZLUTSize(nbeads, planes)  # a zeroed LUT: BuildLUT adds to the LUT's rows
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             t.BeginLUT(abi.BUILDLUT_NORMALIZE)
@@ -561,12 +562,25 @@ def workloads_bench(dev, steps: int, warmup: int) -> dict:
             t.FinalizeLUT()
             lut = t.GetRadialZLUT()  # waits for the LUT
             times.append(time.perf_counter() - t0)
+        # the same build through QTrkB200BuildLUTAsync (the stack stays untouched until FinalizeLUT)
+        t.SetRadialZLUTSize(nbeads, planes)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        t.BeginLUT(abi.BUILDLUT_NORMALIZE)
+        for k in range(planes):
+            t.BuildLUTAsync(hs[k], k)
+        t.FinalizeLUT()
+        lut_async = t.GetRadialZLUT()
+        t_async = time.perf_counter() - t0
         d_plane = torch.empty_like(d_stack[0])
         copy_ms = _timed(stream, lambda: d_plane.copy_(host[0], non_blocking=True), 20, 3)
         out["buildlut_256x200_80x80_u16"] = {
             "workload": "BeginLUT / 200 x BuildLUT(256 ROIs 80x80 u16 from pinned host memory) / FinalizeLUT, "
                         "second build on the instance",
             "rois_per_s": nbeads * planes / times[1], "seconds": times[1], "first_build_seconds": times[0],
+            "async": {"call": "QTrkB200BuildLUTAsync (returns once the plane is queued; the caller keeps the stack "
+                              "until FinalizeLUT)", "rois_per_s": nbeads * planes / t_async, "seconds": t_async,
+                      "lut_equals_sync_build": bool(np.array_equal(lut_async, lut))},
             "copy_bound_rois_per_s": nbeads / (copy_ms / 1e3), "lut_shape": list(lut.shape)}
         cb = reference_cpu("buildlut", -1, settings=cs, stack=hs[:40])
         if cb is not None:

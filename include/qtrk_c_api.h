@@ -401,6 +401,14 @@ QTRK_API void QTRK_CALLCONV RMGetConfig(struct ResultManager *rm, ResultManagerC
 QTRK_API void QTRK_CALLCONV QTrkB200RMStoreResults(struct ResultManager *rm, const LocalizationResult *results,
                                                    int count, int roi_width, int roi_height);
 
+/* QTrkBuildLUT (qtrk_c_api.h:179) that does not wait for the plane's host-to-device copy: for a
+ * stack in pinned (page-locked) host memory the call returns once the copy and the plane's kernel
+ * are queued, so the copies of successive planes run back to back; the caller must keep `data`
+ * unchanged until QTrkFinalizeLUT returns. A pageable stack is staged before the call returns, as by
+ * QTrkBuildLUT. No counterpart in the reference (its BuildLUT is synchronous). */
+QTRK_API void QTRK_CALLCONV QTrkB200BuildLUTAsync(struct QueuedTracker *qtrk, void *data, int pitch,
+                                                  QTRK_PixelDataType_t pdt, int plane, vector2f *known_pos);
+
 /* Instance-level forms of the reference's handle-less calls (qtrk_c_api.h:152-158 act on every or
  * the latest instance), as the LabVIEW layer needs them. */
 QTRK_API void QTRK_CALLCONV QTrkB200SetPixelCalibrationFactors(struct QueuedTracker *qtrk, float offsetFactor,

@@ -218,6 +218,7 @@ B200_PROTOTYPES = {
     "QTrkB200SetZLUTBiasTable": (None, [_TRK, _P, C.c_int, C.c_int]),
     "QTrkB200ComputeZLUTBiasTable": (None, [_TRK, C.c_int, _P, C.c_int, C.c_int]),
     "QTrkB200LocalizeDevice": (C.c_int, [_TRK, _P, C.c_int, C.c_int64, C.c_int, C.c_int, _P, _P, _P]),
+    "QTrkB200BuildLUTAsync": (None, [_TRK, _P, C.c_int, C.c_int, C.c_int, _P]),
     "QTrkB200ZLUTCostGradient": (C.c_int, [_TRK, _P, C.c_int, C.c_int64, C.c_int, C.c_int, _P, _P, _P, _P, _P, _P]),
     "QTrkB200GaussianNLLGradient": (C.c_int, [_TRK, _P, C.c_int, C.c_int64, C.c_int, C.c_int, _P, _P, _P, _P]),
     "QTrkB200RefineZLUT": (None, [_TRK, _P, C.c_int, C.c_int64, C.c_int, C.c_int, C.c_int, _P, C.c_int, C.c_float,

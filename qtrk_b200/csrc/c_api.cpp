@@ -248,6 +248,16 @@ QTRK_API void QTRK_CALLCONV QTrkBuildLUT(QueuedTracker *q, void *data, int pitch
     guarded(q, "QTrkBuildLUT", [&](Tracker *t) { t->BuildLUT(data, pitch, pdt, plane, known_pos); });
 }
 
+// QTrkBuildLUT for a stack in pinned host memory that stays unchanged until QTrkFinalizeLUT
+// returns: the call returns once the plane's copy and kernel are queued. No counterpart in the
+// reference (its BuildLUT is synchronous); a pageable stack is staged before the call returns, as
+// by QTrkBuildLUT.
+QTRK_API void QTRK_CALLCONV QTrkB200BuildLUTAsync(QueuedTracker *q, void *data, int pitch, QTRK_PixelDataType_t pdt,
+                                                  int plane, vector2f *known_pos)
+{
+    guarded(q, "QTrkB200BuildLUTAsync", [&](Tracker *t) { t->BuildLUT(data, pitch, pdt, plane, known_pos, true); });
+}
+
 // Declared (never defined) at cputrack/qtrk_c_api.h:184: BuildLUT from ROIs cropped out of a
 // float frame; ROI i belongs to bead i.
 QTRK_API void QTRK_CALLCONV QTrkBuildLUTFromFrame(QueuedTracker *q, ImageData *frame, int plane, ROIPosition *roipos,

@@ -1395,8 +1395,11 @@ void Tracker::BeginLUT(uint32_t flags)
 
 // QueuedCPUTracker::BuildLUT, QueuedCPUTracker.cpp:580-646: `data` holds one ROI per bead,
 // bead i at data + pitch*height*i. The rows are staged (double-buffered) and the profiles are
-// accumulated into the device LUT by one kernel launch per plane.
-void Tracker::BuildLUT(const void *data, int pitch, int pdt, int plane, const vector2f *known_pos)
+// accumulated into the device LUT by one kernel launch per plane. With `async` a pinned stack is
+// still being copied when the call returns (the caller keeps it unchanged until FinalizeLUT returns),
+// so the copies of successive planes run back to back instead of each waiting for the caller's
+// next call; at most two planes are in flight (the device staging buffers).
+void Tracker::BuildLUT(const void *data, int pitch, int pdt, int plane, const vector2f *known_pos, bool async)
 {
     if (!data) throw std::invalid_argument("BuildLUT: null data");
     if (pdt < 0 || pdt > 2) throw std::invalid_argument("BuildLUT: unknown pixel data type");
@@ -1463,7 +1466,7 @@ void Tracker::BuildLUT(const void *data, int pitch, int pdt, int plane, const ve
     CheckCuda(cudaEventRecord(lut_stage_free_[b], lut_stream_), "cudaEventRecord");
     CheckCuda(cudaEventRecord(lut_ready_, lut_stream_), "cudaEventRecord");
     tc_lut_stale_ = lut_t_stale_ = true;
-    if (pinned) CheckCuda(cudaEventSynchronize(lut_copy_done_[b]), "cudaEventSynchronize(LUT copy)");
+    if (pinned && !async) CheckCuda(cudaEventSynchronize(lut_copy_done_[b]), "cudaEventSynchronize(LUT copy)");
 }
 
 // QueuedCPUTracker::FinalizeLUT, QueuedCPUTracker.cpp:648-659.

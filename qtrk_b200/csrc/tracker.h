@@ -62,7 +62,8 @@ class Tracker : public QueuedTracker {
     void EnableRadialZLUTCompareProfile(bool enabled);
     void GetRadialZLUTCompareProfile(float *dst);
     void BeginLUT(uint32_t flags);
-    void BuildLUT(const void *data, int pitch, int pdt, int plane, const vector2f *known_pos);
+    // async: a pinned `data` may still be read after the call returns, until FinalizeLUT returns
+    void BuildLUT(const void *data, int pitch, int pdt, int plane, const vector2f *known_pos, bool async = false);
     void FinalizeLUT();
     int GetResultCount();
     int FetchResults(LocalizationResult *dst, int maxResults);

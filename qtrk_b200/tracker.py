@@ -136,6 +136,17 @@ class QTrkInstance:
         self.lib.QTrkBuildLUT(self.handle, stack.ctypes.data_as(C.c_void_p), stack.shape[2] * stack.itemsize, pdt,
                               int(plane), None if kp is None else kp.ctypes.data_as(C.c_void_p))
 
+    def BuildLUTAsync(self, stack: np.ndarray, plane: int, known_pos: np.ndarray | None = None) -> None:
+        """BuildLUT that does not wait for the plane's copy: `stack` (nbeads, H, W), contiguous and in
+        pinned memory for the copy to be asynchronous, must stay alive and unchanged until FinalizeLUT
+        returns."""
+        if not stack.flags.c_contiguous:
+            raise ValueError("BuildLUTAsync needs a contiguous stack (it is read after the call returns)")
+        pdt = abi.NUMPY_PDT[stack.dtype]
+        kp = None if known_pos is None else np.ascontiguousarray(known_pos, np.float32)
+        self.lib.QTrkB200BuildLUTAsync(self.handle, stack.ctypes.data_as(C.c_void_p), stack.shape[2] * stack.itemsize,
+                                       pdt, int(plane), None if kp is None else kp.ctypes.data_as(C.c_void_p))
+
     def FinalizeLUT(self) -> None:
         self.lib.QTrkFinalizeLUT(self.handle)
 

@@ -191,3 +191,31 @@ def test_buildlut_pinned_and_pageable_agree():
             t.FinalizeLUT()
             luts.append(t.GetRadialZLUT())
     assert np.array_equal(luts[0], luts[1])
+
+
+def test_buildlut_async_equals_buildlut():
+    """QTrkB200BuildLUTAsync over a whole pinned stack (the copies of successive planes queued
+    without waiting; the stack untouched until FinalizeLUT returns) gives the LUT that QTrkBuildLUT
+    gives, bit for bit; a pageable stack through the async entry as well."""
+    import torch
+
+    s, stack, centres = synth.calib_stack_80x80(nbeads=8, planes=30, seed=16)
+    pinned = torch.empty(stack.shape, dtype=torch.int16).pin_memory().numpy().view(np.uint16)
+    pinned[:] = stack
+    luts = []
+    for form in ("sync", "async_pinned", "async_pageable"):
+        with QTrkInstance(s) as t:
+            t.SetRadialZLUTSize(8, 30)
+            t.BeginLUT(abi.BUILDLUT_NORMALIZE)
+            for k in range(30):
+                kp = centres if k % 3 else None
+                if form == "sync":
+                    t.BuildLUT(stack[k], k, known_pos=kp)
+                elif form == "async_pinned":
+                    t.BuildLUTAsync(pinned[k], k, known_pos=kp)
+                else:
+                    t.BuildLUTAsync(stack[k], k, known_pos=kp)
+            t.FinalizeLUT()
+            luts.append(t.GetRadialZLUT())
+    assert np.array_equal(luts[0], luts[1])
+    assert np.array_equal(luts[0], luts[2])
