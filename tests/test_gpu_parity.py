@@ -431,6 +431,19 @@ def test_com_only_streaming_kernel_matches_reference(ref, case):
     assert np.array_equal(r["frame"], r_ref["frame"])
 
 
+@pytest.mark.parametrize("count", [1, 5, 23])
+def test_com_only_few_rois_match_reference(ref, count):
+    """Fewer ROIs than the COM kernel's ROI groups per CTA (11 for 100x100 u16): the groups without a
+    ROI start no copy and leave at once; the others match the reference."""
+    wl = synth.roi100_u16(count, seed=37)
+    r_ref = ref.track(wl.settings, abi.LT_OnlyCOM, wl.rois)
+    with make_tracker(wl.settings, abi.LT_OnlyCOM) as t:
+        r = t.Localize(wl.rois)
+    assert np.abs(r["pos"][:, :2] - r_ref["pos"][:, :2]).max() < TOL_COM
+    assert (r["error"] == r_ref["error"]).all()
+    np.testing.assert_allclose(r["imageMean"], r_ref["imageMean"], rtol=1e-6)
+
+
 def test_com_only_full_size_equals_fused_kernel_com():
     """Full BASELINE config-2 size (10,000 ROIs of 100x100 u16, device-resident): the streaming COM
     kernel's positions and image means equal the COM stage of the fused localization kernel (its
