@@ -156,9 +156,12 @@ __device__ __forceinline__ void chunk_moments(const float (&v)[ChunkPixels<PDT>:
 
 // chunk_moments for a chunk of 8 u16 pixels without a background threshold, on packed FP32x2
 // pairs: v - mean is formed per pixel exactly as the scalar form forms it (the pixel is exact in
-// FP32), and the sums S and Sj run as two interleaved halves added at the end.
-__device__ __forceinline__ void chunk_moments_u16(const uint4 &q, const ChunkWalk &w, float fW, float mean, float &q0,
-                                                  float &qx, float &qy)
+// FP32), and the sums S and Sj run as two interleaved halves added at the end. Chunks start at
+// multiples of 8 pixels, so with W a multiple of 8 no chunk crosses a row end, and with W = 8k + 4
+// a chunk that does crosses it after its fourth pixel (rows start at 0 or 4 mod 8): then the pixels
+// on the next row are the second half, whose sum the packed additions already form. wmod8 = W % 8.
+__device__ __forceinline__ void chunk_moments_u16(const uint4 &q, const ChunkWalk &w, float fW, int wmod8, float mean,
+                                                  float &q0, float &qx, float &qy)
 {
     const float2 nK = make_float2(-8388608.0f, -8388608.0f), nm = make_float2(-mean, -mean);
     const uint32_t wd[4] = {q.x, q.y, q.z, q.w};
@@ -170,7 +173,8 @@ __device__ __forceinline__ void chunk_moments_u16(const uint4 &q, const ChunkWal
         const float2 d = __fadd2_rn(__fadd2_rn(x, nK), nm);
         a[k] = make_float2(fabsf(d.x), fabsf(d.y));
     }
-    const float2 S2 = __fadd2_rn(__fadd2_rn(a[0], a[1]), __fadd2_rn(a[2], a[3]));
+    const float2 h23 = __fadd2_rn(a[2], a[3]);
+    const float2 S2 = __fadd2_rn(__fadd2_rn(a[0], a[1]), h23);
     float2 J2 = __fmul2_rn(a[0], make_float2(0.0f, 1.0f));
     J2 = __ffma2_rn(a[1], make_float2(2.0f, 3.0f), J2);
     J2 = __ffma2_rn(a[2], make_float2(4.0f, 5.0f), J2);
@@ -178,7 +182,9 @@ __device__ __forceinline__ void chunk_moments_u16(const uint4 &q, const ChunkWal
     const float S = S2.x + S2.y, Sj = J2.x + J2.y;
     const float split = fW - w.fx;  // first j on the next row
     float Sw = 0.0f;
-    if (split < 8.0f) {
+    if (wmod8 == 4) {
+        if (split < 8.0f) Sw = h23.x + h23.y;
+    } else if (wmod8 != 0 && split < 8.0f) {
 #pragma unroll
         for (int j = 0; j < 8; j++)
             if ((float)j >= split) Sw += (j & 1) ? a[j >> 1].y : a[j >> 1].x;
@@ -395,20 +401,6 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
-// The first four pixels of a chunk set to zero (LT_ClearFirstFourPixels, QueuedCPUTracker.cpp:280-282).
-template <int PDT>
-__device__ __forceinline__ void clear_first_four(uint4 &q)
-{
-    if (PDT == 0) {
-        q.x = 0u;
-    } else if (PDT == 1) {
-        q.x = 0u;
-        q.y = 0u;
-    } else {
-        q = make_uint4(0u, 0u, 0u, 0u);
-    }
-}
-
 }  // namespace
 
 // Named barrier over the `n` threads of one warp group (id 1..15; 0 is __syncthreads).
@@ -473,11 +465,16 @@ __global__ void __launch_bounds__(1024, 1) com_warp_kernel(TrackParams P, const 
     const bool clear4 = (P.mode & kLT_ClearFirstFourPixels) != 0;
     const bool bg = P.com_bgcorrection != 0.0f;
     const float invN = 1.0f / (float)n, fW = (float)W;
+    const int wmod8 = W & 7;
     const ChunkWalk wk0 = chunk_walk(t, T, ppc, W);
     for (uint32_t it = 0; roi < count; roi += stride, it++) {
         // the leader waits for the copy; the barrier passes the completed copy (and, on the
         // first ROI, the mbarrier's initialisation) to the group, and makes the outcome uniform
         const bool ok = leader ? mbar_wait(mb, it & 1u, kComWaitLimit) : true;
+        // LT_ClearFirstFourPixels (QueuedCPUTracker.cpp:280-282): the leader zeroes them in the buffer once
+        // the copy has landed; the barrier below orders that before every thread's reads
+        if (leader && ok && clear4)
+            for (int k = 0; k < 16 / ppc; k++) reinterpret_cast<uint32_t *>(gbuf)[k] = 0u;
         if (!group_all(ok, bar_id, T)) {
             // the copy did not complete: flag it, give it a last bounded wait (it writes into this
             // CTA's shared memory) and stop the group
@@ -492,8 +489,7 @@ __global__ void __launch_bounds__(1024, 1) com_warp_kernel(TrackParams P, const 
         if (PDT != 2 && !bg) {
             uint32_t si = 0u;  // exact below 2^20 pixels (u16)
             for (int c = t; c < nchunks; c += T) {
-                uint4 q = buf[c];
-                if (clear4 && c == 0) clear_first_four<PDT>(q);
+                const uint4 q = buf[c];
                 if (PDT == 0) {
                     si = __dp4a(q.x, 0x01010101u, si);
                     si = __dp4a(q.y, 0x01010101u, si);
@@ -514,10 +510,8 @@ __global__ void __launch_bounds__(1024, 1) com_warp_kernel(TrackParams P, const 
                 for (int g = 0; g < G; g++) {
                     const int c = c0 + T * g;
                     if (c < nchunks) {
-                        uint4 q = buf[c];
-                        if (clear4 && c == 0) clear_first_four<PDT>(q);
                         float v[ppc];
-                        unpack<PDT>(q, v);
+                        unpack<PDT>(buf[c], v);
 #pragma unroll
                         for (int j = 0; j < ppc; j++) {
                             s += v[j];
@@ -552,10 +546,9 @@ __global__ void __launch_bounds__(1024, 1) com_warp_kernel(TrackParams P, const 
             for (int g = 0; g < G; g++) {
                 const int c = c0 + T * g;
                 if (c < nchunks) {
-                    uint4 q = buf[c];
-                    if (clear4 && c == 0) clear_first_four<PDT>(q);
+                    const uint4 q = buf[c];
                     if (PDT == 1 && !bg) {
-                        chunk_moments_u16(q, w, fW, mean, q0, qx, qy);
+                        chunk_moments_u16(q, w, fW, wmod8, mean, q0, qx, qy);
                     } else {
                         float v[ppc];
                         unpack<PDT>(q, v);

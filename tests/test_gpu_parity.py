@@ -385,7 +385,8 @@ def test_qi_angstep_factor_matches_reference(ref, shape, factor):
     assert np.abs(r1["pos"][:, :2] - r_ref["pos"][:, :2]).max() > 1e-6
 
 
-@pytest.mark.parametrize("case", ["roi100_u16", "roi60_f32", "u8_64", "u16_bgcorr", "f32_clear4", "u16_128", "f32_180"])
+@pytest.mark.parametrize("case", ["roi100_u16", "roi60_f32", "u8_64", "u16_bgcorr", "f32_clear4", "u16_128", "f32_180",
+                                  "u16_64_clear4", "u16_50x40"])
 def test_com_only_streaming_kernel_matches_reference(ref, case):
     """LT_OnlyCOM on ROIs stored back to back runs the COM kernels of com.cu (resident CTAs with a
     bulk-copy ring of ROIs; for ROIs above 100 KB, like 180x180 f32, one CTA per ROI):
@@ -409,6 +410,14 @@ def test_com_only_streaming_kernel_matches_reference(ref, case):
     elif case == "f32_clear4":
         wl = synth.roi60_f32(200, seed=36)
         s, rois = wl.settings, wl.rois
+    elif case == "u16_64_clear4":  # rows of a multiple of 8 pixels: no 16-byte chunk crosses a row end
+        s = abi.settings(width=64, height=64)
+        rois = np.minimum(rng.poisson(synth.render(64, 64, 32 + rng.uniform(-4, 4, 150), 32 + rng.uniform(-4, 4, 150),
+                                                   rng.uniform(0, 10, 150), 200.0, 2000.0)), 65535).astype(np.uint16)
+    elif case == "u16_50x40":  # rows of 8k + 2 pixels: chunks cross row ends after 2 or 6 pixels
+        s = abi.settings(width=50, height=40)
+        rois = np.minimum(rng.poisson(synth.render(50, 40, 25 + rng.uniform(-4, 4, 150), 20 + rng.uniform(-4, 4, 150),
+                                                   rng.uniform(0, 10, 150), 200.0, 2000.0)), 65535).astype(np.uint16)
     elif case == "f32_180":
         s = abi.settings(width=180, height=180)
         rois = rng.poisson(synth.render(180, 180, 90 + rng.uniform(-8, 8, 40), 90 + rng.uniform(-8, 8, 40),
@@ -417,7 +426,7 @@ def test_com_only_streaming_kernel_matches_reference(ref, case):
         s = abi.settings(width=128, height=128, com_bgcorrection=0.3)
         rois = np.minimum(rng.poisson(synth.render(128, 128, 64 + rng.uniform(-6, 6, 100), 64 + rng.uniform(-6, 6, 100),
                                                    rng.uniform(0, 20, 100), 200.0, 2000.0)), 65535).astype(np.uint16)
-    mode = abi.LT_OnlyCOM | (abi.LT_ClearFirstFourPixels if case == "f32_clear4" else 0)
+    mode = abi.LT_OnlyCOM | (abi.LT_ClearFirstFourPixels if case in ("f32_clear4", "u16_64_clear4") else 0)
     r_ref = ref.track(s, mode, rois)
     with make_tracker(s, mode) as t:
         l0 = t.KernelLaunchCount()
