@@ -1,16 +1,20 @@
-// Streaming centre-of-mass kernel for LT_OnlyCOM (sm_100a).
+// Centre-of-mass kernels for LT_OnlyCOM (sm_100a).
 //
 // CPUTracker::ComputeMeanAndCOM (cputrack/cpu_tracker.cpp:681-729) needs two passes over a ROI:
 // mean and standard deviation first, then the background-corrected moments
 //   v' = max(0, |v - mean| - bgcorrection * stdev),  COM = (sum x v', sum y v') / sum v'.
 // The fused localization kernel stages every ROI as a float tile in shared memory because QI and
-// the radial profile sample it many times; a COM-only localization reads each pixel twice, so
-// here the ROI is held in registers instead: one CTA per ROI, every thread loads its share of
-// 16-byte chunks (8 u16, 16 u8 or 4 f32 pixels) with streaming loads, all of them issued before
-// the first is used, converts them to float once, and both passes run on the registers. The sums
-// meet across the CTA in FP64 (warp shuffles, then one value per warp in shared memory), as the
-// reference accumulates in FP64; per-thread partial sums are FP32 over at most 64 pixels (exact
-// for the mean of u8/u16 data, ~1e-7 relative for the moments).
+// the radial profile sample it many times; a COM-only localization reads each pixel twice and
+// needs no tile. Three forms, by ROI size:
+//  - com_warp_kernel (ROIs up to 55 KB): a group of 2-4 warps per ROI and one shared-memory buffer
+//    per group, filled by a bulk copy; both passes run over the raw buffer and the sums meet
+//    through warp shuffles and a named barrier per group, with no CTA-wide barrier;
+//  - com_stream_kernel: one CTA per ROI in flight with a ring of bulk-copied buffers, the ROI read
+//    into registers once;
+//  - com_kernel (ROIs whose ring does not fit): one CTA per ROI, the ROI loaded into registers.
+// The sums meet in FP64, as the reference accumulates in FP64; per-thread partial sums are FP32
+// over at most 64 pixels (exact for the mean of u8/u16 data, ~1e-7 relative for the moments), or
+// exact integers in the warp-group form's first pass.
 //
 // Moments per chunk: a chunk of ppc pixels starts at pixel i0 = (x0, y0) and may cross one row
 // end (at j = W - x0). With S = sum_j v'_j, Sj = sum_j j v'_j and Sw = sum_{j >= W - x0} v'_j,
