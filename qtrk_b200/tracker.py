@@ -60,12 +60,14 @@ class QTrkInstance:
             raise RuntimeError("QTrkCreateInstance failed: " + last_error())
         self.config = abi.QTrkComputedConfig()
         self.lib.QTrkGetComputedConfig(C.byref(settings), C.byref(self.config))
+        self._async_stacks: list = []  # stacks handed to BuildLUTAsync, kept alive until FinalizeLUT
 
     # -- lifecycle --
     def Destroy(self) -> None:
         if self.handle:
             self.lib.QTrkFreeInstance(self.handle)
             self.handle = None
+        self._async_stacks = []
 
     def __enter__(self):
         return self
@@ -138,10 +140,11 @@ class QTrkInstance:
 
     def BuildLUTAsync(self, stack: np.ndarray, plane: int, known_pos: np.ndarray | None = None) -> None:
         """BuildLUT that does not wait for the plane's copy: `stack` (nbeads, H, W), contiguous and in
-        pinned memory for the copy to be asynchronous, must stay alive and unchanged until FinalizeLUT
-        returns."""
+        pinned memory for the copy to be asynchronous, must stay unchanged until FinalizeLUT returns
+        (the instance holds a reference to it until then, so it stays alive)."""
         if not stack.flags.c_contiguous:
             raise ValueError("BuildLUTAsync needs a contiguous stack (it is read after the call returns)")
+        self._async_stacks.append(stack)
         pdt = abi.NUMPY_PDT[stack.dtype]
         kp = None if known_pos is None else np.ascontiguousarray(known_pos, np.float32)
         self.lib.QTrkB200BuildLUTAsync(self.handle, stack.ctypes.data_as(C.c_void_p), stack.shape[2] * stack.itemsize,
@@ -149,6 +152,7 @@ class QTrkInstance:
 
     def FinalizeLUT(self) -> None:
         self.lib.QTrkFinalizeLUT(self.handle)
+        self._async_stacks = []
 
     # -- scheduling --
     def ScheduleLocalization(self, img: np.ndarray, frame: int = 0, zlut: int = 0, timestamp: int = 0) -> None:
