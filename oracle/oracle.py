@@ -224,6 +224,7 @@ class PortOracle:
                                                  P, C.c_int, _f64p, P]),
             "oracle_joint_refine": (None, [_f64p, C.c_int, C.c_int, C.c_double, _f64p, _f32p, C.c_int, C.c_int,
                                            C.c_int, C.c_double, C.c_double, P, C.c_int, C.c_int]),
+            "oracle_set_joint_prior_scale": (None, [C.c_double]),
             "oracle_zlut_bias_correct": (C.c_double, [C.c_double, C.c_int, _f32p, C.c_int, C.c_int, C.c_int]),
             "oracle_gauss_nll_grad": (C.c_double, [_f64p, C.c_int, C.c_int, _f64p, _f64p]),
             "oracle_find_beads": (C.c_int, [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,

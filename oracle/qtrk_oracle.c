@@ -710,11 +710,18 @@ ORACLE_API double oracle_zcost_grad(const double *img, int w, int h, double mean
     return cost;
 }
 
+/* Stiffness of the joint refinement's (x, y) prior in units of the cost's curvature along z
+ * (100, as the GPU path uses); settable so that tests can sweep it. */
+static double g_joint_prior_scale = 100.0;
+
+ORACLE_API void oracle_set_joint_prior_scale(double scale) { g_joint_prior_scale = scale; }
+
 /*
  * Joint Gauss-Newton refinement of (x, y, z) on the cost above plus a quadratic prior that ties
  * (x, y) to their starting point (the QI estimate):
  *   E = cost(x, y, z) + k ((x - x0)^2 + (y - y0)^2),  k = 100 sum_r w_r^2 (L_iz+1,r - L_iz,r)^2,
- * 100 times the curvature of the cost along z at the starting plane. The prior is needed because
+ * 100 times the curvature of the cost along z at the starting plane (the factor is
+ * g_joint_prior_scale, 100 unless a test sets it). The prior is needed because
  * a radial profile is, to first order, insensitive to where its centre is (the x-derivative of a
  * radially symmetric image averages to zero over a circle), so the cost alone leaves x and y
  * undetermined and its noise-driven minimum lies ~0.1 px from the truth where QI is ~0.02 px
@@ -769,7 +776,7 @@ ORACLE_API void oracle_joint_refine(const double *img, int w, int h, double mean
                 for (int b = 0; b < 3; b++) A[a][b] += wr * wr * J[a] * J[b];
             }
         }
-        if (s == 0) k = 100.0 * A[2][2];
+        if (s == 0) k = g_joint_prior_scale * A[2][2];
         cur = cost + k * ((x - x0) * (x - x0) + (y - y0) * (y - y0));
         A[0][0] += k;
         A[1][1] += k;
