@@ -66,3 +66,30 @@ def test_reference_arm_prints_one_contract_line():
     assert d["impl"] == "reference" and d["value"] > 0 and d["warmup"] >= 3 and d["higher_is_better"] is True
     assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def test_issue_limits_from_the_committed_profile_counts():
+    """The bench line's issue and shared-memory fractions: warp instructions over 148 SMs x 4
+    schedulers x clock x time, wavefronts over 148 x clock x time, and the larger one named."""
+    import json
+
+    for name in ("localize_100x100_u16_traffic.json", "com_100x100_u16_traffic.json"):
+        path = bench.ROOT / "profiles" / name
+        d = json.loads(path.read_text())
+        out = bench.issue_limits(path, 1.0, 2000.0)  # 1 ms at 2 GHz: 2e6 cycles
+        assert abs(out["issue_frac"] - d["warp_instructions_per_launch"] / (148 * 4 * 2e6)) < 1e-12
+        assert abs(out["smem_pipe_frac"] - d["smem_wavefronts_per_launch"] / (148 * 2e6)) < 1e-12
+        want = "instruction issue" if out["issue_frac"] >= out["smem_pipe_frac"] else "shared-memory pipe"
+        assert out["binding_limit"] == want
+        assert out["counts_source"] == f"profiles/{name}"
+    # the fused kernel is bound by its shared-memory gathers, the COM-only kernel by issue
+    fused = bench.issue_limits(bench.ROOT / "profiles" / "localize_100x100_u16_traffic.json", 1.003, 1965.0)
+    com = bench.issue_limits(bench.ROOT / "profiles" / "com_100x100_u16_traffic.json", 0.0576, 1965.0)
+    assert fused["binding_limit"] == "shared-memory pipe" and com["binding_limit"] == "instruction issue"
+
+
+def test_issue_limits_without_counts_or_clock():
+    out = bench.issue_limits(bench.ROOT / "profiles" / "no_such_file.json", 1.0, 2000.0)
+    assert out == {"binding_limit": None, "issue_frac": None, "smem_pipe_frac": None}
+    out = bench.issue_limits(bench.ROOT / "profiles" / "com_100x100_u16_traffic.json", 1.0, None)
+    assert out["issue_frac"] is None
