@@ -1,8 +1,8 @@
 """GPU parity: libqtrk_b200 (through its C ABI) against the reference CPU tracker.
 
 The oracle is the reference's own QueuedCPUTracker (oracle/_ref, when built) and the
-committed golden fixtures it produced (tests/golden/). Tolerances (north star):
-COM 1e-4 px, QI x/y 1e-3 px, Z 0.01 plane; error flags must be identical.
+committed golden fixtures it produced (tests/golden/). Tolerances: COM 1e-4 px, QI x/y
+1e-3 px, Z 0.01 plane; error flags must be identical.
 """
 import ctypes as C
 
